@@ -1,0 +1,55 @@
+"""Compile the native library ``_native/libem3d_b200.so`` for sm_100a with nvcc."""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+NATIVE = os.path.join(HERE, "_native")
+LIB = os.path.join(NATIVE, "libem3d_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-shared",
+    "--expt-relaxed-constexpr",
+]
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    return any(os.path.getmtime(p) > t for p in deps)
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile every ``csrc/*.cu`` into one shared library; returns its path."""
+    if not force and not needs_build():
+        return LIB
+    os.makedirs(NATIVE, exist_ok=True)
+    nvcc = os.environ.get("NVCC", "nvcc")
+    tmp = LIB + ".tmp"
+    cmd = [nvcc, *NVCC_FLAGS, "-I", INCLUDE, *sources(), "-o", tmp]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd))
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"nvcc failed ({proc.returncode}):\n{proc.stdout}\n{proc.stderr}")
+    if verbose and proc.stderr:
+        print(proc.stderr)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose=True, force=True))

@@ -1,0 +1,112 @@
+"""ctypes binding of the C ABI declared in ``include/em3d_b200.h``.
+
+The library is loaded from the package's ``_native`` folder.  There is no
+fallback: if the shared library is missing or a call fails, an exception is
+raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_int, c_int32, c_size_t, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_native", "libem3d_b200.so")
+
+EM3D_OK = 0
+EM3D_ERR_INVALID = 1
+EM3D_ERR_CUDA = 2
+EM3D_ERR_UNSUPPORTED = 3
+EM3D_C64 = 0
+EM3D_C128 = 1
+EM3D_ACOUSTIC = 1
+EM3D_EM = 3
+
+
+class EmGrid(ctypes.Structure):
+    _fields_ = [("nx", c_int32), ("ny", c_int32), ("nz", c_int32),
+                ("lx", c_double), ("ly", c_double), ("lz", c_double)]
+
+
+class NativeError(RuntimeError):
+    """A native entry point returned a non-zero status."""
+
+
+# name -> (restype, argtypes); every entry point of include/em3d_b200.h
+_GRID = POINTER(EmGrid)
+SIGNATURES = {
+    "em3d_abi_version": (c_int, []),
+    "em3d_last_error": (ctypes.c_char_p, []),
+    "em3d_spectrum_bytes": (c_size_t, [_GRID, c_int, c_int]),
+    "em3d_build_workspace_bytes": (c_size_t, [_GRID]),
+    "em3d_apply_workspace_bytes": (c_size_t, [_GRID, c_int, c_int, c_int]),
+    "em3d_em_spectrum_build": (c_int, [_GRID, c_double, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "em3d_acoustic_spectrum_build": (c_int, [_GRID, c_double, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "em3d_em_kernel_hat_full": (c_int, [_GRID, c_double, c_int, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "em3d_acoustic_kernel_hat_full": (c_int, [_GRID, c_double, c_int, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "em3d_em_matvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
+                               c_void_p, c_void_p]),
+    "em3d_em_rmatvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
+                                c_void_p, c_void_p]),
+    "em3d_acoustic_matvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_size_t, c_void_p, c_void_p]),
+    "em3d_acoustic_rmatvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                      c_size_t, c_void_p, c_void_p]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the native library once (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"em3d_b200 native library not found at {LIB_PATH}; build it with "
+            "`python -c 'import __graft_entry__ as g; g.build()'` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().em3d_last_error().decode("utf-8", "replace")
+
+
+def check(status: int, what: str) -> None:
+    if status == EM3D_OK:
+        return
+    msg = last_error()
+    if status == EM3D_ERR_INVALID or status == EM3D_ERR_UNSUPPORTED:
+        raise ValueError(f"{what}: {msg}")
+    raise NativeError(f"{what}: CUDA error: {msg}")
+
+
+def call(name: str, *args) -> int:
+    """Call ``name`` and raise on a non-zero status."""
+    fn = getattr(load(), name)
+    status = fn(*args)
+    check(status, name)
+    return status
+
+
+def make_grid(N, L) -> EmGrid:
+    return EmGrid(int(N[0]), int(N[1]), int(N[2]), float(L[0]), float(L[1]), float(L[2]))
+
+
+def ptr(t) -> int:
+    """Raw device address of a torch tensor (or None -> NULL)."""
+    return None if t is None else t.data_ptr()
+
+
+def stream_handle(stream=None) -> int:
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

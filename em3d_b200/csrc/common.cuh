@@ -1,0 +1,63 @@
+// Shared device helpers for the em3d B200 library: complex arithmetic on
+// float2 / double2, launch checks, the skip flag used by device-resident
+// solver loops.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/em3d_b200.h"
+
+namespace em3d {
+
+template <typename R> struct Cx;
+template <> struct Cx<float> { using T = float2; };
+template <> struct Cx<double> { using T = double2; };
+template <typename R> using cx = typename Cx<R>::T;
+
+template <typename R> __host__ __device__ __forceinline__ cx<R> mk(R re, R im) {
+  cx<R> v; v.x = re; v.y = im; return v;
+}
+template <typename C> __host__ __device__ __forceinline__ C cadd(C a, C b) { a.x += b.x; a.y += b.y; return a; }
+template <typename C> __host__ __device__ __forceinline__ C csub(C a, C b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
+  C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+// conj(a) * b
+template <typename C> __host__ __device__ __forceinline__ C cmulcj(C a, C b) {
+  C r; r.x = a.x * b.x + a.y * b.y; r.y = a.x * b.y - a.y * b.x; return r;
+}
+template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+template <typename C, typename S> __host__ __device__ __forceinline__ C cscale(C a, S s) { a.x *= s; a.y *= s; return a; }
+// multiply by -i (forward) or +i (inverse)
+template <typename C> __host__ __device__ __forceinline__ C mul_mi(C a) { C r; r.x = a.y; r.y = -a.x; return r; }
+template <typename C> __host__ __device__ __forceinline__ C mul_pi(C a) { C r; r.x = -a.y; r.y = a.x; return r; }
+
+__host__ __device__ __forceinline__ double2 to_c64(float2 a) { return make_double2(a.x, a.y); }
+__host__ __device__ __forceinline__ double2 to_c64(double2 a) { return a; }
+template <typename R> __host__ __device__ __forceinline__ cx<R> from_c64(double2 a);
+template <> __host__ __device__ __forceinline__ float2 from_c64<float>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+template <> __host__ __device__ __forceinline__ double2 from_c64<double>(double2 a) { return a; }
+
+// A kernel launched inside a device-resident solver loop returns at once when
+// the loop's status word says the solve has already stopped.
+__device__ __forceinline__ bool skip_launch(const int* flag) {
+  return flag != nullptr && *(volatile const int*)flag != 0;
+}
+
+}  // namespace em3d
+
+#define EM3D_CUDA_TRY(expr)                                     \
+  do {                                                          \
+    cudaError_t _e = (expr);                                    \
+    if (_e != cudaSuccess) { em3d_set_last_error(cudaGetErrorString(_e)); return EM3D_ERR_CUDA; } \
+  } while (0)
+
+#define EM3D_LAUNCH_CHECK()                                     \
+  do {                                                          \
+    cudaError_t _e = cudaGetLastError();                        \
+    if (_e != cudaSuccess) { em3d_set_last_error(cudaGetErrorString(_e)); return EM3D_ERR_CUDA; } \
+  } while (0)
+
+void em3d_set_last_error(const char* msg);

@@ -1,0 +1,277 @@
+"""EM operator ``A = I - B chi`` on the B200: ``PreparedEMKernel`` and ``Operator``.
+
+Drop-in mirror of the reference ``src/em3d/operator.py:151-428``:
+
+* ``PreparedEMKernel.build(grid, *, k, include_adjoint=True,
+  adjoint_storage="explicit"|"derived", build_strategy="standard"|"streamed")``
+  samples the dyadic Green kernel and transforms it in FP64 on the device
+  (``em3d_em_spectrum_build``) and keeps one symmetric octant of the spectrum
+  in the operator precision.  Because the stored blocks are exactly even or
+  odd per axis, the adjoint spectrum ``conj(K_hat(-k))`` equals
+  ``conj(K_hat(k))``: the explicit and the derived adjoint storages share the
+  same bytes, and ``persistent_nbytes`` is about 1/12 of the reference's.
+  ``kernel_hat`` / ``kernel_hat_adjoint`` materialise the reference's full
+  (3,3,2Nx,2Ny,2Nz) spectra on demand.
+* ``Operator(problem, *, prepared_kernel=None)`` applies ``matvec`` /
+  ``rmatvec`` through the five fused passes of ``em3d_em_matvec`` /
+  ``em3d_em_rmatvec``; fields may carry leading batch dimensions.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from math import prod
+from typing import Literal
+
+import numpy as np
+
+from . import _lib
+from .problem import Grid, Problem
+
+AdjointStorage = Literal["explicit", "derived", "none"]
+KernelBuildStrategy = Literal["standard", "streamed"]
+
+
+def _uint8(nbytes, device):
+    import torch
+
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=device)
+
+
+def _build_workspace(grid: Grid):
+    g = _lib.make_grid(grid.N, grid.L)
+    nb = _lib.load().em3d_build_workspace_bytes(ctypes_ref(g))
+    if nb == 0:
+        _lib.check(_lib.EM3D_ERR_INVALID, "em3d_build_workspace_bytes")
+    return g, _uint8(nb, grid.backend.torch_device)
+
+
+def ctypes_ref(obj):
+    import ctypes
+
+    return ctypes.byref(obj)
+
+
+@dataclass(frozen=True)
+class PreparedEMKernel:
+    """Reusable spectrum of the EM convolution kernel for one (grid, k, device, precision)."""
+
+    grid_shape: tuple
+    grid_lengths: tuple
+    wave_number: float
+    device: str
+    precision: str
+    spectrum: object = field(repr=False)
+    adjoint_storage: AdjointStorage = "explicit"
+    build_strategy: KernelBuildStrategy = "standard"
+    _backend: object = field(default=None, repr=False, compare=False)
+    _cache: dict = field(default_factory=dict, repr=False, compare=False)
+
+    @classmethod
+    def build(cls, grid: Grid, *, k: float, include_adjoint: bool = True,
+              adjoint_storage: Literal["explicit", "derived"] = "explicit",
+              build_strategy: KernelBuildStrategy = "standard") -> "PreparedEMKernel":
+        if build_strategy not in {"standard", "streamed"}:
+            raise ValueError(f"build_strategy must be 'standard' or 'streamed', got {build_strategy!r}")
+        if adjoint_storage not in {"explicit", "derived"}:
+            raise ValueError(f"adjoint_storage must be 'explicit' or 'derived', got {adjoint_storage!r}")
+        storage = adjoint_storage if include_adjoint else "none"
+        be = grid.backend
+        g, ws = _build_workspace(grid)
+        dt = be.precision.native_dtype
+        nbytes = _lib.load().em3d_spectrum_bytes(ctypes_ref(g), _lib.EM3D_EM, dt)
+        spec = _uint8(nbytes, be.torch_device)
+        _lib.call("em3d_em_spectrum_build", ctypes_ref(g), float(k), dt, spec.data_ptr(), ws.data_ptr(),
+                  ws.numel(), _lib.stream_handle())
+        del ws
+        return cls(grid_shape=tuple(int(n) for n in grid.N), grid_lengths=tuple(float(v) for v in grid.L),
+                   wave_number=float(k), device=str(be.device), precision=str(be.precision.value),
+                   spectrum=spec, adjoint_storage=storage, build_strategy=build_strategy, _backend=be)
+
+    @property
+    def supports_adjoint(self) -> bool:
+        return self.adjoint_storage != "none"
+
+    @property
+    def persistent_nbytes(self) -> int:
+        return int(self.spectrum.numel())
+
+    def _full(self, adjoint: bool):
+        import torch
+
+        key = "adjoint" if adjoint else "forward"
+        if key not in self._cache:
+            be = self._backend
+            N = self.grid_shape
+            g = _lib.make_grid(N, self.grid_lengths)
+            nb = _lib.load().em3d_build_workspace_bytes(ctypes_ref(g))
+            ws = _uint8(nb, be.torch_device)
+            out = torch.empty((3, 3) + tuple(2 * n for n in N), dtype=be.precision.torch_complex,
+                              device=be.torch_device)
+            _lib.call("em3d_em_kernel_hat_full", ctypes_ref(g), self.wave_number, be.precision.native_dtype,
+                      int(adjoint), out.data_ptr(), ws.data_ptr(), ws.numel(), _lib.stream_handle())
+            self._cache[key] = out
+        return self._cache[key]
+
+    @property
+    def kernel_hat(self):
+        """Reference-layout spectrum ``fftn(K)``, (3,3,2Nx,2Ny,2Nz), built on first access."""
+        return self._full(False)
+
+    @property
+    def kernel_hat_adjoint(self):
+        """``fftn(conj K)`` when the kernel was built with the explicit adjoint storage, else None."""
+        if self.adjoint_storage != "explicit":
+            return None
+        return self._full(True)
+
+    def validate(self, grid: Grid, *, k: float) -> None:
+        errors = []
+        if tuple(grid.N) != self.grid_shape:
+            errors.append(f"grid shape {grid.N!r} != {self.grid_shape!r}")
+        if not np.allclose(grid.L, self.grid_lengths, rtol=0.0, atol=0.0):
+            errors.append(f"grid lengths {grid.L!r} != {self.grid_lengths!r}")
+        if not np.isclose(float(k), self.wave_number, rtol=1e-14, atol=1e-14):
+            errors.append(f"wave number {k!r} != {self.wave_number!r}")
+        if grid.backend.device != self.device:
+            errors.append(f"device {grid.backend.device!r} != {self.device!r}")
+        if grid.backend.precision.value != self.precision:
+            errors.append(f"precision {grid.backend.precision.value!r} != {self.precision!r}")
+        if errors:
+            raise ValueError("incompatible PreparedEMKernel: " + "; ".join(errors))
+
+
+def prep_coeffs_em3d(grid: Grid, *, k: float, volume=None):
+    """``PreparedEMKernel.build(grid, k=k, include_adjoint=False).kernel_hat``."""
+    return PreparedEMKernel.build(grid, k=k, include_adjoint=False).kernel_hat
+
+
+def prep_conj_coeffs_em3d(grid: Grid, *, k: float, volume=None):
+    return PreparedEMKernel.build(grid, k=k, include_adjoint=True, adjoint_storage="explicit").kernel_hat_adjoint
+
+
+class _Applier:
+    """Shared plumbing of the EM and acoustic operators: field checks,
+    workspace per batch size, native calls."""
+
+    _kind = _lib.EM3D_EM
+
+    def _setup_native(self, grid: Grid, spectrum, chi):
+        self._grid_c = _lib.make_grid(grid.N, grid.L)
+        self._spectrum = spectrum
+        self._chi = chi.contiguous()
+        self._workspaces = {}
+        self._dt = self._be.precision.native_dtype
+        self._tc = self._be.precision.torch_complex
+
+    def _field_shape(self):
+        raise NotImplementedError
+
+    def workspace(self, batch: int):
+        ws = self._workspaces.get(batch)
+        if ws is None:
+            nb = _lib.load().em3d_apply_workspace_bytes(ctypes_ref(self._grid_c), self._kind, self._dt, int(batch))
+            if nb == 0:
+                _lib.check(_lib.EM3D_ERR_INVALID, "em3d_apply_workspace_bytes")
+            ws = _uint8(nb, self._be.torch_device)
+            self._workspaces[batch] = ws
+        return ws
+
+    def _as_field(self, x, name="field"):
+        import torch
+
+        fs = self._field_shape()
+        if not isinstance(x, torch.Tensor):
+            x = torch.as_tensor(np.asarray(x))
+        if tuple(x.shape[-len(fs):]) != fs:
+            raise ValueError(f"{name}.shape {tuple(x.shape)} != expected (..., {', '.join(map(str, fs))})")
+        x = x.to(device=self._be.torch_device, dtype=self._tc)
+        return x.contiguous()
+
+    def _batch_of(self, x):
+        fs = self._field_shape()
+        lead = tuple(x.shape[: x.dim() - len(fs)])
+        return int(prod(lead)) if lead else 1
+
+    def apply_into(self, x, out, *, adjoint: bool = False, skip=None, stream=None):
+        """Write ``A x`` (or ``A* x``) into ``out`` without allocating.  ``x`` and
+        ``out`` are contiguous device tensors of the operator dtype; ``skip``
+        is an optional device int32 tensor (non-zero: kernels return at once)."""
+        b = self._batch_of(x)
+        ws = self.workspace(b)
+        name = self._native_names[1 if adjoint else 0]
+        _lib.call(name, ctypes_ref(self._grid_c), self._dt, b, self._spectrum.data_ptr(), self._chi.data_ptr(),
+                  x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(),
+                  None if skip is None else skip.data_ptr(), _lib.stream_handle(stream))
+        return out
+
+
+class Operator(_Applier):
+    """``A = I - B chi`` for one EM problem (reference ``src/em3d/operator.py:320-428``)."""
+
+    _kind = _lib.EM3D_EM
+    _native_names = ("em3d_em_matvec", "em3d_em_rmatvec")
+
+    def __init__(self, problem: Problem, *, prepared_kernel: PreparedEMKernel | None = None):
+        self.problem = problem
+        grid = problem.grid
+        if prepared_kernel is None:
+            prepared_kernel = PreparedEMKernel.build(grid, k=problem.k0)
+        else:
+            prepared_kernel.validate(grid, k=problem.k0)
+        self._prepared_kernel = prepared_kernel
+        self._be = grid.backend
+        self._N = tuple(grid.N)
+        self._setup_native(grid, prepared_kernel.spectrum, problem.eps_tensor)
+
+    @property
+    def backend(self):
+        return self._be
+
+    @property
+    def shape(self):
+        d = 3 * prod(self._N)
+        return d, d
+
+    @property
+    def prepared_kernel(self) -> PreparedEMKernel:
+        return self._prepared_kernel
+
+    def _field_shape(self):
+        return (3,) + self._N
+
+    def matvec(self, field):
+        x = self._as_field(field)
+        import torch
+
+        out = torch.empty_like(x)
+        return self.apply_into(x, out)
+
+    def rmatvec(self, field):
+        if not self._prepared_kernel.supports_adjoint:
+            raise RuntimeError("adjoint action is unavailable: build PreparedEMKernel with include_adjoint=True")
+        x = self._as_field(field)
+        import torch
+
+        out = torch.empty_like(x)
+        return self.apply_into(x, out, adjoint=True)
+
+    def matvec_flat(self, vector):
+        from .layout import flatten_field, unflatten_field
+
+        return flatten_field(self.matvec(unflatten_field(vector, self._N)))
+
+    def rmatvec_flat(self, vector):
+        from .layout import flatten_field, unflatten_field
+
+        return flatten_field(self.rmatvec(unflatten_field(vector, self._N)))
+
+    def iteration_matvec_flat(self, vector, *, mu: complex):
+        if abs(mu) == 0.0:
+            raise ValueError("mu must be non-zero")
+        return vector - self.matvec_flat(vector) / complex(mu)
+
+    def to_dense_operator(self):
+        raise RuntimeError("dense matrix construction requires a NumPy backend")
+
+    to_dense_kernel = to_dense_operator
+    to_dense = to_dense_operator

@@ -1,0 +1,187 @@
+"""Parity of the B200 operators with the reference (golden vectors) and the oracle.
+
+Tolerances (relative 2-norm): FP64 path <= 1e-12, FP32 path <= 1e-5 against
+the reference's own complex128 / complex64 results on the same inputs.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"double": 1e-12, "single": 1e-5}
+
+
+def _be(prec):
+    import em3d_b200 as e
+
+    return e.Backend.b200(e.Precision.DOUBLE if prec == "double" else e.Precision.SINGLE)
+
+
+def _em_problem(g, prec):
+    import em3d_b200 as e
+
+    N, L, k = tuple(int(v) for v in g["N"]), tuple(float(v) for v in g["L"]), float(g["k"])
+    be = _be(prec)
+    grid = e.Grid(N=N, L=L, center=(0.0, 0.0, 0.0), backend=be)
+    prob = e.Problem(grid=grid, eps_tensor=g[f"chi_{prec}"], wave=g[f"wave_{prec}"], k0=k,
+                     volume=grid.dv * int(np.prod(N)))
+    return be, grid, prob
+
+
+@pytest.mark.parametrize("case", ["sphere16", "cyl_lossy4", "aniso12", "odd567"])
+@pytest.mark.parametrize("prec", ["double", "single"])
+def test_em_matvec_rmatvec_match_reference(case, prec):
+    import em3d_b200 as e
+
+    g = golden(f"em_{case}.npz")
+    be, grid, prob = _em_problem(g, prec)
+    op = e.Operator(prob)
+    u = g[f"u_{prec}"]
+    y = be.to_host(op.matvec(u))
+    assert y.dtype == g[f"matvec_u_{prec}"].dtype
+    assert rel_err(y, g[f"matvec_u_{prec}"]) < TOL[prec]
+    assert rel_err(be.to_host(op.matvec(g[f"wave_{prec}"])), g[f"matvec_wave_{prec}"]) < TOL[prec]
+    assert rel_err(be.to_host(op.rmatvec(u)), g[f"rmatvec_u_{prec}"]) < TOL[prec]
+    pk = e.PreparedEMKernel.build(grid, k=prob.k0, adjoint_storage="derived", build_strategy="streamed")
+    op_d = e.Operator(prob, prepared_kernel=pk)
+    assert rel_err(be.to_host(op_d.rmatvec(u)), g[f"rmatvec_u_derived_{prec}"]) < TOL[prec]
+
+
+@pytest.mark.parametrize("case", ["sphere16", "aniso12"])
+def test_fp32_path_against_reference_double(case):
+    """The FP32 operator against the reference complex128 result (north-star bar 1e-5)."""
+    import em3d_b200 as e
+
+    g = golden(f"em_{case}.npz")
+    N, L, k = tuple(int(v) for v in g["N"]), tuple(float(v) for v in g["L"]), float(g["k"])
+    be = _be("single")
+    grid = e.Grid(N=N, L=L, center=(0.0, 0.0, 0.0), backend=be)
+    prob = e.Problem(grid=grid, eps_tensor=g["chi_double"].astype(np.complex64),
+                     wave=g["wave_double"].astype(np.complex64), k0=k, volume=1.0)
+    op = e.Operator(prob)
+    y = be.to_host(op.matvec(g["u_double"].astype(np.complex64)))
+    assert rel_err(y, g["matvec_u_double"]) < 1e-5
+
+
+@pytest.mark.parametrize("tag", ["4x3x3", "4x3x2", "5x6x7"])
+@pytest.mark.parametrize("prec", ["double", "single"])
+def test_em_kernel_hat_full_matches_reference(tag, prec):
+    import em3d_b200 as e
+
+    g = golden(f"em_kernel_hat_{tag}.npz")
+    N, L, k = tuple(int(v) for v in g["N"]), tuple(float(v) for v in g["L"]), float(g["k"])
+    be = _be(prec)
+    grid = e.Grid(N=N, L=L, center=(0.0, 0.0, 0.0), backend=be)
+    pk = e.PreparedEMKernel.build(grid, k=k)
+    tol = 1e-12 if prec == "double" else 1e-5
+    assert rel_err(be.to_host(pk.kernel_hat), g[f"kernel_hat_{prec}"]) < tol
+    assert rel_err(be.to_host(pk.kernel_hat_adjoint), g[f"kernel_hat_adjoint_{prec}"]) < tol
+    assert pk.persistent_nbytes < g[f"kernel_hat_{prec}"].nbytes
+
+
+def test_batched_matvec_equals_single():
+    import torch
+    import em3d_b200 as e
+
+    g = golden("em_aniso12.npz")
+    be, grid, prob = _em_problem(g, "double")
+    op = e.Operator(prob)
+    rng = np.random.default_rng(0)
+    U = (rng.standard_normal((5, 3) + grid.N) + 1j * rng.standard_normal((5, 3) + grid.N)).astype(np.complex128)
+    Y = be.to_host(op.matvec(U))
+    for b in range(5):
+        assert rel_err(Y[b], be.to_host(op.matvec(U[b]))) < 1e-14
+    Ya = be.to_host(op.rmatvec(U))
+    assert rel_err(Ya[2], be.to_host(op.rmatvec(U[2]))) < 1e-14
+    del torch
+
+
+def test_adjoint_identity_em():
+    import em3d_b200 as e
+
+    g = golden("em_odd567.npz")
+    be, grid, prob = _em_problem(g, "double")
+    op = e.Operator(prob)
+    rng = np.random.default_rng(4)
+    u = rng.standard_normal((3,) + grid.N) + 1j * rng.standard_normal((3,) + grid.N)
+    v = rng.standard_normal((3,) + grid.N) + 1j * rng.standard_normal((3,) + grid.N)
+    left = np.vdot(be.to_host(op.matvec(u)), v)
+    right = np.vdot(u, be.to_host(op.rmatvec(v)))
+    assert abs(left - right) < 1e-12 * abs(left)
+
+
+def test_prepared_kernel_rejects_incompatible_wave_number():
+    import em3d_b200 as e
+
+    g = golden("em_cyl_lossy4.npz")
+    be, grid, prob = _em_problem(g, "double")
+    pk = e.PreparedEMKernel.build(grid, k=2.0)
+    with pytest.raises(ValueError, match="wave number"):
+        e.Operator(prob, prepared_kernel=pk)
+
+
+def test_forward_only_kernel_rejects_adjoint_action():
+    import em3d_b200 as e
+
+    g = golden("em_cyl_lossy4.npz")
+    be, grid, prob = _em_problem(g, "double")
+    pk = e.PreparedEMKernel.build(grid, k=prob.k0, include_adjoint=False, build_strategy="streamed")
+    op = e.Operator(prob, prepared_kernel=pk)
+    with pytest.raises(RuntimeError, match="adjoint action is unavailable"):
+        op.rmatvec(prob.wave)
+
+
+def test_em_matvec_against_oracle_random_sizes():
+    """Mixed-radix sizes the golden set does not cover, checked against the oracle live."""
+    import em3d_b200 as e
+    from oracle import em as oem
+
+    rng = np.random.default_rng(12)
+    for N, L, k in (((6, 10, 9), (1.1, 0.9, 1.0), 2.5), ((8, 12, 16), (1.0, 1.0, 1.0), 7.0),
+                    ((24, 20, 15), (1.0, 1.2, 0.8), 5.0)):
+        be = _be("double")
+        grid = e.Grid(N=N, L=L, center=(0.0, 0.0, 0.0), backend=be)
+        chi = (rng.standard_normal((3, 3) + N) + 1j * rng.standard_normal((3, 3) + N)) * 0.3
+        u = rng.standard_normal((3,) + N) + 1j * rng.standard_normal((3,) + N)
+        prob = e.Problem(grid=grid, eps_tensor=chi, wave=u, k0=k, volume=1.0)
+        op = e.Operator(prob)
+        kh = oem.kernel_hat(N, L, k)
+        assert rel_err(be.to_host(op.matvec(u)), oem.matvec(chi, u, kh, N)) < 1e-12
+        assert rel_err(be.to_host(op.rmatvec(u)), oem.rmatvec(chi, u, N, khat=kh)) < 1e-12
+
+
+@pytest.mark.parametrize("case", ["sphere332", "spheres16", "odd765"])
+@pytest.mark.parametrize("prec", ["double", "single"])
+def test_acoustic_matvec_rmatvec_match_reference(case, prec):
+    import em3d_b200 as e
+    from em3d_b200 import acoustics as ea
+
+    g = golden(f"ac_{case}.npz")
+    N, L, k0 = tuple(int(v) for v in g["N"]), tuple(float(v) for v in g["L"]), float(g["k0"])
+    be = _be(prec)
+    grid = e.Grid(N=N, L=L, center=(0.0, 0.0, 0.0), backend=be)
+    prob = ea.make_acoustic_problem(grid, g[f"eta_{prec}"], k0=k0)
+    assert rel_err(be.to_host(prob.wave), g[f"wave_{prec}"]) < (1e-15 if prec == "double" else 1e-7)
+    op = ea.AcousticOperator(prob)
+    u = g[f"u_{prec}"]
+    assert rel_err(be.to_host(op.matvec(u)), g[f"matvec_u_{prec}"]) < TOL[prec]
+    assert rel_err(be.to_host(op.rmatvec(u)), g[f"rmatvec_u_{prec}"]) < TOL[prec]
+
+
+def test_acoustic_identity_for_eta_one():
+    """Reference ``tests/test_acoustics_operator.py:257-263``."""
+    import torch
+    import em3d_b200 as e
+    from em3d_b200 import acoustics as ea
+
+    be = _be("double")
+    grid = e.Grid(N=(3, 2, 2), L=(1.0, 0.8, 0.6), center=(0.0, 0.0, 0.0), backend=be)
+    prob = ea.make_acoustic_problem(grid, ea.eta_homogeneous(grid, 1.0), k0=1.0)
+    op = ea.AcousticOperator(prob)
+    u = torch.ones(grid.N, dtype=torch.complex128, device="cuda") * (2.0 - 0.5j)
+    assert torch.allclose(op.matvec(u), u)
+    assert torch.allclose(op.rmatvec(u), u)
