@@ -406,8 +406,14 @@ static int grid_blocks(size_t n) {
   return (int)(b ? b : 1);
 }
 
+// Opt each kernel instantiation in to the full 227 KB of dynamic shared
+// memory once (the first launch happens outside any stream capture).
 template <typename K> static cudaError_t allow_smem(K kernel) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  static bool done = false;
+  if (done) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e == cudaSuccess) done = true;
+  return e;
 }
 
 static int check_grid(const em3d_grid* g, Dims* d) {

@@ -192,16 +192,15 @@ class _Applier:
         lead = tuple(x.shape[: x.dim() - len(fs)])
         return int(prod(lead)) if lead else 1
 
-    def apply_into(self, x, out, *, adjoint: bool = False, skip=None, stream=None):
+    def apply_into(self, x, out, *, adjoint: bool = False, skip_ptr=None, stream=None):
         """Write ``A x`` (or ``A* x``) into ``out`` without allocating.  ``x`` and
-        ``out`` are contiguous device tensors of the operator dtype; ``skip``
-        is an optional device int32 tensor (non-zero: kernels return at once)."""
+        ``out`` are contiguous device tensors of the operator dtype; ``skip_ptr``
+        is an optional device address of an int (non-zero: kernels return at once)."""
         b = self._batch_of(x)
         ws = self.workspace(b)
         name = self._native_names[1 if adjoint else 0]
         _lib.call(name, ctypes_ref(self._grid_c), self._dt, b, self._spectrum.data_ptr(), self._chi.data_ptr(),
-                  x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(),
-                  None if skip is None else skip.data_ptr(), _lib.stream_handle(stream))
+                  x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(), skip_ptr, _lib.stream_handle(stream))
         return out
 
 

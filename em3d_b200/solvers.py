@@ -1,0 +1,450 @@
+"""Device-resident BiCGStab, SIM and TwoStep with the reference's interface.
+
+Mirror of ``src/em3d/solvers/{base,bicgstab,sim,twostep}.py``: the same
+``SolverConfig`` / ``SolverResult`` fields, statuses, action counting and
+residual histories.  The iteration runs on the GPU: fused update kernels with
+FP64 inner products keep every scalar on the device and decide the stopping
+rules there (``em3d_b200/csrc/krylov.cu``); the host launches a chunk of
+iterations (replayed from a CUDA graph) and reads the status word once per
+chunk instead of synchronising on every reduction as the reference does.
+
+Additions over the reference (all optional, defaults keep its behaviour):
+``solve(operator, rhs, x0=None)`` accepts an initial guess, and
+``DefectCorrection`` runs FP32 inner solves inside an FP64 residual loop.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import c_double, c_int32, c_uint32
+from dataclasses import dataclass, field
+from typing import Any, List, Optional, Protocol
+
+import numpy as np
+
+from . import _lib
+
+STATUS_NAMES = {
+    0: "running", 1: "converged", 2: "max_iter", 3: "max_operator_actions", 4: "nonfinite",
+    5: "divergence_guard", 6: "breakdown_rho", 7: "breakdown_alpha", 8: "breakdown_omega",
+    9: "breakdown_t", 10: "breakdown_gradient",
+}
+
+
+@dataclass
+class SolverConfig:
+    """Same fields and defaults as the reference (``src/em3d/solvers/base.py:7-25``)."""
+
+    max_iter: int = 200
+    rtol: float = 1e-6
+    atol: float = 0.0
+    divergence_guard: float | None = None
+    max_operator_actions: int | None = None
+    log: bool = False
+    mu: Optional[complex] = None
+    radius: Optional[float] = None
+
+    def require_gamma(self) -> None:
+        if self.mu is None or self.radius is None:
+            raise ValueError("SolverConfig: mu and radius must be set (call gamma0.find_params)")
+        if abs(self.mu) == 0.0:
+            raise ValueError("SolverConfig: mu must be non-zero")
+
+
+@dataclass
+class SolverResult:
+    """Same fields as the reference (``src/em3d/solvers/base.py:28-44``)."""
+
+    u: Any
+    iterations: int
+    residual_history: List[float]
+    converged: bool
+    matvec_count: int = 0
+    rmatvec_count: int = 0
+    residual_action_counts: List[int] = field(default_factory=list)
+    status: str = "unknown"
+    true_final_residual: float | None = None
+
+    @property
+    def operator_action_count(self) -> int:
+        return int(self.matvec_count + self.rmatvec_count)
+
+
+class BaseSolver(Protocol):
+    def solve(self, operator, rhs) -> SolverResult: ...
+
+
+class KrylovState(ctypes.Structure):
+    """Host mirror of ``em3d_krylov_state`` (``include/em3d_b200.h``)."""
+
+    _fields_ = [
+        ("rhs_norm", c_double), ("tol", c_double), ("guard", c_double),
+        ("gamma_re", c_double), ("gamma_im", c_double),
+        ("rho_re", c_double), ("rho_im", c_double), ("rho_prev_re", c_double), ("rho_prev_im", c_double),
+        ("alpha_re", c_double), ("alpha_im", c_double), ("omega_re", c_double), ("omega_im", c_double),
+        ("t", c_double), ("h", c_double), ("last_rel", c_double), ("dots", c_double * 4),
+        ("status", c_int32), ("iter", c_int32), ("matvecs", c_int32), ("rmatvecs", c_int32),
+        ("max_iter", c_int32), ("max_actions", c_int32), ("hist_len", c_int32), ("hist_cap", c_int32),
+        ("pending", c_int32), ("first", c_int32), ("ticket", c_uint32), ("reserved", c_int32),
+    ]
+
+
+def _check_abi():
+    lib = _lib.load()
+    got = lib.em3d_krylov_state_size()
+    if got != ctypes.sizeof(KrylovState):
+        raise ImportError(f"em3d_krylov_state size mismatch: library {got}, binding {ctypes.sizeof(KrylovState)}")
+
+
+class DeviceState:
+    """One solver's state buffer on the device (struct + history + partials)."""
+
+    STATUS_OFFSET = KrylovState.status.offset
+
+    def __init__(self, device, hist_cap: int):
+        import torch
+
+        _check_abi()
+        lib = _lib.load()
+        self.cap = int(max(hist_cap, 2))
+        nbytes = lib.em3d_krylov_state_bytes(self.cap)
+        self.buf = torch.zeros(nbytes, dtype=torch.uint8, device=device)
+        self.hist_off = lib.em3d_krylov_history_offset(self.cap)
+        self.counts_off = lib.em3d_krylov_counts_offset(self.cap)
+        self.host = KrylovState()
+        self.host.hist_cap = self.cap
+        self._status_view = self.buf[self.STATUS_OFFSET:self.STATUS_OFFSET + 4].view(torch.int32)
+
+    @property
+    def ptr(self) -> int:
+        return self.buf.data_ptr()
+
+    @property
+    def status_ptr(self) -> int:
+        return self.buf.data_ptr() + self.STATUS_OFFSET
+
+    def upload(self, hist=(), counts=()):
+        import torch
+
+        self.host.hist_cap = self.cap
+        self.host.hist_len = len(hist)
+        raw = bytes(self.host)
+        self.buf[: len(raw)].copy_(torch.frombuffer(bytearray(raw), dtype=torch.uint8))
+        if len(hist):
+            h = np.asarray(hist, dtype=np.float64)
+            c = np.asarray(counts, dtype=np.int32)
+            self.buf[self.hist_off:self.hist_off + h.nbytes].copy_(torch.from_numpy(h.view(np.uint8)))
+            self.buf[self.counts_off:self.counts_off + c.nbytes].copy_(torch.from_numpy(c.view(np.uint8)))
+
+    def status(self) -> int:
+        return int(self._status_view.item())
+
+    def download(self):
+        head = self.buf[: ctypes.sizeof(KrylovState)].cpu().numpy().tobytes()
+        st = KrylovState.from_buffer_copy(head)
+        n = int(st.hist_len)
+        hist = self.buf[self.hist_off:self.hist_off + 8 * n].cpu().numpy().view(np.float64).tolist()
+        counts = self.buf[self.counts_off:self.counts_off + 4 * n].cpu().numpy().view(np.int32).tolist()
+        return st, hist, counts
+
+    def dots(self):
+        head = self.buf[: ctypes.sizeof(KrylovState)].cpu().numpy().tobytes()
+        st = KrylovState.from_buffer_copy(head)
+        return complex(st.dots[0], st.dots[1]), complex(st.dots[2], st.dots[3])
+
+
+def _native_dtype(t) -> int:
+    import torch
+
+    if t.dtype == torch.complex64:
+        return _lib.EM3D_C64
+    if t.dtype == torch.complex128:
+        return _lib.EM3D_C128
+    raise TypeError(f"solver vectors must be complex64 or complex128, got {t.dtype}")
+
+
+class _Engine:
+    """Vector plumbing shared by the three solvers."""
+
+    def __init__(self, operator, rhs, hist_cap):
+        import torch
+
+        self.op = operator
+        self.be = operator.backend
+        if not isinstance(rhs, torch.Tensor):
+            rhs = torch.as_tensor(np.asarray(rhs))
+        tc = self.be.precision.torch_complex if hasattr(self.be, "precision") else rhs.dtype
+        self.rhs = rhs.to(device=self.be.torch_device, dtype=tc).contiguous()
+        self.n = int(self.rhs.numel())
+        self.dt = _native_dtype(self.rhs)
+        self.state = DeviceState(self.rhs.device, hist_cap)
+        self.native_op = hasattr(operator, "apply_into")
+        self.lib = _lib.load()
+
+    def vec(self):
+        import torch
+
+        return torch.zeros_like(self.rhs)
+
+    def stream(self):
+        return _lib.stream_handle()
+
+    def apply(self, x, out, adjoint=False):
+        if self.native_op:
+            self.op.apply_into(x, out, adjoint=adjoint, skip_ptr=self.state.status_ptr)
+        else:
+            import torch
+
+            y = self.op.rmatvec(x) if adjoint else self.op.matvec(x)
+            out.copy_(torch.as_tensor(y, device=out.device).reshape(out.shape))
+
+    def norm(self, x) -> float:
+        _lib.call("em3d_vec_dots", self.dt, self.n, x.data_ptr(), x.data_ptr(), None, None, self.state.ptr,
+                  self.stream())
+        d0, _ = self.state.dots()
+        return float(np.sqrt(max(d0.real, 0.0)))
+
+    def step(self, name, *ptrs):
+        fn = getattr(self.lib, name)
+        status = fn(self.dt, ctypes.c_size_t(self.n), ctypes.c_void_p(self.state.ptr),
+                    *[ctypes.c_void_p(p) for p in ptrs], ctypes.c_void_p(self.stream()))
+        _lib.check(status, name)
+
+    def run(self, iteration, chunk: int, use_graph: bool):
+        """Launch ``iteration`` until the device status says stop.  With a native
+        operator the iterations are replayed ``chunk`` at a time from a CUDA graph."""
+        import torch
+
+        iteration()
+        if self.state.status() != 0:
+            return
+        graph = None
+        if use_graph and self.native_op:
+            try:
+                graph = torch.cuda.CUDAGraph()
+                side = torch.cuda.Stream(device=self.rhs.device)
+                side.wait_stream(torch.cuda.current_stream())
+                with torch.cuda.graph(graph, stream=side, capture_error_mode="thread_local"):
+                    for _ in range(chunk):
+                        iteration()
+                torch.cuda.current_stream().wait_stream(side)
+            except RuntimeError:
+                graph = None
+        while self.state.status() == 0:
+            if graph is not None:
+                graph.replay()
+            else:
+                for _ in range(chunk if self.native_op else 1):
+                    iteration()
+        if graph is not None:
+            torch.cuda.current_stream().synchronize()
+            del graph
+
+
+def _status_name(code: int) -> str:
+    return STATUS_NAMES.get(int(code), f"status_{code}")
+
+
+def _log(tag, history, counts, label="iter"):
+    for i, (r, c) in enumerate(zip(history, counts)):
+        print(f"[{tag}] {label}={i}, actions={c}, rel_res={r:.3e}")
+
+
+def _result(u, st, hist, counts, rmv=0) -> SolverResult:
+    status = _status_name(st.status)
+    return SolverResult(u=u, iterations=int(st.iter), residual_history=[float(h) for h in hist],
+                        converged=status == "converged", matvec_count=int(st.matvecs),
+                        rmatvec_count=int(st.rmatvecs), residual_action_counts=[int(c) for c in counts],
+                        status=status, true_final_residual=float(hist[-1]) if hist else float("inf"))
+
+
+def _trivial(rhs, x0=None) -> SolverResult:
+    import torch
+
+    u = torch.zeros_like(rhs) if x0 is None else x0.clone()
+    return SolverResult(u=u, iterations=0, residual_history=[0.0], converged=True, matvec_count=0,
+                        residual_action_counts=[0], status="converged", true_final_residual=0.0)
+
+
+def _guard(v):
+    return -1.0 if v is None else float(v)
+
+
+def _budget(v):
+    return -1 if v is None else int(v)
+
+
+def _init_u(eng, x0):
+    import torch
+
+    if x0 is None:
+        return eng.vec()
+    x = x0 if isinstance(x0, torch.Tensor) else torch.as_tensor(np.asarray(x0))
+    return x.to(device=eng.rhs.device, dtype=eng.rhs.dtype).reshape(eng.rhs.shape).clone()
+
+
+class BiCGStab:
+    """BiCGStab (reference ``src/em3d/solvers/bicgstab.py``), device resident."""
+
+    graph_chunk = 4
+
+    def __init__(self, config: SolverConfig):
+        self.cfg = config
+
+    def solve(self, operator, rhs, x0=None) -> SolverResult:
+        cfg = self.cfg
+        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2)
+        rhs = eng.rhs
+        rhs_norm = eng.norm(rhs)
+        if rhs_norm == 0.0:
+            return _trivial(rhs)
+        tol = max(float(cfg.rtol), float(cfg.atol) / rhs_norm)
+        u = _init_u(eng, x0)
+        r = eng.vec()
+        eng.apply(u, r)
+        _lib.call("em3d_vec_axpby", eng.dt, eng.n, r.data_ptr(), 1.0, 0.0, rhs.data_ptr(), -1.0, 0.0, r.data_ptr(),
+                  eng.stream())
+        rr = eng.norm(r)
+        rel0 = rr / rhs_norm
+        st = eng.state.host
+        st.rhs_norm, st.tol, st.guard = rhs_norm, tol, _guard(cfg.divergence_guard)
+        st.matvecs, st.rmatvecs, st.iter = 1, 0, 0
+        st.max_iter, st.max_actions = int(cfg.max_iter), _budget(cfg.max_operator_actions)
+        st.last_rel = rel0
+        early = None
+        if not np.isfinite(rel0):
+            early = 4
+        elif rel0 < tol:
+            early = 1
+        elif cfg.max_operator_actions is not None and 1 >= int(cfg.max_operator_actions):
+            early = 3
+        elif int(cfg.max_iter) <= 0:
+            early = 2
+        if early is not None:
+            st.status = early
+            return _result(u, st, [rel0], [1])
+        r_hat = r.clone()
+        p, v, s, t = eng.vec(), eng.vec(), eng.vec(), eng.vec()
+        st.rho_re, st.rho_im = rr * rr, 0.0
+        st.rho_prev_re, st.rho_prev_im = 1.0, 0.0
+        st.alpha_re, st.alpha_im = 1.0, 0.0
+        st.omega_re, st.omega_im = 1.0, 0.0
+        st.status, st.pending = 0, 0
+        eng.state.upload([rel0], [1])
+
+        def iteration():
+            eng.step("em3d_bicgstab_p", r.data_ptr(), p.data_ptr(), v.data_ptr())
+            eng.apply(p, v)
+            eng.step("em3d_bicgstab_alpha", r_hat.data_ptr(), v.data_ptr())
+            eng.step("em3d_bicgstab_s", r.data_ptr(), v.data_ptr(), s.data_ptr())
+            eng.apply(s, t)
+            eng.step("em3d_bicgstab_omega", t.data_ptr(), s.data_ptr())
+            eng.step("em3d_bicgstab_update", u.data_ptr(), p.data_ptr(), s.data_ptr(), t.data_ptr(), r.data_ptr(),
+                     r_hat.data_ptr())
+            eng.step("em3d_bicgstab_finalize", u.data_ptr(), p.data_ptr())
+
+        eng.run(iteration, self.graph_chunk, use_graph=True)
+        stf, hist, counts = eng.state.download()
+        if cfg.log:
+            _log("BiCGStab", hist, counts)
+        return _result(u, stf, hist, counts)
+
+
+class SIM:
+    """Simple iteration ``u <- u - gamma (A u - f)`` (reference ``src/em3d/solvers/sim.py``)."""
+
+    graph_chunk = 8
+
+    def __init__(self, config: SolverConfig):
+        config.require_gamma()
+        self.cfg = config
+
+    def solve(self, operator, rhs, x0=None) -> SolverResult:
+        cfg = self.cfg
+        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2)
+        rhs = eng.rhs
+        rhs_norm = eng.norm(rhs)
+        if rhs_norm == 0.0:
+            return _trivial(rhs)
+        gamma = 1.0 / complex(cfg.mu)
+        st = eng.state.host
+        st.rhs_norm = rhs_norm
+        st.tol = max(float(cfg.rtol), float(cfg.atol) / rhs_norm)
+        st.guard = _guard(cfg.divergence_guard)
+        st.gamma_re, st.gamma_im = gamma.real, gamma.imag
+        st.max_iter, st.max_actions = int(cfg.max_iter), _budget(cfg.max_operator_actions)
+        st.status = st.iter = st.matvecs = st.rmatvecs = 0
+        eng.state.upload()
+        u = _init_u(eng, x0)
+        res = eng.vec()
+
+        def iteration():
+            eng.apply(u, res)
+            eng.step("em3d_sim_residual", res.data_ptr(), rhs.data_ptr())
+            eng.step("em3d_sim_update", u.data_ptr(), res.data_ptr())
+
+        eng.run(iteration, self.graph_chunk, use_graph=True)
+        stf, hist, counts = eng.state.download()
+        if cfg.log:
+            _log("SIM", hist, counts, "updates")
+        return _result(u, stf, hist, counts)
+
+
+class TwoStep:
+    """Two-step minimal-residual gradient method (reference ``src/em3d/solvers/twostep.py``)."""
+
+    graph_chunk = 4
+
+    def __init__(self, config: SolverConfig):
+        self.cfg = config
+
+    def solve(self, operator, rhs, x0=None) -> SolverResult:
+        cfg = self.cfg
+        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2)
+        rhs = eng.rhs
+        rhs_norm = eng.norm(rhs)
+        if rhs_norm == 0.0:
+            return _trivial(rhs)
+        st = eng.state.host
+        st.rhs_norm = rhs_norm
+        st.tol = max(float(cfg.rtol), float(cfg.atol) / rhs_norm)
+        st.guard = _guard(cfg.divergence_guard)
+        st.max_iter, st.max_actions = int(cfg.max_iter), _budget(cfg.max_operator_actions)
+        st.status = st.iter = st.matvecs = st.rmatvecs = 0
+        st.first = 1
+        eng.state.upload()
+        u = _init_u(eng, x0)
+        up, r, rp, g, hg = eng.vec(), eng.vec(), eng.vec(), eng.vec(), eng.vec()
+
+        def iteration():
+            eng.apply(u, r)
+            eng.step("em3d_twostep_residual", r.data_ptr(), rhs.data_ptr())
+            eng.apply(r, g, adjoint=True)
+            eng.apply(g, hg)
+            eng.step("em3d_twostep_coeffs", r.data_ptr(), rp.data_ptr(), g.data_ptr(), hg.data_ptr())
+            eng.step("em3d_twostep_update", u.data_ptr(), up.data_ptr(), r.data_ptr(), rp.data_ptr(), g.data_ptr())
+
+        eng.run(iteration, self.graph_chunk, use_graph=True)
+        stf, hist, counts = eng.state.download()
+        if cfg.log:
+            _log("TwoStep", hist, counts, "updates")
+        return _result(u, stf, hist, counts)
+
+
+def true_relative_residual(operator, solution, rhs) -> float:
+    """``||A u - f|| / ||f||`` with FP64 norms (reference
+    ``src/em3d/experiments/stationary_validation.py:172-180``)."""
+    eng = _Engine(operator, rhs, hist_cap=2)
+    import torch
+
+    u = solution if isinstance(solution, torch.Tensor) else torch.as_tensor(np.asarray(solution))
+    u = u.to(device=eng.rhs.device, dtype=eng.rhs.dtype).reshape(eng.rhs.shape).contiguous()
+    rhs_norm = eng.norm(eng.rhs)
+    res = eng.vec()
+    if eng.native_op:
+        operator.apply_into(u, res)
+    else:
+        res.copy_(torch.as_tensor(operator.matvec(u)).reshape(res.shape))
+    _lib.call("em3d_vec_axpby", eng.dt, eng.n, res.data_ptr(), 1.0, 0.0, res.data_ptr(), -1.0, 0.0,
+              eng.rhs.data_ptr(), eng.stream())
+    rn = eng.norm(res)
+    return rn if rhs_norm == 0.0 else rn / rhs_norm

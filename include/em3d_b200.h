@@ -117,6 +117,102 @@ int em3d_acoustic_matvec(const em3d_grid* g, int dtype, int batch, const void* s
 int em3d_acoustic_rmatvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi,
                           const void* v, void* out, void* ws, size_t ws_bytes, const int* skip, void* stream);
 
+
+/* ------------------------------------------------------------------------
+ * Device-resident Krylov solvers
+ *
+ * The solver scalars, counters, status and residual history live in one
+ * device buffer (em3d_krylov_state followed by the history and the
+ * reduction partials; size from em3d_krylov_state_bytes).  Inner products
+ * and norms accumulate in FP64 whatever the vector dtype.  Every step kernel
+ * returns at once when status != 0, and the operator entry points take
+ * &state->status as their `skip` flag, so a sequence of iterations can be
+ * launched (or replayed from a CUDA graph) without host round trips; the host
+ * reads `status` once per chunk of iterations.
+ * ------------------------------------------------------------------------ */
+
+enum em3d_solver_status {
+  EM3D_RUNNING = 0,
+  EM3D_CONVERGED = 1,
+  EM3D_MAX_ITER = 2,
+  EM3D_MAX_OPERATOR_ACTIONS = 3,
+  EM3D_NONFINITE = 4,
+  EM3D_DIVERGENCE_GUARD = 5,
+  EM3D_BREAKDOWN_RHO = 6,
+  EM3D_BREAKDOWN_ALPHA = 7,
+  EM3D_BREAKDOWN_OMEGA = 8,
+  EM3D_BREAKDOWN_T = 9,
+  EM3D_BREAKDOWN_GRADIENT = 10,
+};
+
+typedef struct em3d_krylov_state {
+  double rhs_norm;             /* ||f||                                        */
+  double tol;                  /* max(rtol, atol / ||f||)                      */
+  double guard;                /* divergence guard; < 0 disables it            */
+  double gamma_re, gamma_im;   /* SIM step 1/mu                                */
+  double rho_re, rho_im, rho_prev_re, rho_prev_im;
+  double alpha_re, alpha_im, omega_re, omega_im;
+  double t, h;                 /* TwoStep step coefficients                    */
+  double last_rel;             /* last recorded relative residual              */
+  double dots[4];              /* output of em3d_vec_dots (re, im pairs)       */
+  int32_t status;              /* enum em3d_solver_status                      */
+  int32_t iter;                /* completed updates                            */
+  int32_t matvecs, rmatvecs;   /* operator actions so far                      */
+  int32_t max_iter;
+  int32_t max_actions;         /* < 0 disables the action budget               */
+  int32_t hist_len, hist_cap;  /* residual history entries used / capacity     */
+  int32_t pending;             /* BiCGStab: 1 = u += alpha p still to apply    */
+  int32_t first;               /* TwoStep: 1 before the first update           */
+  uint32_t ticket;             /* last-block counter of the reductions         */
+  int32_t reserved;
+} em3d_krylov_state;
+
+/* sizeof(em3d_krylov_state) as compiled into the library (ABI check). */
+size_t em3d_krylov_state_size(void);
+
+/* Bytes of the state buffer: the struct (padded to 256 B), the residual
+ * history (double[hist_cap]) and its action counts (int32[hist_cap]), and the
+ * reduction partials. */
+size_t em3d_krylov_state_bytes(int hist_cap);
+/* Offsets of the history arrays inside the state buffer. */
+size_t em3d_krylov_history_offset(int hist_cap);
+size_t em3d_krylov_counts_offset(int hist_cap);
+
+/* state->dots[0..1] = vdot(x0, y0); state->dots[2..3] = vdot(x1, y1) (when
+ * x1 != NULL); FP64 accumulation.  Replaces xp.vdot / xp.linalg.norm of the
+ * solvers (src/em3d/solvers/bicgstab.py:70,90). */
+int em3d_vec_dots(int dtype, size_t n, const void* x0, const void* y0, const void* x1, const void* y1,
+                  void* state, void* stream);
+/* out = a*x + b*y (scalars rounded to the vector dtype; y may be NULL). */
+int em3d_vec_axpby(int dtype, size_t n, void* out, double a_re, double a_im, const void* x, double b_re,
+                   double b_im, const void* y, void* stream);
+/* Precision conversion dst = src (complex64 <-> complex128), or, with
+ * accumulate = 1, dst += src. */
+int em3d_vec_convert(size_t n, int src_dtype, const void* src, int dst_dtype, void* dst, int accumulate,
+                     void* stream);
+
+/* BiCGStab (src/em3d/solvers/bicgstab.py:12-211), one iteration =
+ *   p -> [matvec v = A p] -> alpha -> s -> [matvec t = A s] -> omega -> update -> finalize */
+int em3d_bicgstab_p(int dtype, size_t n, void* state, const void* r, void* p, const void* v, void* stream);
+int em3d_bicgstab_alpha(int dtype, size_t n, void* state, const void* r_hat, const void* v, void* stream);
+int em3d_bicgstab_s(int dtype, size_t n, void* state, const void* r, const void* v, void* s, void* stream);
+int em3d_bicgstab_omega(int dtype, size_t n, void* state, const void* t, const void* s, void* stream);
+int em3d_bicgstab_update(int dtype, size_t n, void* state, void* u, const void* p, const void* s, const void* t,
+                         void* r, const void* r_hat, void* stream);
+int em3d_bicgstab_finalize(int dtype, size_t n, void* state, void* u, const void* p, void* stream);
+
+/* SIM (src/em3d/solvers/sim.py:13-91): [matvec res = A u] -> residual -> update */
+int em3d_sim_residual(int dtype, size_t n, void* state, void* res, const void* f, void* stream);
+int em3d_sim_update(int dtype, size_t n, void* state, void* u, const void* res, void* stream);
+
+/* TwoStep (src/em3d/solvers/twostep.py:16-139):
+ *   [matvec r = A u] -> residual -> [rmatvec g = A* r] -> [matvec hg = A g] -> coeffs -> update */
+int em3d_twostep_residual(int dtype, size_t n, void* state, void* r, const void* f, void* stream);
+int em3d_twostep_coeffs(int dtype, size_t n, void* state, const void* r, const void* r_prev, const void* g,
+                        const void* hg, void* stream);
+int em3d_twostep_update(int dtype, size_t n, void* state, void* u, void* u_prev, const void* r, void* r_prev,
+                        const void* g, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
