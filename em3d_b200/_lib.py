@@ -109,11 +109,25 @@ def check(status: int, what: str) -> None:
     raise NativeError(f"{what}: CUDA error: {msg}")
 
 
+# kernels each entry point launches (the operator passes count five)
+LAUNCHES = {
+    "em3d_em_matvec": 5, "em3d_em_rmatvec": 5, "em3d_acoustic_matvec": 5, "em3d_acoustic_rmatvec": 5,
+}
+launch_count = 0
+
+
+def count_launches(name: str) -> None:
+    global launch_count
+    if name.startswith("em3d_") and not name.endswith(("_bytes", "_offset", "_size", "_error", "_version")):
+        launch_count += LAUNCHES.get(name, 1)
+
+
 def call(name: str, *args) -> int:
     """Call ``name`` and raise on a non-zero status."""
     fn = getattr(load(), name)
     status = fn(*args)
     check(status, name)
+    count_launches(name)
     return status
 
 

@@ -150,6 +150,20 @@ class AcousticOperator(_Applier):
         x = self._as_field(v, "v")
         return self.apply_into(x, torch.empty_like(x), adjoint=True)
 
+    def with_precision(self, precision) -> "AcousticOperator":
+        """The same operator at another precision (FP32 twin for inner solves)."""
+        from .backend import Backend
+
+        if precision == self._be.precision:
+            return self
+        be = Backend.b200(precision, device_index=self._be.device_index)
+        g = self.problem.grid
+        grid = Grid(N=g.N, L=g.L, center=g.center, backend=be)
+        tc = precision.torch_complex
+        prob = AcousticProblem(grid=grid, eta=self.problem.eta.to(tc), wave=self.problem.wave.to(tc),
+                               k0=self.problem.k0, volume=self.problem.volume)
+        return AcousticOperator(prob)
+
     def kernel_hat(self, adjoint: bool = False):
         """Reference-layout spectrum ``fftn(K)`` (or ``fftn(conj K)``), (2Nx,2Ny,2Nz)."""
         import torch

@@ -14,7 +14,9 @@
 // the stored spectrum, and the spectrum is stored as one symmetric octant.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <unordered_set>
 
 #include "common.cuh"
 #include "fft.cuh"
@@ -406,13 +408,16 @@ static int grid_blocks(size_t n) {
   return (int)(b ? b : 1);
 }
 
-// Opt each kernel instantiation in to the full 227 KB of dynamic shared
-// memory once (the first launch happens outside any stream capture).
+// Opt each kernel in to the full 227 KB of dynamic shared memory once, keyed
+// by the kernel's address (its first launch happens outside any capture).
 template <typename K> static cudaError_t allow_smem(K kernel) {
-  static bool done = false;
-  if (done) return cudaSuccess;
+  static std::mutex mu;
+  static std::unordered_set<const void*> done;
+  const void* key = reinterpret_cast<const void*>(kernel);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(key)) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  if (e == cudaSuccess) done = true;
+  if (e == cudaSuccess) done.insert(key);
   return e;
 }
 

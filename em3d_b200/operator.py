@@ -245,6 +245,24 @@ class Operator(_Applier):
         out = torch.empty_like(x)
         return self.apply_into(x, out)
 
+    def with_precision(self, precision) -> "Operator":
+        """The same operator (grid, k0, contrast) at another precision: the
+        FP32 twin used for inner solves of a defect-correction loop.  Its
+        spectrum is rebuilt from the FP64 sampling and stored in ``precision``."""
+        from .backend import Backend
+        from .problem import Grid, Problem
+
+        if precision == self._be.precision:
+            return self
+        be = Backend.b200(precision, device_index=self._be.device_index)
+        g = self.problem.grid
+        grid = Grid(N=g.N, L=g.L, center=g.center, backend=be)
+        tc = precision.torch_complex
+        prob = Problem(grid=grid, eps_tensor=self.problem.eps_tensor.to(tc), wave=self.problem.wave.to(tc),
+                       k0=self.problem.k0, volume=self.problem.volume)
+        pk = PreparedEMKernel.build(grid, k=self.problem.k0, include_adjoint=self._prepared_kernel.supports_adjoint)
+        return Operator(prob, prepared_kernel=pk)
+
     def rmatvec(self, field):
         if not self._prepared_kernel.supports_adjoint:
             raise RuntimeError("adjoint action is unavailable: build PreparedEMKernel with include_adjoint=True")

@@ -208,6 +208,7 @@ class _Engine:
         status = fn(self.dt, ctypes.c_size_t(self.n), ctypes.c_void_p(self.state.ptr),
                     *[ctypes.c_void_p(p) for p in ptrs], ctypes.c_void_p(self.stream()))
         _lib.check(status, name)
+        _lib.count_launches(name)
 
     def run(self, iteration, chunk: int, use_graph: bool):
         """Launch ``iteration`` until the device status says stop.  With a native
@@ -218,7 +219,9 @@ class _Engine:
         if self.state.status() != 0:
             return
         graph = None
+        per_replay = 0
         if use_graph and self.native_op:
+            before = _lib.launch_count
             try:
                 graph = torch.cuda.CUDAGraph()
                 side = torch.cuda.Stream(device=self.rhs.device)
@@ -229,9 +232,12 @@ class _Engine:
                 torch.cuda.current_stream().wait_stream(side)
             except RuntimeError:
                 graph = None
+            per_replay = _lib.launch_count - before
+            _lib.launch_count = before  # captured, not launched
         while self.state.status() == 0:
             if graph is not None:
                 graph.replay()
+                _lib.launch_count += per_replay
             else:
                 for _ in range(chunk if self.native_op else 1):
                     iteration()
@@ -448,3 +454,107 @@ def true_relative_residual(operator, solution, rhs) -> float:
               eng.rhs.data_ptr(), eng.stream())
     rn = eng.norm(res)
     return rn if rhs_norm == 0.0 else rn / rhs_norm
+
+
+@dataclass
+class DefectCorrectionResult(SolverResult):
+    """``SolverResult`` of :class:`DefectCorrection`; the counts above add both
+    precisions, the fields below split them."""
+
+    outer_iterations: int = 0
+    inner_iterations: List[int] = field(default_factory=list)
+    fp64_matvecs: int = 0
+    fp32_matvecs: int = 0
+    fp32_rmatvecs: int = 0
+
+
+class DefectCorrection:
+    """FP64 defect correction around low-precision inner Krylov solves.
+
+    Each outer step forms the true residual ``r = f - A u`` with the FP64
+    operator and FP64 norms, solves ``A d = r`` with the FP32 twin of the
+    operator to a loose tolerance, and updates ``u += d`` in FP64.  The
+    outer relative residual is the stopping test, so the returned accuracy
+    is that of the FP64 operator.  ``residual_history`` holds the outer true
+    residuals.
+
+    ``inner_rtol`` is the FP32 solve's tolerance for the first correction;
+    later corrections only need to bring the remaining residual down to
+    ``rtol`` (with a safety factor), never looser than ``inner_rtol_max``.
+    """
+
+    def __init__(self, config: SolverConfig, *, inner: str = "bicgstab", inner_rtol: float = 1e-4,
+                 inner_rtol_max: float = 1e-2, inner_max_iter: int | None = None, max_outer: int = 20,
+                 safety: float = 0.3):
+        if inner not in ("bicgstab", "twostep"):
+            raise ValueError(f"inner must be 'bicgstab' or 'twostep', got {inner!r}")
+        self.cfg = config
+        self.inner = inner
+        self.inner_rtol = float(inner_rtol)
+        self.inner_rtol_max = float(inner_rtol_max)
+        self.inner_max_iter = inner_max_iter
+        self.max_outer = int(max_outer)
+        self.safety = float(safety)
+
+    def solve(self, operator, rhs, x0=None, *, operator_low=None) -> DefectCorrectionResult:
+        from .backend import Precision
+
+        cfg = self.cfg
+        op_lo = operator_low if operator_low is not None else operator.with_precision(Precision.SINGLE)
+        eng = _Engine(operator, rhs, hist_cap=4)
+        f = eng.rhs
+        fn = eng.norm(f)
+        if fn == 0.0:
+            base = _trivial(f)
+            return DefectCorrectionResult(**base.__dict__)
+        tol = max(float(cfg.rtol), float(cfg.atol) / fn)
+        u = _init_u(eng, x0)
+        r = eng.vec()
+        lo_dt = _lib.EM3D_C64
+        import torch
+
+        r_lo = torch.empty(f.shape, dtype=torch.complex64, device=f.device)
+        hist, counts = [], []
+        mv64 = mv32 = rmv32 = 0
+        inner_its = []
+        status = "max_iter"
+        inner_cls = BiCGStab if self.inner == "bicgstab" else TwoStep
+        budget_inner = int(self.inner_max_iter or cfg.max_iter)
+        for outer in range(self.max_outer + 1):
+            operator.apply_into(u, r)
+            mv64 += 1
+            _lib.call("em3d_vec_axpby", eng.dt, eng.n, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0, r.data_ptr(),
+                      eng.stream())
+            rel = eng.norm(r) / fn
+            hist.append(rel)
+            counts.append(mv64 + mv32 + rmv32)
+            if cfg.log:
+                print(f"[DefectCorrection] outer={outer}, actions={counts[-1]}, rel_res={rel:.3e}")
+            if not np.isfinite(rel):
+                status = "nonfinite"
+                break
+            if rel < tol:
+                status = "converged"
+                break
+            if cfg.divergence_guard is not None and rel > float(cfg.divergence_guard):
+                status = "divergence_guard"
+                break
+            if outer == self.max_outer:
+                status = "max_iter"
+                break
+            target = min(self.inner_rtol_max, max(self.inner_rtol, self.safety * tol / rel))
+            _lib.call("em3d_vec_convert", eng.n, eng.dt, r.data_ptr(), lo_dt, r_lo.data_ptr(), 0, eng.stream())
+            res = inner_cls(SolverConfig(max_iter=budget_inner, rtol=target)).solve(op_lo, r_lo)
+            mv32 += res.matvec_count
+            rmv32 += res.rmatvec_count
+            inner_its.append(res.iterations)
+            if res.status in ("nonfinite",):
+                status = "nonfinite"
+                break
+            d = res.u.contiguous()
+            _lib.call("em3d_vec_convert", eng.n, lo_dt, d.data_ptr(), eng.dt, u.data_ptr(), 1, eng.stream())
+        return DefectCorrectionResult(
+            u=u, iterations=sum(inner_its), residual_history=hist, converged=status == "converged",
+            matvec_count=mv64 + mv32, rmatvec_count=rmv32, residual_action_counts=counts, status=status,
+            true_final_residual=float(hist[-1]), outer_iterations=len(inner_its), inner_iterations=inner_its,
+            fp64_matvecs=mv64, fp32_matvecs=mv32, fp32_rmatvecs=rmv32)

@@ -1,0 +1,108 @@
+"""Seeded synthetic inputs of the benchmark configurations (host NumPy).
+
+Each builder returns plain arrays (contrast, incident wave, grid data) so that
+the same inputs can feed the B200 operator, the CPU oracle and the reference.
+
+* ``sphere_em``: dielectric sphere, README configuration (16^3, k0 = 4,
+  eps_r = 2, radius 0.25, +z, x-polarised).
+* ``aniso_ellipsoid_em``: absorbing anisotropic ellipsoid, radii
+  (0.30, 0.20, 0.25), eps = R diag(2.5+0.1i, 3.0+0.2i, 2.0+0.05i) R^T with R
+  a seeded uniform rotation, k0 = 12, +z, x-polarised (128^3 by default).
+* ``acoustic_spheres``: 200 non-overlapping spheres, radius U[0.02, 0.06],
+  eta U[1.2, 2.5] + i U[0, 0.1], k0 = 20 (256^3 by default).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import setup as _setup
+
+
+@dataclass
+class EMCase:
+    name: str
+    N: tuple
+    L: tuple
+    center: tuple
+    k0: float
+    chi: np.ndarray    # (3,3,Nx,Ny,Nz)
+    wave: np.ndarray   # (3,Nx,Ny,Nz)
+
+
+@dataclass
+class AcousticCase:
+    name: str
+    N: tuple
+    L: tuple
+    center: tuple
+    k0: float
+    eta: np.ndarray    # (Nx,Ny,Nz)
+
+
+def sphere_em(N: int = 16, precision: str = "double", k0: float = 4.0) -> EMCase:
+    cdt = _setup.complex_dtype_of(precision)
+    Ns, L, c = (N, N, N), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0)
+    axes = _setup.grid_axes_host(Ns, L, c, precision)
+    chi = _setup.sample_contrast_tensor(axes, L, background_eps_r=1.0, feature_eps_r=2.0,
+                                        geometry=_setup.Ellipsoid(c, (0.25, 0.25, 0.25)), dtype=cdt)
+    wave = _setup.flat_wave_vec_host(axes, k=k0, orient=(0, 0, 1), amplitude=(1, 0, 0), dtype=cdt)
+    return EMCase(f"em_sphere_{N}^3", Ns, L, c, k0, chi, wave)
+
+
+def rotation_matrix(seed: int = 0) -> np.ndarray:
+    """Uniform random SO(3) matrix (``scipy.spatial.transform.Rotation.random``)."""
+    from scipy.spatial.transform import Rotation
+
+    return Rotation.random(random_state=seed).as_matrix()
+
+
+def aniso_permittivity(seed: int = 0) -> np.ndarray:
+    R = rotation_matrix(seed)
+    return R @ np.diag([2.5 + 0.1j, 3.0 + 0.2j, 2.0 + 0.05j]) @ R.T
+
+
+def aniso_ellipsoid_em(N: int = 128, precision: str = "double", k0: float = 12.0, seed: int = 0,
+                       orient=(0.0, 0.0, 1.0), amplitude=(1.0, 0.0, 0.0)) -> EMCase:
+    cdt = _setup.complex_dtype_of(precision)
+    Ns, L, c = (N, N, N), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0)
+    axes = _setup.grid_axes_host(Ns, L, c, precision)
+    chi = _setup.sample_contrast_tensor(axes, L, background_eps_r=1.0, feature_eps_r=aniso_permittivity(seed),
+                                        geometry=_setup.Ellipsoid(c, (0.30, 0.20, 0.25)), dtype=cdt)
+    wave = _setup.flat_wave_vec_host(axes, k=k0, orient=orient, amplitude=amplitude, dtype=cdt)
+    return EMCase(f"em_aniso_ellipsoid_{N}^3", Ns, L, c, k0, chi, wave)
+
+
+def acoustic_spheres(N: int = 256, precision: str = "double", k0: float = 20.0, count: int = 200,
+                     seed: int = 0) -> AcousticCase:
+    """Rejection-sampled non-overlapping spheres with centres in [-0.5+r, 0.5-r]^3."""
+    cdt = _setup.complex_dtype_of(precision)
+    rng = np.random.default_rng(seed)
+    Ns, L, c = (N, N, N), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0)
+    axes = _setup.grid_axes_host(Ns, L, c, precision)
+    spheres = []
+    tries = 0
+    while len(spheres) < count:
+        tries += 1
+        if tries > 200000:
+            raise RuntimeError("could not place the spheres")
+        r = rng.uniform(0.02, 0.06)
+        ctr = rng.uniform(-0.5 + r, 0.5 - r, size=3)
+        if all(np.linalg.norm(ctr - c2) > r + r2 for c2, r2, _ in spheres):
+            val = rng.uniform(1.2, 2.5) + 1j * rng.uniform(0.0, 0.1)
+            spheres.append((ctr, r, val))
+    eta = np.ones(Ns, dtype=cdt)
+    ax = [np.asarray(a, dtype=np.float64) for a in axes]
+    for ctr, r, val in spheres:
+        # cell-centre test inside the sphere's bounding box only
+        sl = []
+        for d in range(3):
+            lo = int(np.searchsorted(ax[d], ctr[d] - r, side="left"))
+            hi = int(np.searchsorted(ax[d], ctr[d] + r, side="right"))
+            sl.append(slice(lo, hi))
+        X, Y, Z = np.meshgrid(ax[0][sl[0]], ax[1][sl[1]], ax[2][sl[2]], indexing="ij")
+        m = ((X - ctr[0]) ** 2 + (Y - ctr[1]) ** 2 + (Z - ctr[2]) ** 2) <= r * r
+        box = eta[sl[0], sl[1], sl[2]]
+        box[m] = cdt(val)
+    return AcousticCase(f"acoustic_{count}_spheres_{N}^3", Ns, L, c, k0, eta)
