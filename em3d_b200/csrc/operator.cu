@@ -13,6 +13,7 @@
 // inside the inverse passes, the 1/(8N) normalisation of ifftn is folded into
 // the stored spectrum, and the spectrum is stored as one symmetric octant.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -20,6 +21,7 @@
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "passes_fast.cuh"
 
 namespace {
 thread_local std::string g_last_error;
@@ -634,6 +636,100 @@ static int ac_kernel_hat_full(const em3d_grid* g, const Dims& d, double k0, int 
   return EM3D_OK;
 }
 
+// ---- register-FFT dispatch (power-of-two doubled axes 32..512) -----------
+
+static bool generic_forced() {
+  const char* v = getenv("EM3D_FFT_GENERIC");
+  return v && v[0] == '1';
+}
+
+static bool fast_len(int L) {
+  return !generic_forced() && (L == 32 || L == 64 || L == 128 || L == 256 || L == 512);
+}
+
+template <typename R, int L, int C, int LD, int ST, bool INV>
+static int go_rows(const cx<R>* in, const cx<R>* chi, const cx<R>* base, cx<R>* out, const cx<R>* tw, int rows_pb,
+                   int nrows, const int* skip, cudaStream_t st) {
+  using G = RowsGeom<L, FastE<R>::E, C>;
+  auto kern = kf_rows<R, L, C, LD, ST, INV>;
+  EM3D_CUDA_TRY(allow_smem(kern));
+  const size_t smem = (size_t)(L + C * G::RPB * G::PSTRIDE) * sizeof(cx<R>);
+  const int grid = (nrows + G::RPB - 1) / G::RPB;
+  kern<<<grid, G::NT, smem, st>>>(in, chi, base, out, tw, rows_pb, nrows, skip);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+template <typename R, int C, int LD, int ST, bool INV>
+static int launch_rows_fast(int L, const cx<R>* in, const cx<R>* chi, const cx<R>* base, cx<R>* out,
+                            const cx<R>* tw, int rows_pb, int nrows, const int* skip, cudaStream_t st) {
+  switch (L) {
+    case 32: return go_rows<R, 32, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
+    case 64: return go_rows<R, 64, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
+    case 128: return go_rows<R, 128, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
+    case 256: return go_rows<R, 256, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
+    case 512: return go_rows<R, 512, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
+  }
+  em3d_set_last_error("no register FFT for this length");
+  return EM3D_ERR_UNSUPPORTED;
+}
+
+template <typename R, int L, bool INV>
+static int go_strided(const cx<R>* in, cx<R>* out, const cx<R>* tw, int outer, int inner, const int* skip,
+                      cudaStream_t st) {
+  using G = StridedGeom<L, FastE<R>::E>;
+  auto kern = kf_strided<R, L, INV>;
+  EM3D_CUDA_TRY(allow_smem(kern));
+  const int ntiles = (inner + G::P - 1) / G::P;
+  const size_t smem = (size_t)(L + L * G::S) * sizeof(cx<R>);
+  const size_t grid = (size_t)outer * ntiles;
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(in, out, tw, inner, ntiles, skip);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+template <typename R, bool INV>
+static int launch_strided_fast(int L, const cx<R>* in, cx<R>* out, const cx<R>* tw, int outer, int inner,
+                               const int* skip, cudaStream_t st) {
+  switch (L) {
+    case 32: return go_strided<R, 32, INV>(in, out, tw, outer, inner, skip, st);
+    case 64: return go_strided<R, 64, INV>(in, out, tw, outer, inner, skip, st);
+    case 128: return go_strided<R, 128, INV>(in, out, tw, outer, inner, skip, st);
+    case 256: return go_strided<R, 256, INV>(in, out, tw, outer, inner, skip, st);
+    case 512: return go_strided<R, 512, INV>(in, out, tw, outer, inner, skip, st);
+  }
+  em3d_set_last_error("no register FFT for this length");
+  return EM3D_ERR_UNSUPPORTED;
+}
+
+template <typename R, int L, int C, bool ADJ>
+static int go_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
+                   cudaStream_t st) {
+  using G = XmulGeom<L, FastE<R>::E, C>;
+  auto kern = kf_xmul<R, L, C, ADJ>;
+  EM3D_CUDA_TRY(allow_smem(kern));
+  const int ntz = (2 * d.nz + G::P - 1) / G::P;
+  const size_t smem = (size_t)(L + G::REGIONS * L * G::S) * sizeof(cx<R>);
+  const size_t grid = (size_t)batch * 2 * d.ny * ntz;
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, skip);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+template <typename R, int C, bool ADJ>
+static int launch_xmul_fast(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
+                            const int* skip, cudaStream_t st) {
+  switch (2 * d.nx) {
+    case 32: return go_xmul<R, 32, C, ADJ>(T2, spec, tw, d, batch, skip, st);
+    case 64: return go_xmul<R, 64, C, ADJ>(T2, spec, tw, d, batch, skip, st);
+    case 128: return go_xmul<R, 128, C, ADJ>(T2, spec, tw, d, batch, skip, st);
+    case 256: return go_xmul<R, 256, C, ADJ>(T2, spec, tw, d, batch, skip, st);
+    case 512: return go_xmul<R, 512, C, ADJ>(T2, spec, tw, d, batch, skip, st);
+  }
+  em3d_set_last_error("no register FFT for this length");
+  return EM3D_ERR_UNSUPPORTED;
+}
+
 // The five passes of one application.
 template <typename R, int C, bool ADJ>
 static int apply(const Dims& d, int batch, const void* spectrum, const void* chi, const void* u, void* out, void* ws,
@@ -657,27 +753,40 @@ static int apply(const Dims& d, int batch, const void* spectrum, const void* chi
   const int rows = d.nx * d.ny;
   const int nrows = batch * rows;
   int rc;
-  // pass 1
-  if (!ADJ) {
-    if (C == 3) rc = launch_rows<R, C, LD_EM_CHI, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, 2 * d.nz, rows, nrows, d.nz, 2 * d.nz, skip, st);
-    else rc = launch_rows<R, C, LD_AC_CHI, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, 2 * d.nz, rows, nrows, d.nz, 2 * d.nz, skip, st);
+  const int Lz = 2 * d.nz, Ly = 2 * d.ny;
+  const bool fz = fast_len(Lz), fy = fast_len(Ly), fx = fast_len(2 * d.nx);
+  constexpr int LDF = C == 3 ? LD_EM_CHI : LD_AC_CHI;
+  constexpr int FLDF = C == 3 ? FLD_EM_CHI : FLD_AC_CHI;
+  constexpr int STA = C == 3 ? ST_EM_ADJ : ST_AC_ADJ;
+  constexpr int FSTA = C == 3 ? FST_EM_ADJ : FST_AC_ADJ;
+  // pass 1: rows along z, chi applied on load (matvec) or plain (rmatvec)
+  if (fz) {
+    if (!ADJ) rc = launch_rows_fast<R, C, FLDF, FST_PLAIN, false>(Lz, uu, ch, nullptr, T1, twz, rows, nrows, skip, st);
+    else rc = launch_rows_fast<R, C, FLD_PLAIN, FST_PLAIN, false>(Lz, uu, nullptr, nullptr, T1, twz, rows, nrows, skip, st);
   } else {
-    rc = launch_rows<R, C, LD_PLAIN, ST_PLAIN, false>(uu, nullptr, nullptr, T1, twz, 2 * d.nz, rows, nrows, d.nz, 2 * d.nz, skip, st);
+    if (!ADJ) rc = launch_rows<R, C, LDF, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st);
+    else rc = launch_rows<R, C, LD_PLAIN, ST_PLAIN, false>(uu, nullptr, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st);
   }
   if (rc) return rc;
   // pass 2: (batch*C*Nx, Ny, 2Nz) -> (batch*C*Nx, 2Ny, 2Nz)
-  if ((rc = launch_strided<R, false>(T1, T2, twy, 2 * d.ny, batch * C * d.nx, d.ny, 2 * d.ny, 2 * d.nz, skip, st))) return rc;
+  if (fy) rc = launch_strided_fast<R, false>(Ly, T1, T2, twy, batch * C * d.nx, Lz, skip, st);
+  else rc = launch_strided<R, false>(T1, T2, twy, Ly, batch * C * d.nx, d.ny, Ly, Lz, skip, st);
+  if (rc) return rc;
   // pass 3
-  if ((rc = launch_xmul<R, C, ADJ>(T2, oct, twx, d, batch, skip, st))) return rc;
+  if (fx) rc = launch_xmul_fast<R, C, ADJ>(T2, oct, twx, d, batch, skip, st);
+  else rc = launch_xmul<R, C, ADJ>(T2, oct, twx, d, batch, skip, st);
+  if (rc) return rc;
   // pass 4: (batch*C*Nx, 2Ny, 2Nz) -> (batch*C*Nx, Ny, 2Nz)
-  if ((rc = launch_strided<R, true>(T2, T1, twy, 2 * d.ny, batch * C * d.nx, 2 * d.ny, d.ny, 2 * d.nz, skip, st))) return rc;
-  // pass 5
-  if (!ADJ) {
-    rc = launch_rows<R, C, LD_PLAIN, ST_SUB, true>(T1, nullptr, uu, o, twz, 2 * d.nz, rows, nrows, 2 * d.nz, d.nz, skip, st);
-  } else if (C == 3) {
-    rc = launch_rows<R, C, LD_PLAIN, ST_EM_ADJ, true>(T1, ch, uu, o, twz, 2 * d.nz, rows, nrows, 2 * d.nz, d.nz, skip, st);
+  if (fy) rc = launch_strided_fast<R, true>(Ly, T2, T1, twy, batch * C * d.nx, Lz, skip, st);
+  else rc = launch_strided<R, true>(T2, T1, twy, Ly, batch * C * d.nx, Ly, d.ny, Lz, skip, st);
+  if (rc) return rc;
+  // pass 5: rows along z, crop and combine
+  if (fz) {
+    if (!ADJ) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_SUB, true>(Lz, T1, nullptr, uu, o, twz, rows, nrows, skip, st);
+    else rc = launch_rows_fast<R, C, FLD_PLAIN, FSTA, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st);
   } else {
-    rc = launch_rows<R, C, LD_PLAIN, ST_AC_ADJ, true>(T1, ch, uu, o, twz, 2 * d.nz, rows, nrows, 2 * d.nz, d.nz, skip, st);
+    if (!ADJ) rc = launch_rows<R, C, LD_PLAIN, ST_SUB, true>(T1, nullptr, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st);
+    else rc = launch_rows<R, C, LD_PLAIN, STA, true>(T1, ch, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st);
   }
   return rc;
 }

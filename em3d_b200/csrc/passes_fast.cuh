@@ -1,0 +1,341 @@
+// Operator passes on the register-resident FFT (power-of-two axes 32..512).
+// Same data layouts and fused work as the generic passes in operator.cu:
+//   kf_rows    pass 1 (z forward, chi applied on load) and pass 5 (z inverse,
+//              crop, u - y or v - chi^H y on store)
+//   kf_strided passes 2 and 4 (y forward with zero padding, y inverse with crop)
+//   kf_xmul    pass 3 (x forward, spectrum multiply in registers, x inverse, crop)
+#pragma once
+
+#include "fft_reg.cuh"
+
+namespace em3d {
+
+enum { FLD_PLAIN = 0, FLD_EM_CHI = 1, FLD_AC_CHI = 2 };
+enum { FST_PLAIN = 0, FST_SUB = 1, FST_EM_ADJ = 2, FST_AC_ADJ = 3 };
+
+template <typename R> struct FastE { static constexpr int E = sizeof(R) == 4 ? 16 : 8; };
+
+template <int L, int E, int C> struct RowsGeom {
+  static constexpr int TT = L / E;
+  static constexpr int RPB = (256 / (C * TT)) > 0 ? (256 / (C * TT)) : 1;
+  static constexpr int NT = C * RPB * TT;
+  static constexpr int PSTRIDE = rows_pencil_stride(L);
+};
+
+// Rows along z.  Forward (INV = false): input rows of length L/2 (pruned),
+// output rows of length L.  Inverse: input rows of length L, output the
+// first L/2 (crop).  One thread handles one (component, row) pencil slice.
+template <typename R, int L, int C, int LD, int ST, bool INV>
+__global__ void __launch_bounds__(RowsGeom<L, FastE<R>::E, C>::NT)
+kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>* out,
+        const cx<R>* __restrict__ twg, int rows_pb, int nrows, const int* skip) {
+  using T = cx<R>;
+  constexpr int E = FastE<R>::E;
+  using G = RowsGeom<L, E, C>;
+  using P = RegPlan<L, E>;
+  constexpr int TT = G::TT, RPB = G::RPB;
+  constexpr int R1 = P::first(false), RL = P::last(false);
+  constexpr int M1 = L / R1, ML = L / RL;
+  constexpr int LIN = INV ? L : L / 2;
+  constexpr int LOUT = INV ? L / 2 : L;
+  if (skip_launch(skip)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tw = reinterpret_cast<T*>(smem_raw);
+  T* sm = tw + L;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
+  const int t = threadIdx.x % TT;
+  const int pen = threadIdx.x / TT;
+  const int c = pen / RPB, rl = pen - c * RPB;
+  const int g = blockIdx.x * RPB + rl;
+  const bool valid = g < nrows;
+  const int b = valid ? g / rows_pb : 0;
+  const int row = valid ? g - b * rows_pb : 0;
+
+  T a[1][E];
+#pragma unroll
+  for (int q = 0; q < E / R1; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+      const int pos = j + r * M1;
+      T v = mk<R>(0, 0);
+      if (valid && (INV || r < R1 / 2)) {
+        if constexpr (LD == FLD_EM_CHI) {
+          const size_t o = (size_t)row * LIN + pos;
+          const size_t cs = (size_t)rows_pb * LIN;
+          const T* ub = in + (size_t)b * 3 * cs;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) v = cadd(v, cmul(chi[(size_t)(c * 3 + k) * cs + o], ub[k * cs + o]));
+        } else if constexpr (LD == FLD_AC_CHI) {
+          v = cmul(chi[(size_t)row * LIN + pos], in[((size_t)b * rows_pb + row) * LIN + pos]);
+        } else {
+          v = in[((size_t)(b * C + c) * rows_pb + row) * LIN + pos];
+        }
+      }
+      a[0][q * R1 + r] = v;
+    }
+  }
+  __syncthreads();
+  const LayRows lay{pen * G::PSTRIDE, G::PSTRIDE};
+  reg_fft<L, E, INV, false, 1>(a, t, sm, tw, lay);
+
+  if constexpr (ST == FST_EM_ADJ) {
+    // v - chi^H y needs all three components of y at each z: stage y through
+    // shared memory (the last exchange ended with a sync).
+#pragma unroll
+    for (int q = 0; q < E / RL; ++q) {
+      const int j = t + q * TT;
+#pragma unroll
+      for (int r = 0; r < RL / 2; ++r) sm[lay(0, j + r * ML)] = a[0][q * RL + r];
+    }
+    __syncthreads();
+    if (!valid) return;
+    const size_t cs = (size_t)rows_pb * LOUT;
+#pragma unroll
+    for (int q = 0; q < E / RL; ++q) {
+      const int j = t + q * TT;
+#pragma unroll
+      for (int r = 0; r < RL / 2; ++r) {
+        const int pos = j + r * ML;
+        const size_t o = (size_t)row * LOUT + pos;
+        T acc = mk<R>(0, 0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const T yk = sm[(k * RPB + rl) * G::PSTRIDE + pos + (pos >> 4)];
+          acc = cadd(acc, cmulcj(chi[(size_t)(k * 3 + c) * cs + o], yk));
+        }
+        const size_t oo = (size_t)(b * 3 + c) * cs + o;
+        out[oo] = csub(base[oo], acc);
+      }
+    }
+    return;
+  } else {
+    if (!valid) return;
+#pragma unroll
+    for (int q = 0; q < E / RL; ++q) {
+      const int j = t + q * TT;
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        if (INV && r >= RL / 2) continue;
+        const int pos = j + r * ML;
+        const T y = a[0][q * RL + r];
+        const size_t oo = ((size_t)(b * C + c) * rows_pb + row) * LOUT + pos;
+        if constexpr (ST == FST_PLAIN) out[oo] = y;
+        else if constexpr (ST == FST_SUB) out[oo] = csub(base[oo], y);
+        else if constexpr (ST == FST_AC_ADJ) out[oo] = csub(base[oo], cmulcj(chi[(size_t)row * LOUT + pos], y));
+      }
+    }
+  }
+}
+
+template <int L, int E> struct StridedGeom {
+  static constexpr int TT = L / E;
+  static constexpr int P = (256 / TT) >= 8 ? (256 / TT) : 8;
+  static constexpr int NT = P * TT;
+  static constexpr int S = (P & 1) ? P : P + 1;
+};
+
+// Pencils along y: in (outer, L/2 or L, inner) -> out (outer, L or L/2, inner).
+template <typename R, int L, bool INV>
+__global__ void __launch_bounds__(StridedGeom<L, FastE<R>::E>::NT)
+kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner, int ntiles, const int* skip) {
+  using T = cx<R>;
+  constexpr int E = FastE<R>::E;
+  using G = StridedGeom<L, E>;
+  using PL = RegPlan<L, E>;
+  constexpr int TT = G::TT, PP = G::P, S = G::S;
+  constexpr int R1 = PL::first(false), RL = PL::last(false);
+  constexpr int M1 = L / R1, ML = L / RL;
+  constexpr int LIN = INV ? L : L / 2;
+  constexpr int LOUT = INV ? L / 2 : L;
+  if (skip_launch(skip)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tw = reinterpret_cast<T*>(smem_raw);
+  T* sm = tw + L;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
+  const int p = threadIdx.x % PP, t = threadIdx.x / PP;
+  const int o = blockIdx.x / ntiles;
+  const int i = (blockIdx.x - o * ntiles) * PP + p;
+  const bool valid = i < inner;
+  const T* src = in + (size_t)o * LIN * inner + i;
+  T a[1][E];
+#pragma unroll
+  for (int q = 0; q < E / R1; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+      const int pos = j + r * M1;
+      a[0][q * R1 + r] = (valid && (INV || r < R1 / 2)) ? src[(size_t)pos * inner] : mk<R>(0, 0);
+    }
+  }
+  __syncthreads();
+  const LayInter lay{p, S, 0};
+  reg_fft<L, E, INV, false, 1>(a, t, sm, tw, lay);
+  if (!valid) return;
+  T* dst = out + (size_t)o * LOUT * inner + i;
+#pragma unroll
+  for (int q = 0; q < E / RL; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      if (INV && r >= RL / 2) continue;
+      dst[(size_t)(j + r * ML) * inner] = a[0][q * RL + r];
+    }
+  }
+}
+
+template <int L, int E, int C> struct XmulGeom {
+  static constexpr int TT = L / E;
+  static constexpr int P = (256 / TT) >= 4 ? (256 / TT) : 4;
+  static constexpr int NT = P * TT;
+  static constexpr int S = (P & 1) ? P : P + 1;
+  // FP64 exchanges one component at a time to keep shared memory small
+  static constexpr bool SEQ = (E == 8);
+  static constexpr int REGIONS = SEQ ? 1 : C;
+};
+
+template <int L, int E, int R, int NSV, int RN, int C, typename T>
+__device__ __forceinline__ void reg_exchange_seq(T (&a)[C][E], int t, T* sm, const LayInter& lay) {
+  constexpr int TT = L / E;
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+#pragma unroll
+    for (int q = 0; q < E / R; ++q) {
+      const int j = t + q * TT;
+      const int bse = (j / NSV) * NSV * R + (j % NSV);
+#pragma unroll
+      for (int r = 0; r < R; ++r) sm[lay(0, bse + r * NSV)] = a[c][q * R + r];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < E / RN; ++q) {
+      const int j = t + q * TT;
+#pragma unroll
+      for (int r = 0; r < RN; ++r) a[c][q * RN + r] = sm[lay(0, j + r * (L / RN))];
+    }
+    __syncthreads();
+  }
+}
+
+template <int L, int E, bool INV, bool REV, int S> struct RegFFTSeq {
+  template <int C, typename T>
+  __device__ __forceinline__ static void run(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const LayInter& lay) {
+    using P = RegPlan<L, E>;
+    constexpr int R = P::rad(REV, S);
+    constexpr int NSV = P::nsb(REV, S);
+    reg_stage<L, E, R, NSV, INV, C>(a, t, tw);
+    if constexpr (S + 1 < P::NS) {
+      constexpr int RN = P::rad(REV, S + 1);
+      reg_exchange_seq<L, E, R, NSV, RN, C>(a, t, sm, lay);
+      RegFFTSeq<L, E, INV, REV, S + 1>::template run<C>(a, t, sm, tw, lay);
+    }
+  }
+};
+
+template <int L, int E, bool INV, bool REV, bool SEQ, int C, typename T>
+__device__ __forceinline__ void reg_fft_x(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const LayInter& lay) {
+  if constexpr (SEQ) RegFFTSeq<L, E, INV, REV, 0>::template run<C>(a, t, sm, tw, lay);
+  else reg_fft<L, E, INV, REV, C>(a, t, sm, tw, lay);
+}
+
+__device__ __forceinline__ int kfold(int k, int n) { return k <= n ? k : 2 * n - k; }
+
+// Pencils along x for one (batch, ky, kz tile): forward FFT, spectrum multiply
+// in registers, reversed-plan inverse FFT, crop to x < Nx, in place in T2.
+template <typename R, int L, int C, bool ADJ>
+__global__ void __launch_bounds__(XmulGeom<L, FastE<R>::E, C>::NT)
+kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
+        const int* skip) {
+  using T = cx<R>;
+  constexpr int E = FastE<R>::E;
+  using G = XmulGeom<L, E, C>;
+  using PL = RegPlan<L, E>;
+  constexpr int TT = G::TT, PP = G::P, S = G::S;
+  constexpr int Nx = L / 2;
+  constexpr int R1 = PL::first(false), RL = PL::last(false);
+  constexpr int M1 = L / R1, ML = L / RL;
+  if (skip_launch(skip)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tw = reinterpret_cast<T*>(smem_raw);
+  T* sm = tw + L;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
+  const int p = threadIdx.x % PP, t = threadIdx.x / PP;
+  int idx = blockIdx.x;
+  const int tile = idx % ntz;
+  idx /= ntz;
+  const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
+  const int ky = idx % Ny2;
+  const int b = idx / Ny2;
+  const int kz = tile * PP + p;
+  const bool valid = kz < Nz2;
+  const size_t xstride = (size_t)Ny2 * Nz2;
+  T* col = T2 + (size_t)b * C * Nx * xstride + (size_t)ky * Nz2 + kz;
+
+  T a[C][E];
+#pragma unroll
+  for (int q = 0; q < E / R1; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+      const int x = j + r * M1;
+#pragma unroll
+      for (int c = 0; c < C; ++c)
+        a[c][q * R1 + r] = (valid && r < R1 / 2) ? col[((size_t)c * Nx + x) * xstride] : mk<R>(0, 0);
+    }
+  }
+  __syncthreads();
+  const LayInter lay{p, S, L * S};
+  reg_fft_x<L, E, false, false, G::SEQ, C>(a, t, sm, tw, lay);
+
+  // spectrum multiply on the forward outputs kx = j + r * ML
+  const int jy = kfold(ky, Ny);
+  const int l = kfold(valid ? kz : 0, Nz);
+  const size_t ostride = (size_t)(Nx + 1) * (Ny + 1) * (Nz + 1);
+  const T* sp = spec + (size_t)jy * (Nz + 1) + l;
+  const R sy = ky <= Ny ? (R)1 : (R)-1;
+  const R sz = kz <= Nz ? (R)1 : (R)-1;
+#pragma unroll
+  for (int q = 0; q < E / RL; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      const int kx = j + r * ML;
+      const int ix = kfold(kx, Nx);
+      const T* s0 = sp + (size_t)ix * (Ny + 1) * (Nz + 1);
+      const int e = q * RL + r;
+      if constexpr (C == 1) {
+        const T k0 = valid ? s0[0] : mk<R>(0, 0);
+        a[0][e] = ADJ ? cmulcj(k0, a[0][e]) : cmul(k0, a[0][e]);
+      } else {
+        const R sx = kx <= Nx ? (R)1 : (R)-1;
+        T kxx = mk<R>(0, 0), kyy = kxx, kzz = kxx, kxy = kxx, kxz = kxx, kyz = kxx;
+        if (valid) {
+          kxx = s0[0]; kyy = s0[ostride]; kzz = s0[2 * ostride];
+          kxy = cscale(s0[3 * ostride], sx * sy);
+          kxz = cscale(s0[4 * ostride], sx * sz);
+          kyz = cscale(s0[5 * ostride], sy * sz);
+        }
+        if (ADJ) { kxx = cconj(kxx); kyy = cconj(kyy); kzz = cconj(kzz); kxy = cconj(kxy); kxz = cconj(kxz); kyz = cconj(kyz); }
+        const T X0 = a[0][e], X1 = a[1][e], X2 = a[2][e];
+        a[0][e] = cadd(cadd(cmul(kxx, X0), cmul(kxy, X1)), cmul(kxz, X2));
+        a[1][e] = cadd(cadd(cmul(kxy, X0), cmul(kyy, X1)), cmul(kyz, X2));
+        a[2][e] = cadd(cadd(cmul(kxz, X0), cmul(kyz, X1)), cmul(kzz, X2));
+      }
+    }
+  }
+  reg_fft_x<L, E, true, true, G::SEQ, C>(a, t, sm, tw, lay);
+  if (!valid) return;
+  // reversed plan: last inverse stage has radix R1, outputs x = j + r * M1
+#pragma unroll
+  for (int q = 0; q < E / R1; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < R1 / 2; ++r) {
+      const int x = j + r * M1;
+#pragma unroll
+      for (int c = 0; c < C; ++c) col[((size_t)c * Nx + x) * xstride] = a[c][q * R1 + r];
+    }
+  }
+}
+
+}  // namespace em3d

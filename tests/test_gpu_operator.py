@@ -185,3 +185,57 @@ def test_acoustic_identity_for_eta_one():
     u = torch.ones(grid.N, dtype=torch.complex128, device="cuda") * (2.0 - 0.5j)
     assert torch.allclose(op.matvec(u), u)
     assert torch.allclose(op.rmatvec(u), u)
+
+
+@pytest.mark.parametrize("prec", ["double", "single"])
+@pytest.mark.parametrize("kind", ["em", "acoustic"])
+def test_register_fft_path_matches_generic_path(prec, kind, monkeypatch):
+    """The register-resident FFT passes (power-of-two doubled axes) against the
+    generic shared-memory Stockham passes on the same inputs."""
+    import torch
+    import em3d_b200 as e
+    from em3d_b200 import acoustics as ea
+
+    be = _be(prec)
+    rng = np.random.default_rng(3)
+    tol = 1e-13 if prec == "double" else 3e-6
+    for N in ((32, 16, 64), (64, 64, 64), (128, 128, 128)) if kind == "em" else ((32, 64, 16), (128, 128, 128), (256, 128, 64)):
+        grid = e.Grid(N=N, L=(1.0, 0.9, 1.1), center=(0.0, 0.0, 0.0), backend=be)
+        tc = be.precision.torch_complex
+        if kind == "em":
+            chi = (torch.randn((3, 3) + N, dtype=tc, device="cuda") * 0.3).contiguous()
+            u = torch.randn((3,) + N, dtype=tc, device="cuda")
+            op = e.Operator(e.Problem(grid=grid, eps_tensor=chi, wave=u, k0=7.0, volume=1.0))
+        else:
+            eta = (1.0 + torch.rand(N, dtype=tc, device="cuda")).contiguous()
+            op = ea.AcousticOperator(ea.make_acoustic_problem(grid, eta, k0=9.0))
+            u = torch.randn(N, dtype=tc, device="cuda")
+        fast_mv, fast_rmv = op.matvec(u), op.rmatvec(u)
+        monkeypatch.setenv("EM3D_FFT_GENERIC", "1")
+        gen_mv, gen_rmv = op.matvec(u), op.rmatvec(u)
+        monkeypatch.delenv("EM3D_FFT_GENERIC")
+        assert rel_err(be.to_host(fast_mv), be.to_host(gen_mv)) < tol, N
+        assert rel_err(be.to_host(fast_rmv), be.to_host(gen_rmv)) < tol, N
+    del rng
+
+
+def test_em_matvec_oracle_at_32_cubed_both_paths(monkeypatch):
+    """Register path and generic path both against the oracle (FP64, 1e-12)."""
+    import em3d_b200 as e
+    from oracle import em as oem
+
+    g = golden("em_aniso12.npz")
+    N, L, k = (32, 32, 32), (1.0, 1.0, 1.0), 12.0
+    rng = np.random.default_rng(8)
+    chi = (rng.standard_normal((3, 3) + N) + 1j * rng.standard_normal((3, 3) + N)) * 0.2
+    u = rng.standard_normal((3,) + N) + 1j * rng.standard_normal((3,) + N)
+    be = _be("double")
+    grid = e.Grid(N=N, L=L, center=(0.0, 0.0, 0.0), backend=be)
+    op = e.Operator(e.Problem(grid=grid, eps_tensor=chi, wave=u, k0=k, volume=1.0))
+    kh = oem.kernel_hat(N, L, k)
+    ref, ref_a = oem.matvec(chi, u, kh, N), oem.rmatvec(chi, u, N, khat=kh)
+    for generic in ("0", "1"):
+        monkeypatch.setenv("EM3D_FFT_GENERIC", generic)
+        assert rel_err(be.to_host(op.matvec(u)), ref) < 1e-12
+        assert rel_err(be.to_host(op.rmatvec(u)), ref_a) < 1e-12
+    del g
