@@ -52,6 +52,9 @@ SIGNATURES = {
                                      c_size_t, c_void_p, c_void_p]),
     "em3d_acoustic_rmatvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                       c_size_t, c_void_p, c_void_p]),
+    "em3d_em_matvec_static_scratch": (c_int, [_GRID, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                              c_void_p]),
+    "em3d_static_scratch_bytes": (c_size_t, []),
     "em3d_krylov_state_size": (c_size_t, []),
     "em3d_krylov_state_bytes": (c_size_t, [c_int]),
     "em3d_krylov_history_offset": (c_size_t, [c_int]),

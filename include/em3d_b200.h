@@ -110,6 +110,20 @@ int em3d_em_matvec(const em3d_grid* g, int dtype, int batch, const void* spectru
 int em3d_em_rmatvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi,
                     const void* v, void* out, void* ws, size_t ws_bytes, const int* skip, void* stream);
 
+/* EM matvec for callers that cannot allocate device memory (no counterpart
+ * in the reference).  Same result as em3d_em_matvec with batch = 1, but the
+ * workspace is a fixed 64 MiB device array inside the library (held on every
+ * GPU that uses the library until the process exits), so the caller passes
+ * only inputs and outputs.  Grids whose workspace exceeds 64 MiB are rejected
+ * with EM3D_ERR_INVALID (about 466k cells in complex64, 233k in complex128).
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller. */
+int em3d_em_matvec_static_scratch(const em3d_grid* g, int dtype, const void* spectrum, const void* chi,
+                                  const void* u, void* out, const int* skip, void* stream);
+/* Size of that fixed workspace in bytes. */
+size_t em3d_static_scratch_bytes(void);
+
 /* Scalar versions.  Replace AcousticOperator.matvec / rmatvec
  * (src/em3d/acoustics/operator.py:40-67). */
 int em3d_acoustic_matvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi,
