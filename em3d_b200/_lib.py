@@ -21,6 +21,8 @@ EM3D_C64 = 0
 EM3D_C128 = 1
 EM3D_ACOUSTIC = 1
 EM3D_EM = 3
+EM3D_TUNE_XPASS_VARIANT = 0
+EM3D_TUNE_FFT_GENERIC = 1
 
 
 class EmGrid(ctypes.Structure):
@@ -55,6 +57,8 @@ SIGNATURES = {
     "em3d_em_matvec_static_scratch": (c_int, [_GRID, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                               c_void_p]),
     "em3d_static_scratch_bytes": (c_size_t, []),
+    "em3d_set_tuning": (c_int, [c_int, c_int]),
+    "em3d_get_tuning": (c_int, [c_int]),
     "em3d_krylov_state_size": (c_size_t, []),
     "em3d_krylov_state_bytes": (c_size_t, [c_int]),
     "em3d_krylov_history_offset": (c_size_t, [c_int]),
@@ -121,7 +125,8 @@ launch_count = 0
 
 def count_launches(name: str) -> None:
     global launch_count
-    if name.startswith("em3d_") and not name.endswith(("_bytes", "_offset", "_size", "_error", "_version")):
+    if name.startswith("em3d_") and not name.endswith(("_bytes", "_offset", "_size", "_error", "_version",
+                                                       "_tuning")):
         launch_count += LAUNCHES.get(name, 1)
 
 

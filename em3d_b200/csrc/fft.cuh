@@ -101,11 +101,58 @@ template <bool INV, typename C> __device__ __forceinline__ void dft16(C* a) {
   const R sn[8] = {(R)0, s1, h, c1, (R)1, c1, h, s1};
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
-    // w16^q = cos(2 pi q/16) -+ i sin(2 pi q/16)
-    C w = mk<R>(cs[q], INV ? sn[q] : -sn[q]);
-    C t = cmul(o[q], w);
+    // w16^q = cos(2 pi q/16) -+ i sin(2 pi q/16); q = 0 and q = 4 are exact
+    C t;
+    if (q == 0) t = o[0];
+    else if (q == 4) t = rot_q<INV>(o[4]);
+    else t = cmul(o[q], mk<R>(cs[q], INV ? sn[q] : -sn[q]));
     a[q] = cadd(e[q], t);
     a[q + 8] = csub(e[q], t);
+  }
+}
+
+// DFTs of length R whose inputs a[R/2 .. R-1] are zero (the zero-padded half
+// of a forward transform):  y[2m] = DFT_{R/2}(a)[m],
+// y[2m+1] = DFT_{R/2}(a[r] w_R^r)[m].  Only a[0 .. R/2-1] are read.
+template <int RX, bool INV, typename C> __device__ __forceinline__ void dft_fixed_half_in(C* a) {
+  using R = decltype(a[0].x);
+  if constexpr (RX == 2) {
+    a[1] = a[0];
+  } else if constexpr (RX == 4) {
+    C a0 = a[0], a1 = a[1];
+    C w1 = rot_q<INV>(a1);
+    a[0] = cadd(a0, a1); a[2] = cadd(a0, w1); a[1] = csub(a0, a1); a[3] = csub(a0, w1);
+    // natural order: y0 = E0, y1 = O0, y2 = E1, y3 = O1
+    C y0 = a[0], y1 = a[2], y2 = a[1], y3 = a[3];
+    a[0] = y0; a[1] = y1; a[2] = y2; a[3] = y3;
+  } else if constexpr (RX == 8) {
+    const R h = (R)0.70710678118654752440;
+    C e0 = a[0], e1 = a[1], e2 = a[2], e3 = a[3];
+    // odd half: a[r] * w8^r
+    C o0 = a[0];
+    C o1 = INV ? mk<R>(h * (a[1].x - a[1].y), h * (a[1].y + a[1].x)) : mk<R>(h * (a[1].x + a[1].y), h * (a[1].y - a[1].x));
+    C o2 = rot_q<INV>(a[2]);
+    C o3 = INV ? mk<R>(-h * (a[3].x + a[3].y), h * (a[3].x - a[3].y)) : mk<R>(h * (a[3].y - a[3].x), -h * (a[3].x + a[3].y));
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
+    a[0] = e0; a[1] = o0; a[2] = e1; a[3] = o1; a[4] = e2; a[5] = o2; a[6] = e3; a[7] = o3;
+  } else if constexpr (RX == 16) {
+    const R c1 = (R)0.92387953251128675613, s1 = (R)0.38268343236508977173;
+    const R h = (R)0.70710678118654752440;
+    const R cs[8] = {(R)1, c1, h, s1, (R)0, -s1, -h, -c1};
+    const R sn[8] = {(R)0, s1, h, c1, (R)1, c1, h, s1};
+    C e[8], o[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      e[r] = a[r];
+      if (r == 0) o[r] = a[0];
+      else if (r == 4) o[r] = rot_q<INV>(a[4]);
+      else o[r] = cmul(a[r], mk<R>(cs[r], INV ? sn[r] : -sn[r]));
+    }
+    dft8<INV>(e);
+    dft8<INV>(o);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) { a[2 * m] = e[m]; a[2 * m + 1] = o[m]; }
   }
 }
 

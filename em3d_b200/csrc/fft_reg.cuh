@@ -43,7 +43,7 @@ template <int L, int E> struct RegPlan {
 
 // Twiddle-multiply and DFT of this thread's butterflies in one stage, for C
 // pencils held as a[c][E] (register index q*R + r).
-template <int L, int E, int R, int NSV, bool INV, int C, typename T>
+template <int L, int E, int R, int NSV, bool INV, int C, bool HALF_IN = false, typename T>
 __device__ __forceinline__ void reg_stage(T (&a)[C][E], int t, const T* __restrict__ tw) {
   constexpr int TT = L / E;
   constexpr int Q = E / R;
@@ -62,7 +62,8 @@ __device__ __forceinline__ void reg_stage(T (&a)[C][E], int t, const T* __restri
           b[r] = INV ? cmulcj(w, b[r]) : cmul(w, b[r]);
         }
       }
-      dft_fixed<R, INV>(b);
+      if constexpr (HALF_IN) dft_fixed_half_in<R, INV>(b);
+      else dft_fixed<R, INV>(b);
     }
   }
 }
@@ -93,26 +94,27 @@ __device__ __forceinline__ void reg_exchange(T (&a)[C][E], int t, T* sm, const L
   __syncthreads();
 }
 
-template <int L, int E, bool INV, bool REV, int S> struct RegFFT {
+template <int L, int E, bool INV, bool REV, int S, bool HALF_IN> struct RegFFT {
   template <int C, typename T, class Lay>
   __device__ __forceinline__ static void run(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const Lay& lay) {
     using P = RegPlan<L, E>;
     constexpr int R = P::rad(REV, S);
     constexpr int NSV = P::nsb(REV, S);
-    reg_stage<L, E, R, NSV, INV, C>(a, t, tw);
+    reg_stage<L, E, R, NSV, INV, C, HALF_IN && S == 0>(a, t, tw);
     if constexpr (S + 1 < P::NS) {
       constexpr int RN = P::rad(REV, S + 1);
       reg_exchange<L, E, R, NSV, RN, C>(a, t, sm, lay);
-      RegFFT<L, E, INV, REV, S + 1>::template run<C>(a, t, sm, tw, lay);
+      RegFFT<L, E, INV, REV, S + 1, HALF_IN>::template run<C>(a, t, sm, tw, lay);
     }
   }
 };
 
 // Full transform of C pencils in registers: inputs in first-stage order,
-// outputs in last-stage order (see the header comment).
-template <int L, int E, bool INV, bool REV, int C, typename T, class Lay>
+// outputs in last-stage order (see the header comment).  HALF_IN: the
+// first-stage inputs with r >= R/2 are zero padding and are not read.
+template <int L, int E, bool INV, bool REV, int C, bool HALF_IN = false, typename T, class Lay>
 __device__ __forceinline__ void reg_fft(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const Lay& lay) {
-  RegFFT<L, E, INV, REV, 0>::template run<C>(a, t, sm, tw, lay);
+  RegFFT<L, E, INV, REV, 0, HALF_IN>::template run<C>(a, t, sm, tw, lay);
 }
 
 // Shared-memory layouts.

@@ -638,9 +638,13 @@ static int ac_kernel_hat_full(const em3d_grid* g, const Dims& d, double k0, int 
 
 // ---- register-FFT dispatch (power-of-two doubled axes 32..512) -----------
 
+// Tuning knobs (em3d_set_tuning / em3d_get_tuning).  They select among
+// equivalent implementations; results do not depend on them beyond rounding.
+static int g_tuning[EM3D_TUNE_COUNT] = {0, 0};
+
 static bool generic_forced() {
   const char* v = getenv("EM3D_FFT_GENERIC");
-  return v && v[0] == '1';
+  return g_tuning[EM3D_TUNE_FFT_GENERIC] != 0 || (v && v[0] == '1');
 }
 
 static bool fast_len(int L) {
@@ -702,11 +706,11 @@ static int launch_strided_fast(int L, const cx<R>* in, cx<R>* out, const cx<R>* 
   return EM3D_ERR_UNSUPPORTED;
 }
 
-template <typename R, int L, int C, bool ADJ>
+template <typename R, int L, int C, bool ADJ, int E, int NTT = 256>
 static int go_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
                    cudaStream_t st) {
-  using G = XmulGeom<L, FastE<R>::E, C>;
-  auto kern = kf_xmul<R, L, C, ADJ>;
+  using G = XmulGeom<L, E, C, NTT>;
+  auto kern = kf_xmul<R, L, C, ADJ, E, NTT>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const int ntz = (2 * d.nz + G::P - 1) / G::P;
   const size_t smem = (size_t)(L + G::REGIONS * L * G::S) * sizeof(cx<R>);
@@ -716,19 +720,51 @@ static int go_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d,
   return EM3D_OK;
 }
 
+template <typename R, int L, bool ADJ, int E>
+static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
+                     cudaStream_t st) {
+  using G = XsplitGeom<L, E>;
+  auto kern = kf_xmul_split<R, L, ADJ, E>;
+  EM3D_CUDA_TRY(allow_smem(kern));
+  const int ntz = (2 * d.nz + G::PZ - 1) / G::PZ;
+  const size_t smem = (size_t)(L + 3 * G::REGION) * sizeof(cx<R>);
+  const size_t grid = (size_t)batch * 2 * d.ny * ntz;
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, skip);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+// x-pass variant (tuning key EM3D_TUNE_XPASS_VARIANT): 0 = three components
+// in registers, 256-thread CTAs; 1 = the same with 128-thread CTAs (two per
+// SM); 2 = component-split threads (EM only).
+static int xmul_variant() { return g_tuning[EM3D_TUNE_XPASS_VARIANT]; }
+
+template <typename R, int C, bool ADJ, int L>
+static int launch_xmul_len(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
+                           const int* skip, cudaStream_t st) {
+  constexpr int EB = FastE<R>::E;
+  const int v = xmul_variant();
+  if constexpr (C == 3) {
+    if (v == 2) return go_xsplit<R, L, ADJ, EB>(T2, spec, tw, d, batch, skip, st);
+  }
+  if (v == 1) return go_xmul<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st);
+  return go_xmul<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st);
+}
+
 template <typename R, int C, bool ADJ>
 static int launch_xmul_fast(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
                             const int* skip, cudaStream_t st) {
   switch (2 * d.nx) {
-    case 32: return go_xmul<R, 32, C, ADJ>(T2, spec, tw, d, batch, skip, st);
-    case 64: return go_xmul<R, 64, C, ADJ>(T2, spec, tw, d, batch, skip, st);
-    case 128: return go_xmul<R, 128, C, ADJ>(T2, spec, tw, d, batch, skip, st);
-    case 256: return go_xmul<R, 256, C, ADJ>(T2, spec, tw, d, batch, skip, st);
-    case 512: return go_xmul<R, 512, C, ADJ>(T2, spec, tw, d, batch, skip, st);
+    case 32: return launch_xmul_len<R, C, ADJ, 32>(T2, spec, tw, d, batch, skip, st);
+    case 64: return launch_xmul_len<R, C, ADJ, 64>(T2, spec, tw, d, batch, skip, st);
+    case 128: return launch_xmul_len<R, C, ADJ, 128>(T2, spec, tw, d, batch, skip, st);
+    case 256: return launch_xmul_len<R, C, ADJ, 256>(T2, spec, tw, d, batch, skip, st);
+    case 512: return launch_xmul_len<R, C, ADJ, 512>(T2, spec, tw, d, batch, skip, st);
   }
   em3d_set_last_error("no register FFT for this length");
   return EM3D_ERR_UNSUPPORTED;
 }
+
 
 // The five passes of one application.
 template <typename R, int C, bool ADJ>
@@ -809,6 +845,18 @@ static int apply_dispatch(const em3d_grid* g, int dtype, int batch, const void* 
 using namespace em3d;
 
 extern "C" {
+
+int em3d_set_tuning(int key, int value) {
+  if (key < 0 || key >= EM3D_TUNE_COUNT) { em3d_set_last_error("unknown tuning key"); return EM3D_ERR_INVALID; }
+  if (key == EM3D_TUNE_XPASS_VARIANT && (value < 0 || value > 2)) {
+    em3d_set_last_error("x-pass variant must be 0, 1 or 2");
+    return EM3D_ERR_INVALID;
+  }
+  g_tuning[key] = value;
+  return EM3D_OK;
+}
+
+int em3d_get_tuning(int key) { return (key >= 0 && key < EM3D_TUNE_COUNT) ? g_tuning[key] : -1; }
 
 size_t em3d_spectrum_bytes(const em3d_grid* g, int kind, int dtype) {
   Dims d;

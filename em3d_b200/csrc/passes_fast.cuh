@@ -77,7 +77,7 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
   }
   __syncthreads();
   const LayRows lay{pen * G::PSTRIDE, G::PSTRIDE};
-  reg_fft<L, E, INV, false, 1>(a, t, sm, tw, lay);
+  reg_fft<L, E, INV, false, 1, !INV>(a, t, sm, tw, lay);
 
   if constexpr (ST == FST_EM_ADJ) {
     // v - chi^H y needs all three components of y at each z: stage y through
@@ -170,7 +170,7 @@ kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner
   }
   __syncthreads();
   const LayInter lay{p, S, 0};
-  reg_fft<L, E, INV, false, 1>(a, t, sm, tw, lay);
+  reg_fft<L, E, INV, false, 1, !INV>(a, t, sm, tw, lay);
   if (!valid) return;
   T* dst = out + (size_t)o * LOUT * inner + i;
 #pragma unroll
@@ -184,13 +184,13 @@ kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner
   }
 }
 
-template <int L, int E, int C> struct XmulGeom {
+template <int L, int E, int C, int NTT = 256> struct XmulGeom {
   static constexpr int TT = L / E;
-  static constexpr int P = (256 / TT) >= 4 ? (256 / TT) : 4;
+  static constexpr int P = (NTT / TT) > 32 ? 32 : ((NTT / TT) >= 4 ? (NTT / TT) : 4);
   static constexpr int NT = P * TT;
   static constexpr int S = (P & 1) ? P : P + 1;
-  // FP64 exchanges one component at a time to keep shared memory small
-  static constexpr bool SEQ = (E == 8);
+  // small-E plans exchange one component at a time to keep shared memory small
+  static constexpr bool SEQ = (E <= 8);
   static constexpr int REGIONS = SEQ ? 1 : C;
 };
 
@@ -217,38 +217,37 @@ __device__ __forceinline__ void reg_exchange_seq(T (&a)[C][E], int t, T* sm, con
   }
 }
 
-template <int L, int E, bool INV, bool REV, int S> struct RegFFTSeq {
+template <int L, int E, bool INV, bool REV, int S, bool HALF_IN> struct RegFFTSeq {
   template <int C, typename T>
   __device__ __forceinline__ static void run(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const LayInter& lay) {
     using P = RegPlan<L, E>;
     constexpr int R = P::rad(REV, S);
     constexpr int NSV = P::nsb(REV, S);
-    reg_stage<L, E, R, NSV, INV, C>(a, t, tw);
+    reg_stage<L, E, R, NSV, INV, C, HALF_IN && S == 0>(a, t, tw);
     if constexpr (S + 1 < P::NS) {
       constexpr int RN = P::rad(REV, S + 1);
       reg_exchange_seq<L, E, R, NSV, RN, C>(a, t, sm, lay);
-      RegFFTSeq<L, E, INV, REV, S + 1>::template run<C>(a, t, sm, tw, lay);
+      RegFFTSeq<L, E, INV, REV, S + 1, HALF_IN>::template run<C>(a, t, sm, tw, lay);
     }
   }
 };
 
 template <int L, int E, bool INV, bool REV, bool SEQ, int C, typename T>
 __device__ __forceinline__ void reg_fft_x(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const LayInter& lay) {
-  if constexpr (SEQ) RegFFTSeq<L, E, INV, REV, 0>::template run<C>(a, t, sm, tw, lay);
-  else reg_fft<L, E, INV, REV, C>(a, t, sm, tw, lay);
+  if constexpr (SEQ) RegFFTSeq<L, E, INV, REV, 0, !INV>::template run<C>(a, t, sm, tw, lay);
+  else reg_fft<L, E, INV, REV, C, !INV>(a, t, sm, tw, lay);
 }
 
 __device__ __forceinline__ int kfold(int k, int n) { return k <= n ? k : 2 * n - k; }
 
 // Pencils along x for one (batch, ky, kz tile): forward FFT, spectrum multiply
 // in registers, reversed-plan inverse FFT, crop to x < Nx, in place in T2.
-template <typename R, int L, int C, bool ADJ>
-__global__ void __launch_bounds__(XmulGeom<L, FastE<R>::E, C>::NT)
+template <typename R, int L, int C, bool ADJ, int E, int NTT>
+__global__ void __launch_bounds__(XmulGeom<L, E, C, NTT>::NT)
 kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
         const int* skip) {
   using T = cx<R>;
-  constexpr int E = FastE<R>::E;
-  using G = XmulGeom<L, E, C>;
+  using G = XmulGeom<L, E, C, NTT>;
   using PL = RegPlan<L, E>;
   constexpr int TT = G::TT, PP = G::P, S = G::S;
   constexpr int Nx = L / 2;
@@ -335,6 +334,123 @@ kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg
 #pragma unroll
       for (int c = 0; c < C; ++c) col[((size_t)c * Nx + x) * xstride] = a[c][q * R1 + r];
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Component-split x pass (EM only): each thread transforms one component
+// pencil slice, so a thread holds E elements instead of 3E; the 3x3 dyadic
+// multiply reads the other two components of the same frequency through
+// shared memory.  Small CTAs (PZ = 8 columns) let two CTAs share an SM, so
+// one CTA's loads overlap the other's transforms.
+// ---------------------------------------------------------------------------
+template <int L, int E> struct XsplitGeom {
+  static constexpr int TT = L / E;
+  static constexpr int PZ = (384 / (3 * TT)) > 16 ? 16 : ((384 / (3 * TT)) < 2 ? 2 : (384 / (3 * TT)));
+  static constexpr int NT = 3 * PZ * TT;
+  static constexpr int S = (PZ & 1) ? PZ : PZ + 1;
+  static constexpr int REGION = L * S;
+};
+
+template <typename R, int L, bool ADJ, int E>
+__global__ void __launch_bounds__(XsplitGeom<L, E>::NT, 2)
+kf_xmul_split(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
+              const int* skip) {
+  using T = cx<R>;
+  using G = XsplitGeom<L, E>;
+  using PL = RegPlan<L, E>;
+  constexpr int TT = G::TT, PZ = G::PZ, S = G::S;
+  constexpr int Nx = L / 2;
+  constexpr int R1 = PL::first(false), RL = PL::last(false);
+  constexpr int M1 = L / R1, ML = L / RL;
+  if (skip_launch(skip)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tw = reinterpret_cast<T*>(smem_raw);
+  T* sm = tw + L;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
+  const int c = threadIdx.x / (PZ * TT);  // uniform per warp
+  const int rem = threadIdx.x - c * (PZ * TT);
+  const int p = rem % PZ, t = rem / PZ;
+  int idx = blockIdx.x;
+  const int tile = idx % ntz;
+  idx /= ntz;
+  const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
+  const int ky = idx % Ny2;
+  const int b = idx / Ny2;
+  const int kz = tile * PZ + p;
+  const bool valid = kz < Nz2;
+  const size_t xstride = (size_t)Ny2 * Nz2;
+  T* col = T2 + ((size_t)(b * 3 + c) * Nx) * xstride + (size_t)ky * Nz2 + kz;
+
+  T a[1][E];
+#pragma unroll
+  for (int q = 0; q < E / R1; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < R1 / 2; ++r) a[0][q * R1 + r] = valid ? col[(size_t)(j + r * M1) * xstride] : mk<R>(0, 0);
+#pragma unroll
+    for (int r = R1 / 2; r < R1; ++r) a[0][q * R1 + r] = mk<R>(0, 0);
+  }
+  __syncthreads();
+  const LayInter lay{c * G::REGION + p, S, 0};
+  reg_fft<L, E, false, false, 1, true>(a, t, sm, tw, lay);
+
+  // publish this component's spectrum values, then multiply by row c of the
+  // symmetric dyadic block (blocks xx yy zz xy xz yz)
+#pragma unroll
+  for (int q = 0; q < E / RL; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < RL; ++r) sm[lay(0, j + r * ML)] = a[0][q * RL + r];
+  }
+  __syncthreads();
+  const int bd = c;
+  const int b1 = (c == 2) ? 4 : 3;
+  const int b2 = (c == 0) ? 4 : 5;
+  const int r1 = ((c == 0) ? 1 : 0) * G::REGION + p;  // shared-memory base of component c1
+  const int r2 = ((c == 2) ? 1 : 2) * G::REGION + p;  // and of component c2
+  const R sy = ky <= Ny ? (R)1 : (R)-1;
+  const R sz = kz <= Nz ? (R)1 : (R)-1;
+  // sign of block (c, c1) = sx * f1; of block (c, c2) = (c == 0 ? sx * sz : sy * sz)
+  const R f1 = (c == 2) ? sz : sy;
+  const bool b2x = (c == 0);
+  const R syz = sy * sz;
+  const int jy = kfold(ky, Ny);
+  const int l = kfold(valid ? kz : 0, Nz);
+  const size_t ostride = (size_t)(Nx + 1) * (Ny + 1) * (Nz + 1);
+  const size_t rowstride = (size_t)(Ny + 1) * (Nz + 1);
+  const T* spd = spec + bd * ostride + (size_t)jy * (Nz + 1) + l;
+  const T* sp1 = spec + b1 * ostride + (size_t)jy * (Nz + 1) + l;
+  const T* sp2 = spec + b2 * ostride + (size_t)jy * (Nz + 1) + l;
+#pragma unroll
+  for (int q = 0; q < E / RL; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      const int kx = j + r * ML;
+      const R sx = kx <= Nx ? (R)1 : (R)-1;
+      const size_t o = (size_t)kfold(kx, Nx) * rowstride;
+      T kd = mk<R>(0, 0), k1 = kd, k2 = kd;
+      if (valid) {
+        kd = spd[o];
+        k1 = cscale(sp1[o], sx * f1);
+        k2 = cscale(sp2[o], b2x ? sx * sz : syz);
+      }
+      if (ADJ) { kd = cconj(kd); k1 = cconj(k1); k2 = cconj(k2); }
+      const T X1 = sm[kx * S + r1];
+      const T X2 = sm[kx * S + r2];
+      const int e = q * RL + r;
+      a[0][e] = cadd(cadd(cmul(kd, a[0][e]), cmul(k1, X1)), cmul(k2, X2));
+    }
+  }
+  __syncthreads();
+  reg_fft<L, E, true, true, 1>(a, t, sm, tw, lay);
+  if (!valid) return;
+#pragma unroll
+  for (int q = 0; q < E / R1; ++q) {
+    const int j = t + q * TT;
+#pragma unroll
+    for (int r = 0; r < R1 / 2; ++r) col[(size_t)(j + r * M1) * xstride] = a[0][q * R1 + r];
   }
 }
 

@@ -52,6 +52,18 @@ int em3d_abi_version(void);
 const char* em3d_last_error(void);
 
 /* ------------------------------------------------------------------------
+ * Tuning (process-wide; chosen by em3d_b200.tune.autotune).  No counterpart
+ * in the reference, which has no native code to tune.
+ * ------------------------------------------------------------------------ */
+enum em3d_tune_key {
+  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: 0 register 256-thread, 1 register 128-thread, 2 component-split */
+  EM3D_TUNE_FFT_GENERIC = 1,   /* 1 = use the generic shared-memory FFT passes for every axis length */
+  EM3D_TUNE_COUNT = 2,
+};
+int em3d_set_tuning(int key, int value);
+int em3d_get_tuning(int key);
+
+/* ------------------------------------------------------------------------
  * Sizes
  * ------------------------------------------------------------------------ */
 

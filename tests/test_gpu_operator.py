@@ -210,12 +210,18 @@ def test_register_fft_path_matches_generic_path(prec, kind, monkeypatch):
             eta = (1.0 + torch.rand(N, dtype=tc, device="cuda")).contiguous()
             op = ea.AcousticOperator(ea.make_acoustic_problem(grid, eta, k0=9.0))
             u = torch.randn(N, dtype=tc, device="cuda")
-        fast_mv, fast_rmv = op.matvec(u), op.rmatvec(u)
-        monkeypatch.setenv("EM3D_FFT_GENERIC", "1")
+        from em3d_b200 import _lib
+        from em3d_b200.tune import set_xpass_variant
+
+        _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 1)
         gen_mv, gen_rmv = op.matvec(u), op.rmatvec(u)
-        monkeypatch.delenv("EM3D_FFT_GENERIC")
-        assert rel_err(be.to_host(fast_mv), be.to_host(gen_mv)) < tol, N
-        assert rel_err(be.to_host(fast_rmv), be.to_host(gen_rmv)) < tol, N
+        _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 0)
+        for v in (0, 1, 2):
+            set_xpass_variant(v)
+            fast_mv, fast_rmv = op.matvec(u), op.rmatvec(u)
+            assert rel_err(be.to_host(fast_mv), be.to_host(gen_mv)) < tol, (N, v)
+            assert rel_err(be.to_host(fast_rmv), be.to_host(gen_rmv)) < tol, (N, v)
+        set_xpass_variant(0)
     del rng
 
 
@@ -234,8 +240,11 @@ def test_em_matvec_oracle_at_32_cubed_both_paths(monkeypatch):
     op = e.Operator(e.Problem(grid=grid, eps_tensor=chi, wave=u, k0=k, volume=1.0))
     kh = oem.kernel_hat(N, L, k)
     ref, ref_a = oem.matvec(chi, u, kh, N), oem.rmatvec(chi, u, N, khat=kh)
-    for generic in ("0", "1"):
-        monkeypatch.setenv("EM3D_FFT_GENERIC", generic)
+    from em3d_b200 import _lib
+
+    for generic in (0, 1):
+        _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, generic)
         assert rel_err(be.to_host(op.matvec(u)), ref) < 1e-12
         assert rel_err(be.to_host(op.rmatvec(u)), ref_a) < 1e-12
+    _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 0)
     del g
