@@ -63,23 +63,22 @@ SIGNATURES = {
     "em3d_krylov_state_bytes": (c_size_t, [c_int]),
     "em3d_krylov_history_offset": (c_size_t, [c_int]),
     "em3d_krylov_counts_offset": (c_size_t, [c_int]),
-    "em3d_vec_dots": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "em3d_vec_dots": (c_int, [c_int, c_size_t, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
+                              c_void_p]),
     "em3d_vec_axpby": (c_int, [c_int, c_size_t, c_void_p, c_double, c_double, c_void_p, c_double, c_double,
                                c_void_p, c_void_p]),
     "em3d_vec_convert": (c_int, [c_size_t, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p]),
-    "em3d_bicgstab_p": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "em3d_bicgstab_alpha": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "em3d_bicgstab_s": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "em3d_bicgstab_omega": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "em3d_bicgstab_update": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
-                                     c_void_p, c_void_p]),
-    "em3d_bicgstab_finalize": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "em3d_sim_residual": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "em3d_sim_update": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "em3d_twostep_residual": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "em3d_twostep_coeffs": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "em3d_twostep_update": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
-                                    c_void_p]),
+    "em3d_bicgstab_p": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "em3d_bicgstab_alpha": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]),
+    "em3d_bicgstab_s": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "em3d_bicgstab_omega": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]),
+    "em3d_bicgstab_update": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "em3d_bicgstab_finalize": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]),
+    "em3d_sim_residual": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]),
+    "em3d_sim_update": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]),
+    "em3d_twostep_residual": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]),
+    "em3d_twostep_coeffs": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "em3d_twostep_update": (c_int, [c_int, c_size_t, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

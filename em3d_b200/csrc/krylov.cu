@@ -33,13 +33,16 @@ __host__ __device__ inline size_t hist_off(int cap) { return kStateHeader; }
 __host__ __device__ inline size_t counts_off(int cap) { return kStateHeader + ((size_t)8 * cap + 255) / 256 * 256; }
 __host__ __device__ inline size_t partials_off(int cap) { return counts_off(cap) + ((size_t)4 * cap + 255) / 256 * 256; }
 
-__device__ inline StateView view(void* base) {
+// State of right-hand side blockIdx.y; states are `stride` bytes apart and
+// state 0 also carries the batch-wide running count and done flag.
+__device__ inline StateView view(void* base, size_t stride) {
   StateView v;
-  v.st = (em3d_krylov_state*)base;
+  v.st = (em3d_krylov_state*)((char*)base + blockIdx.y * stride);
   const int cap = v.st->hist_cap;
-  v.hist = (double*)((char*)base + hist_off(cap));
-  v.counts = (int*)((char*)base + counts_off(cap));
-  v.partials = (double*)((char*)base + partials_off(cap));
+  char* mine = (char*)v.st;
+  v.hist = (double*)(mine + hist_off(cap));
+  v.counts = (int*)(mine + counts_off(cap));
+  v.partials = (double*)(mine + partials_off(cap));
   return v;
 }
 
@@ -120,6 +123,16 @@ __device__ inline void record(StateView& sv, double rel, int actions) {
   st->last_rel = rel;
 }
 
+// Set a stop status for this right-hand side (once) and maintain the batch
+// count; the last one to stop raises batch_done, the operator's skip flag.
+__device__ inline void stop_rhs(em3d_krylov_state* st, void* base, int code) {
+  if (st->status != EM3D_RUNNING || code == EM3D_RUNNING) return;
+  st->status = code;
+  em3d_krylov_state* b0 = (em3d_krylov_state*)base;
+  __threadfence();
+  if (atomicSub(&b0->batch_running, 1) == 1) b0->batch_done = 1;
+}
+
 __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
   // plain complex division (the magnitudes here are far from over/underflow)
   const double den = b.x * b.x + b.y * b.y;
@@ -141,8 +154,11 @@ template <typename C> __device__ __forceinline__ void acc_dot(double& re, double
 
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_dots(size_t n, const cx<R>* x0, const cx<R>* y0, const cx<R>* x1,
-                                                   const cx<R>* y1, void* state) {
-  StateView sv = view(state);
+                                                   const cx<R>* y1, void* state, size_t sstride) {
+  StateView sv = view(state, sstride);
+  const size_t vo = blockIdx.y * n;
+  x0 += vo; y0 += vo;
+  if (x1) { x1 += vo; y1 += vo; }
   double v[4] = {0, 0, 0, 0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     acc_dot(v[0], v[1], x0[i], y0[i]);
@@ -183,16 +199,17 @@ __global__ void k_convert(size_t n, const S* src, D* dst, int accumulate) {
 // rho / omega checks, beta, p = r + beta (p - omega v) (p = r on the first
 // iteration), then the action-budget check before the matvec v = A p.
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_bicg_p(size_t n, void* state, const cx<R>* r, cx<R>* p, const cx<R>* v) {
-  em3d_krylov_state* st = (em3d_krylov_state*)state;
+__global__ void __launch_bounds__(kThreads) k_bicg_p(size_t n, void* state, size_t sstride, const cx<R>* r, cx<R>* p, const cx<R>* v) {
+  em3d_krylov_state* st = (em3d_krylov_state*)((char*)state + blockIdx.y * sstride);
   if (!running(st)) return;
+  { const size_t vo = blockIdx.y * n; r += vo; p += vo; v += vo; }
   const double2 rho = make_double2(st->rho_re, st->rho_im);
   const double2 omega = make_double2(st->omega_re, st->omega_im);
   int stop = EM3D_RUNNING;
   if (cabs2(rho) == 0.0) stop = EM3D_BREAKDOWN_RHO;
   else if (st->iter > 0 && cabs2(omega) == 0.0) stop = EM3D_BREAKDOWN_OMEGA;
   if (stop != EM3D_RUNNING) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->status = stop;
+    if (blockIdx.x == 0 && threadIdx.x == 0) stop_rhs(st, state, stop);
     return;
   }
   if (st->iter == 0) {
@@ -206,15 +223,16 @@ __global__ void __launch_bounds__(kThreads) k_bicg_p(size_t n, void* state, cons
       p[i] = cadd(r[i], cmul(b, csub(p[i], cmul(w, v[i]))));
   }
   if (st->max_actions >= 0 && st->matvecs + 1 > st->max_actions) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->status = EM3D_MAX_OPERATOR_ACTIONS;
+    if (blockIdx.x == 0 && threadIdx.x == 0) stop_rhs(st, state, EM3D_MAX_OPERATOR_ACTIONS);
   }
 }
 
 // den = vdot(r_hat, v); alpha = rho / den.
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, const cx<R>* rh, const cx<R>* v) {
-  StateView sv = view(state);
+__global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, size_t sstride, const cx<R>* rh, const cx<R>* v) {
+  StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
+  { const size_t vo = blockIdx.y * n; rh += vo; v += vo; }
   double a[2] = {0, 0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     acc_dot(a[0], a[1], rh[i], v[i]);
@@ -223,7 +241,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, 
     em3d_krylov_state* st = sv.st;
     st->matvecs += 1;
     const double2 den = make_double2(tot[0], tot[1]);
-    if (cabs2(den) == 0.0) { st->status = EM3D_BREAKDOWN_ALPHA; return; }
+    if (cabs2(den) == 0.0) { stop_rhs(st, state, EM3D_BREAKDOWN_ALPHA); return; }
     const double2 al = cdiv(make_double2(st->rho_re, st->rho_im), den);
     st->alpha_re = al.x;
     st->alpha_im = al.y;
@@ -233,9 +251,10 @@ __global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, 
 // s = r - alpha v, ||s||; stopping checks on ||s|| (the update u += alpha p
 // of an early exit is applied by the finalize kernel).
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_bicg_s(size_t n, void* state, const cx<R>* r, const cx<R>* v, cx<R>* s) {
-  StateView sv = view(state);
+__global__ void __launch_bounds__(kThreads) k_bicg_s(size_t n, void* state, size_t sstride, const cx<R>* r, const cx<R>* v, cx<R>* s) {
+  StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
+  { const size_t vo = blockIdx.y * n; r += vo; v += vo; s += vo; }
   const cx<R> al = cast_s<R>(sv.st->alpha_re, sv.st->alpha_im);
   double a[1] = {0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -257,16 +276,17 @@ __global__ void __launch_bounds__(kThreads) k_bicg_s(size_t n, void* state, cons
       record(sv, srel, st->matvecs);
       st->iter += 1;
       st->pending = 1;
-      st->status = stop;
+      stop_rhs(st, state, stop);
     }
   }
 }
 
 // tt = vdot(t, t), ts = vdot(t, s); omega = ts / tt with the breakdown checks.
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_bicg_omega(size_t n, void* state, const cx<R>* t, const cx<R>* s) {
-  StateView sv = view(state);
+__global__ void __launch_bounds__(kThreads) k_bicg_omega(size_t n, void* state, size_t sstride, const cx<R>* t, const cx<R>* s) {
+  StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
+  { const size_t vo = blockIdx.y * n; t += vo; s += vo; }
   double a[3] = {0, 0, 0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const cx<R> ti = t[i];
@@ -291,7 +311,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_omega(size_t n, void* state, 
       record(sv, st->last_rel, st->matvecs);
       st->iter += 1;
       st->pending = 1;
-      st->status = stop;
+      stop_rhs(st, state, stop);
     }
   }
 }
@@ -299,11 +319,12 @@ __global__ void __launch_bounds__(kThreads) k_bicg_omega(size_t n, void* state, 
 // u = (u + alpha p) + omega s;  r = s - omega t;  ||r||, vdot(r_hat, r) for the
 // next rho; stopping checks on ||r||.
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_bicg_update(size_t n, void* state, cx<R>* u, const cx<R>* p,
+__global__ void __launch_bounds__(kThreads) k_bicg_update(size_t n, void* state, size_t sstride, cx<R>* u, const cx<R>* p,
                                                           const cx<R>* s, const cx<R>* t, cx<R>* r,
                                                           const cx<R>* rh) {
-  StateView sv = view(state);
+  StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
+  { const size_t vo = blockIdx.y * n; u += vo; p += vo; s += vo; t += vo; r += vo; rh += vo; }
   const cx<R> al = cast_s<R>(sv.st->alpha_re, sv.st->alpha_im);
   const cx<R> om = cast_s<R>(sv.st->omega_re, sv.st->omega_im);
   double a[3] = {0, 0, 0};
@@ -333,16 +354,17 @@ __global__ void __launch_bounds__(kThreads) k_bicg_update(size_t n, void* state,
       st->rho_im = tot[2];
       if (st->iter >= st->max_iter) stop = EM3D_MAX_ITER;
     }
-    st->status = stop;
+    stop_rhs(st, state, stop);
   }
 }
 
 // Early exits at s (converged / guard / budget / breakdown_t / breakdown_omega)
 // return u + alpha p.  Runs whatever the status; pending goes 1 -> 2 when done.
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_bicg_finalize(size_t n, void* state, cx<R>* u, const cx<R>* p) {
-  StateView sv = view(state);
+__global__ void __launch_bounds__(kThreads) k_bicg_finalize(size_t n, void* state, size_t sstride, cx<R>* u, const cx<R>* p) {
+  StateView sv = view(state, sstride);
   if (*(volatile int*)&sv.st->pending != 1) return;
+  { const size_t vo = blockIdx.y * n; u += vo; p += vo; }
   const cx<R> al = cast_s<R>(sv.st->alpha_re, sv.st->alpha_im);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     u[i] = cadd(u[i], cmul(al, p[i]));
@@ -356,9 +378,10 @@ __global__ void __launch_bounds__(kThreads) k_bicg_finalize(size_t n, void* stat
 // ---------------------------------------------------------------------------
 
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_sim_residual(size_t n, void* state, cx<R>* res, const cx<R>* f) {
-  StateView sv = view(state);
+__global__ void __launch_bounds__(kThreads) k_sim_residual(size_t n, void* state, size_t sstride, cx<R>* res, const cx<R>* f) {
+  StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
+  { const size_t vo = blockIdx.y * n; res += vo; f += vo; }
   double a[1] = {0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const cx<R> ri = csub(res[i], f[i]);
@@ -377,14 +400,15 @@ __global__ void __launch_bounds__(kThreads) k_sim_residual(size_t n, void* state
     else if (st->guard >= 0.0 && rel > st->guard) stop = EM3D_DIVERGENCE_GUARD;
     else if (st->max_actions >= 0 && st->matvecs >= st->max_actions) stop = EM3D_MAX_OPERATOR_ACTIONS;
     else if (st->iter >= st->max_iter) stop = EM3D_MAX_ITER;
-    st->status = stop;
+    stop_rhs(st, state, stop);
   }
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_sim_update(size_t n, void* state, cx<R>* u, const cx<R>* res) {
-  StateView sv = view(state);
+__global__ void __launch_bounds__(kThreads) k_sim_update(size_t n, void* state, size_t sstride, cx<R>* u, const cx<R>* res) {
+  StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
+  { const size_t vo = blockIdx.y * n; u += vo; res += vo; }
   const cx<R> g = cast_s<R>(sv.st->gamma_re, sv.st->gamma_im);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     u[i] = csub(u[i], cmul(g, res[i]));
@@ -398,9 +422,10 @@ __global__ void __launch_bounds__(kThreads) k_sim_update(size_t n, void* state, 
 // ---------------------------------------------------------------------------
 
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_ts_residual(size_t n, void* state, cx<R>* r, const cx<R>* f) {
-  StateView sv = view(state);
+__global__ void __launch_bounds__(kThreads) k_ts_residual(size_t n, void* state, size_t sstride, cx<R>* r, const cx<R>* f) {
+  StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
+  { const size_t vo = blockIdx.y * n; r += vo; f += vo; }
   double a[1] = {0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const cx<R> ri = csub(r[i], f[i]);
@@ -421,17 +446,18 @@ __global__ void __launch_bounds__(kThreads) k_ts_residual(size_t n, void* state,
     else if (st->max_actions >= 0 && acts >= st->max_actions) stop = EM3D_MAX_OPERATOR_ACTIONS;
     else if (st->iter >= st->max_iter) stop = EM3D_MAX_ITER;
     else if (st->max_actions >= 0 && acts + 2 > st->max_actions) stop = EM3D_MAX_OPERATOR_ACTIONS;
-    st->status = stop;
+    stop_rhs(st, state, stop);
   }
 }
 
 // a11 = Re<Hg,Hg>; first update: h = Re<g,g>/a11; later: the 2x2 minimal-residual
 // system in (t, h) with dr = r - r_prev.
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_ts_coeffs(size_t n, void* state, const cx<R>* r, const cx<R>* rp,
+__global__ void __launch_bounds__(kThreads) k_ts_coeffs(size_t n, void* state, size_t sstride, const cx<R>* r, const cx<R>* rp,
                                                         const cx<R>* g, const cx<R>* hg) {
-  StateView sv = view(state);
+  StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
+  { const size_t vo = blockIdx.y * n; r += vo; rp += vo; g += vo; hg += vo; }
   const bool first = sv.st->first != 0;
   double a[5] = {0, 0, 0, 0, 0};  // a11, gg | a00, a01, b0, b1
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -455,7 +481,7 @@ __global__ void __launch_bounds__(kThreads) k_ts_coeffs(size_t n, void* state, c
     st->rmatvecs += 1;
     st->matvecs += 1;
     const double a11 = tot[0];
-    if (!isfinite(a11) || a11 <= 0.0) { st->status = EM3D_BREAKDOWN_GRADIENT; return; }
+    if (!isfinite(a11) || a11 <= 0.0) { stop_rhs(st, state, EM3D_BREAKDOWN_GRADIENT); return; }
     if (first) {
       st->t = 0.0;
       st->h = tot[1] / a11;
@@ -475,10 +501,11 @@ __global__ void __launch_bounds__(kThreads) k_ts_coeffs(size_t n, void* state, c
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_ts_update(size_t n, void* state, cx<R>* u, cx<R>* up, const cx<R>* r,
+__global__ void __launch_bounds__(kThreads) k_ts_update(size_t n, void* state, size_t sstride, cx<R>* u, cx<R>* up, const cx<R>* r,
                                                         cx<R>* rp, const cx<R>* g) {
-  StateView sv = view(state);
+  StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
+  { const size_t vo = blockIdx.y * n; u += vo; up += vo; r += vo; rp += vo; g += vo; }
   const bool first = sv.st->first != 0;
   const R t = (R)sv.st->t, h = (R)sv.st->h;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -521,6 +548,12 @@ inline int check_state(const void* state, size_t n) {
   return EM3D_OK;
 }
 
+inline int check_batch(int batch, size_t stride) {
+  if (batch < 1 || batch > 65535) { em3d_set_last_error("batch must be in [1, 65535]"); return EM3D_ERR_INVALID; }
+  if (batch > 1 && stride < kStateHeader) { em3d_set_last_error("state stride too small"); return EM3D_ERR_INVALID; }
+  return EM3D_OK;
+}
+
 }  // namespace
 }  // namespace em3d
 
@@ -537,13 +570,16 @@ size_t em3d_krylov_state_bytes(int hist_cap) {
 size_t em3d_krylov_history_offset(int hist_cap) { return hist_off(hist_cap); }
 size_t em3d_krylov_counts_offset(int hist_cap) { return counts_off(hist_cap); }
 
-int em3d_vec_dots(int dtype, size_t n, const void* x0, const void* y0, const void* x1, const void* y1, void* state,
-                  void* stream) {
+int em3d_vec_dots(int dtype, size_t n, int batch, const void* x0, const void* y0, const void* x1, const void* y1,
+                  void* state, size_t state_stride, void* stream) {
   if (int rc = check_state(state, n)) return rc;
+  if (int rc = check_batch(batch, state_stride)) return rc;
   if (!x0 || !y0 || (x1 && !y1)) { em3d_set_last_error("NULL vector"); return EM3D_ERR_INVALID; }
   cudaStream_t st = (cudaStream_t)stream;
-  EM3D_DTYPE_DISPATCH(dtype, (k_dots<R><<<nblocks(n), kThreads, 0, st>>>(n, (const cx<R>*)x0, (const cx<R>*)y0,
-                                                                           (const cx<R>*)x1, (const cx<R>*)y1, state)));
+  const dim3 grid(nblocks(n), batch);
+  EM3D_DTYPE_DISPATCH(dtype, (k_dots<R><<<grid, kThreads, 0, st>>>(n, (const cx<R>*)x0, (const cx<R>*)y0,
+                                                                     (const cx<R>*)x1, (const cx<R>*)y1, state,
+                                                                     state_stride)));
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
@@ -579,47 +615,49 @@ int em3d_vec_convert(size_t n, int src_dtype, const void* src, int dst_dtype, vo
 #define EM3D_STEP(NAME, KERNEL, PARAMS, ARGS)                                         \
   int NAME PARAMS {                                                                   \
     if (int rc = check_state(state, n)) return rc;                                    \
+    if (int rc = check_batch(batch, sstride)) return rc;                              \
     cudaStream_t st = (cudaStream_t)stream;                                           \
-    EM3D_DTYPE_DISPATCH(dtype, (KERNEL<R><<<nblocks(n), kThreads, 0, st>>> ARGS));    \
+    const dim3 grid(nblocks(n), batch);                                               \
+    EM3D_DTYPE_DISPATCH(dtype, (KERNEL<R><<<grid, kThreads, 0, st>>> ARGS));          \
     EM3D_LAUNCH_CHECK();                                                              \
     return EM3D_OK;                                                                   \
   }
 
 EM3D_STEP(em3d_bicgstab_p, k_bicg_p,
-          (int dtype, size_t n, void* state, const void* r, void* p, const void* v, void* stream),
-          (n, state, (const cx<R>*)r, (cx<R>*)p, (const cx<R>*)v))
+          (int dtype, size_t n, int batch, void* state, size_t sstride, const void* r, void* p, const void* v, void* stream),
+          (n, state, sstride, (const cx<R>*)r, (cx<R>*)p, (const cx<R>*)v))
 EM3D_STEP(em3d_bicgstab_alpha, k_bicg_alpha,
-          (int dtype, size_t n, void* state, const void* r_hat, const void* v, void* stream),
-          (n, state, (const cx<R>*)r_hat, (const cx<R>*)v))
+          (int dtype, size_t n, int batch, void* state, size_t sstride, const void* r_hat, const void* v, void* stream),
+          (n, state, sstride, (const cx<R>*)r_hat, (const cx<R>*)v))
 EM3D_STEP(em3d_bicgstab_s, k_bicg_s,
-          (int dtype, size_t n, void* state, const void* r, const void* v, void* s, void* stream),
-          (n, state, (const cx<R>*)r, (const cx<R>*)v, (cx<R>*)s))
+          (int dtype, size_t n, int batch, void* state, size_t sstride, const void* r, const void* v, void* s, void* stream),
+          (n, state, sstride, (const cx<R>*)r, (const cx<R>*)v, (cx<R>*)s))
 EM3D_STEP(em3d_bicgstab_omega, k_bicg_omega,
-          (int dtype, size_t n, void* state, const void* t, const void* s, void* stream),
-          (n, state, (const cx<R>*)t, (const cx<R>*)s))
+          (int dtype, size_t n, int batch, void* state, size_t sstride, const void* t, const void* s, void* stream),
+          (n, state, sstride, (const cx<R>*)t, (const cx<R>*)s))
 EM3D_STEP(em3d_bicgstab_update, k_bicg_update,
-          (int dtype, size_t n, void* state, void* u, const void* p, const void* s, const void* t, void* r,
+          (int dtype, size_t n, int batch, void* state, size_t sstride, void* u, const void* p, const void* s, const void* t, void* r,
            const void* r_hat, void* stream),
-          (n, state, (cx<R>*)u, (const cx<R>*)p, (const cx<R>*)s, (const cx<R>*)t, (cx<R>*)r, (const cx<R>*)r_hat))
+          (n, state, sstride, (cx<R>*)u, (const cx<R>*)p, (const cx<R>*)s, (const cx<R>*)t, (cx<R>*)r, (const cx<R>*)r_hat))
 EM3D_STEP(em3d_bicgstab_finalize, k_bicg_finalize,
-          (int dtype, size_t n, void* state, void* u, const void* p, void* stream),
-          (n, state, (cx<R>*)u, (const cx<R>*)p))
+          (int dtype, size_t n, int batch, void* state, size_t sstride, void* u, const void* p, void* stream),
+          (n, state, sstride, (cx<R>*)u, (const cx<R>*)p))
 EM3D_STEP(em3d_sim_residual, k_sim_residual,
-          (int dtype, size_t n, void* state, void* res, const void* f, void* stream),
-          (n, state, (cx<R>*)res, (const cx<R>*)f))
+          (int dtype, size_t n, int batch, void* state, size_t sstride, void* res, const void* f, void* stream),
+          (n, state, sstride, (cx<R>*)res, (const cx<R>*)f))
 EM3D_STEP(em3d_sim_update, k_sim_update,
-          (int dtype, size_t n, void* state, void* u, const void* res, void* stream),
-          (n, state, (cx<R>*)u, (const cx<R>*)res))
+          (int dtype, size_t n, int batch, void* state, size_t sstride, void* u, const void* res, void* stream),
+          (n, state, sstride, (cx<R>*)u, (const cx<R>*)res))
 EM3D_STEP(em3d_twostep_residual, k_ts_residual,
-          (int dtype, size_t n, void* state, void* r, const void* f, void* stream),
-          (n, state, (cx<R>*)r, (const cx<R>*)f))
+          (int dtype, size_t n, int batch, void* state, size_t sstride, void* r, const void* f, void* stream),
+          (n, state, sstride, (cx<R>*)r, (const cx<R>*)f))
 EM3D_STEP(em3d_twostep_coeffs, k_ts_coeffs,
-          (int dtype, size_t n, void* state, const void* r, const void* r_prev, const void* g, const void* hg,
+          (int dtype, size_t n, int batch, void* state, size_t sstride, const void* r, const void* r_prev, const void* g, const void* hg,
            void* stream),
-          (n, state, (const cx<R>*)r, (const cx<R>*)r_prev, (const cx<R>*)g, (const cx<R>*)hg))
+          (n, state, sstride, (const cx<R>*)r, (const cx<R>*)r_prev, (const cx<R>*)g, (const cx<R>*)hg))
 EM3D_STEP(em3d_twostep_update, k_ts_update,
-          (int dtype, size_t n, void* state, void* u, void* u_prev, const void* r, void* r_prev, const void* g,
+          (int dtype, size_t n, int batch, void* state, size_t sstride, void* u, void* u_prev, const void* r, void* r_prev, const void* g,
            void* stream),
-          (n, state, (cx<R>*)u, (cx<R>*)u_prev, (const cx<R>*)r, (cx<R>*)r_prev, (const cx<R>*)g))
+          (n, state, sstride, (cx<R>*)u, (cx<R>*)u_prev, (const cx<R>*)r, (cx<R>*)r_prev, (const cx<R>*)g))
 
 }  // extern "C"

@@ -231,7 +231,7 @@ __device__ __forceinline__ int fsign(int k, int n) { return k <= n ? 1 : -1; }
 template <typename R, int C, bool ADJ>
 __global__ void __launch_bounds__(kThreads) k_xmul(cx<R>* T2, const cx<R>* __restrict__ spec,
                                                    const cx<R>* __restrict__ twg, AxisPlan pl, int Nx, int Ny,
-                                                   int Nz, int Pz, int ntz, const int* skip) {
+                                                   int Nz, int Pz, int ntz, int nb, const int* skip) {
   using T = cx<R>;
   if (skip_launch(skip)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -243,9 +243,9 @@ __global__ void __launch_bounds__(kThreads) k_xmul(cx<R>* T2, const cx<R>* __res
   T* tw = Bf + (size_t)L * S;
   load_twiddles(tw, twg, L);
   int idx = blockIdx.x;
-  const int tile = idx % ntz; idx /= ntz;
-  const int ky = idx % Ny2;
-  const int b = idx / Ny2;
+  const int b = idx % nb; idx /= nb;
+  const int tile = idx % ntz;
+  const int ky = idx / ntz;
   const int kz0 = tile * Pz;
   const size_t xstride = (size_t)Ny2 * Nz2;
 
@@ -501,7 +501,7 @@ static int launch_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims
   auto kern = k_xmul<R, C, ADJ>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const size_t grid = (size_t)batch * 2 * d.ny * ntz;
-  kern<<<(unsigned)grid, kThreads, smem, st>>>(T2, spec, tw, pl, d.nx, d.ny, d.nz, Pz, ntz, skip);
+  kern<<<(unsigned)grid, kThreads, smem, st>>>(T2, spec, tw, pl, d.nx, d.ny, d.nz, Pz, ntz, batch, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
@@ -715,7 +715,7 @@ static int go_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d,
   const int ntz = (2 * d.nz + G::P - 1) / G::P;
   const size_t smem = (size_t)(L + G::REGIONS * L * G::S) * sizeof(cx<R>);
   const size_t grid = (size_t)batch * 2 * d.ny * ntz;
-  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, skip);
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
@@ -729,7 +729,7 @@ static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& 
   const int ntz = (2 * d.nz + G::PZ - 1) / G::PZ;
   const size_t smem = (size_t)(L + 3 * G::REGION) * sizeof(cx<R>);
   const size_t grid = (size_t)batch * 2 * d.ny * ntz;
-  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, skip);
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }

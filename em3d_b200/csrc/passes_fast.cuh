@@ -245,7 +245,7 @@ __device__ __forceinline__ int kfold(int k, int n) { return k <= n ? k : 2 * n -
 template <typename R, int L, int C, bool ADJ, int E, int NTT>
 __global__ void __launch_bounds__(XmulGeom<L, E, C, NTT>::NT)
 kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
-        const int* skip) {
+        int nb, const int* skip) {
   using T = cx<R>;
   using G = XmulGeom<L, E, C, NTT>;
   using PL = RegPlan<L, E>;
@@ -259,12 +259,13 @@ kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg
   T* sm = tw + L;
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
   const int p = threadIdx.x % PP, t = threadIdx.x / PP;
+  // batch index fastest: consecutive CTAs share one spectrum tile in L2
   int idx = blockIdx.x;
+  const int b = idx % nb;
+  idx /= nb;
   const int tile = idx % ntz;
-  idx /= ntz;
+  const int ky = idx / ntz;
   const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
-  const int ky = idx % Ny2;
-  const int b = idx / Ny2;
   const int kz = tile * PP + p;
   const bool valid = kz < Nz2;
   const size_t xstride = (size_t)Ny2 * Nz2;
@@ -355,7 +356,7 @@ template <int L, int E> struct XsplitGeom {
 template <typename R, int L, bool ADJ, int E>
 __global__ void __launch_bounds__(XsplitGeom<L, E>::NT, 2)
 kf_xmul_split(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
-              const int* skip) {
+              int nb, const int* skip) {
   using T = cx<R>;
   using G = XsplitGeom<L, E>;
   using PL = RegPlan<L, E>;
@@ -371,12 +372,13 @@ kf_xmul_split(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict
   const int c = threadIdx.x / (PZ * TT);  // uniform per warp
   const int rem = threadIdx.x - c * (PZ * TT);
   const int p = rem % PZ, t = rem / PZ;
+  // batch index fastest: consecutive CTAs share one spectrum tile in L2
   int idx = blockIdx.x;
+  const int b = idx % nb;
+  idx /= nb;
   const int tile = idx % ntz;
-  idx /= ntz;
+  const int ky = idx / ntz;
   const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
-  const int ky = idx % Ny2;
-  const int b = idx / Ny2;
   const int kz = tile * PZ + p;
   const bool valid = kz < Nz2;
   const size_t xstride = (size_t)Ny2 * Nz2;

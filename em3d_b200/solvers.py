@@ -84,7 +84,8 @@ class KrylovState(ctypes.Structure):
         ("t", c_double), ("h", c_double), ("last_rel", c_double), ("dots", c_double * 4),
         ("status", c_int32), ("iter", c_int32), ("matvecs", c_int32), ("rmatvecs", c_int32),
         ("max_iter", c_int32), ("max_actions", c_int32), ("hist_len", c_int32), ("hist_cap", c_int32),
-        ("pending", c_int32), ("first", c_int32), ("ticket", c_uint32), ("reserved", c_int32),
+        ("pending", c_int32), ("first", c_int32), ("ticket", c_uint32), ("batch_running", c_int32),
+        ("batch_done", c_int32),
     ]
 
 
@@ -96,60 +97,90 @@ def _check_abi():
 
 
 class DeviceState:
-    """One solver's state buffer on the device (struct + history + partials)."""
+    """The solver states of a batch of right-hand sides on the device: one
+    block per right-hand side (struct + history + reduction partials)."""
 
-    STATUS_OFFSET = KrylovState.status.offset
+    DONE_OFFSET = KrylovState.batch_done.offset
 
-    def __init__(self, device, hist_cap: int):
+    def __init__(self, device, hist_cap: int, batch: int = 1):
         import torch
 
         _check_abi()
         lib = _lib.load()
         self.cap = int(max(hist_cap, 2))
-        nbytes = lib.em3d_krylov_state_bytes(self.cap)
-        self.buf = torch.zeros(nbytes, dtype=torch.uint8, device=device)
+        self.batch = int(batch)
+        self.stride = int(lib.em3d_krylov_state_bytes(self.cap))
+        self.buf = torch.zeros(self.stride * self.batch, dtype=torch.uint8, device=device)
         self.hist_off = lib.em3d_krylov_history_offset(self.cap)
         self.counts_off = lib.em3d_krylov_counts_offset(self.cap)
-        self.host = KrylovState()
-        self.host.hist_cap = self.cap
-        self._status_view = self.buf[self.STATUS_OFFSET:self.STATUS_OFFSET + 4].view(torch.int32)
+        self.hosts = [KrylovState() for _ in range(self.batch)]
+        for h in self.hosts:
+            h.hist_cap = self.cap
+        self._done_view = self.buf[self.DONE_OFFSET:self.DONE_OFFSET + 4].view(torch.int32)
+
+    @property
+    def host(self) -> KrylovState:
+        return self.hosts[0]
 
     @property
     def ptr(self) -> int:
         return self.buf.data_ptr()
 
     @property
-    def status_ptr(self) -> int:
-        return self.buf.data_ptr() + self.STATUS_OFFSET
+    def done_ptr(self) -> int:
+        """Device address of the batch-wide done flag (the operators' skip flag)."""
+        return self.buf.data_ptr() + self.DONE_OFFSET
 
-    def upload(self, hist=(), counts=()):
+    def upload(self, hists=None, counts=None):
+        """Copy the host headers (and initial histories) of all right-hand sides.
+        The batch running count and done flag are derived from the statuses."""
         import torch
 
-        self.host.hist_cap = self.cap
-        self.host.hist_len = len(hist)
-        raw = bytes(self.host)
-        self.buf[: len(raw)].copy_(torch.frombuffer(bytearray(raw), dtype=torch.uint8))
-        if len(hist):
-            h = np.asarray(hist, dtype=np.float64)
-            c = np.asarray(counts, dtype=np.int32)
-            self.buf[self.hist_off:self.hist_off + h.nbytes].copy_(torch.from_numpy(h.view(np.uint8)))
-            self.buf[self.counts_off:self.counts_off + c.nbytes].copy_(torch.from_numpy(c.view(np.uint8)))
+        running = sum(1 for h in self.hosts if h.status == 0)
+        raw = bytearray()
+        for b, h in enumerate(self.hosts):
+            h.hist_cap = self.cap
+            h.hist_len = len(hists[b]) if hists else 0
+            h.ticket = 0
+            h.batch_running = running if b == 0 else 0
+            h.batch_done = (1 if running == 0 else 0) if b == 0 else 0
+            blk = bytearray(self.stride)
+            hb = bytes(h)
+            blk[: len(hb)] = hb
+            if hists and len(hists[b]):
+                hv = np.asarray(hists[b], dtype=np.float64).tobytes()
+                cv = np.asarray(counts[b], dtype=np.int32).tobytes()
+                blk[self.hist_off:self.hist_off + len(hv)] = hv
+                blk[self.counts_off:self.counts_off + len(cv)] = cv
+            raw += blk
+        self.buf.copy_(torch.frombuffer(raw, dtype=torch.uint8))
 
-    def status(self) -> int:
-        return int(self._status_view.item())
+    def done(self) -> bool:
+        return int(self._done_view.item()) != 0
 
     def download(self):
-        head = self.buf[: ctypes.sizeof(KrylovState)].cpu().numpy().tobytes()
-        st = KrylovState.from_buffer_copy(head)
-        n = int(st.hist_len)
-        hist = self.buf[self.hist_off:self.hist_off + 8 * n].cpu().numpy().view(np.float64).tolist()
-        counts = self.buf[self.counts_off:self.counts_off + 4 * n].cpu().numpy().view(np.int32).tolist()
-        return st, hist, counts
+        """[(state, history, counts)] for every right-hand side."""
+        host = self.buf.cpu().numpy()
+        out = []
+        sz = ctypes.sizeof(KrylovState)
+        for b in range(self.batch):
+            base = b * self.stride
+            st = KrylovState.from_buffer_copy(host[base:base + sz].tobytes())
+            n = int(st.hist_len)
+            hist = host[base + self.hist_off:base + self.hist_off + 8 * n].view(np.float64).tolist()
+            counts = host[base + self.counts_off:base + self.counts_off + 4 * n].view(np.int32).tolist()
+            out.append((st, hist, counts))
+        return out
 
     def dots(self):
-        head = self.buf[: ctypes.sizeof(KrylovState)].cpu().numpy().tobytes()
-        st = KrylovState.from_buffer_copy(head)
-        return complex(st.dots[0], st.dots[1]), complex(st.dots[2], st.dots[3])
+        """[(dot0, dot1)] per right-hand side from the last em3d_vec_dots."""
+        host = self.buf.cpu().numpy()
+        sz = ctypes.sizeof(KrylovState)
+        res = []
+        for b in range(self.batch):
+            st = KrylovState.from_buffer_copy(host[b * self.stride:b * self.stride + sz].tobytes())
+            res.append((complex(st.dots[0], st.dots[1]), complex(st.dots[2], st.dots[3])))
+        return res
 
 
 def _native_dtype(t) -> int:
@@ -163,9 +194,10 @@ def _native_dtype(t) -> int:
 
 
 class _Engine:
-    """Vector plumbing shared by the three solvers."""
+    """Vector plumbing shared by the solvers.  ``rhs`` holds ``batch``
+    right-hand sides stacked along a leading axis (batch 1: no extra axis)."""
 
-    def __init__(self, operator, rhs, hist_cap):
+    def __init__(self, operator, rhs, hist_cap, batch: int = 1):
         import torch
 
         self.op = operator
@@ -174,10 +206,13 @@ class _Engine:
             rhs = torch.as_tensor(np.asarray(rhs))
         tc = self.be.precision.torch_complex if hasattr(self.be, "precision") else rhs.dtype
         self.rhs = rhs.to(device=self.be.torch_device, dtype=tc).contiguous()
-        self.n = int(self.rhs.numel())
+        self.batch = int(batch)
+        self.n = int(self.rhs.numel()) // self.batch
         self.dt = _native_dtype(self.rhs)
-        self.state = DeviceState(self.rhs.device, hist_cap)
+        self.state = DeviceState(self.rhs.device, hist_cap, self.batch)
         self.native_op = hasattr(operator, "apply_into")
+        if self.batch > 1 and not self.native_op:
+            raise TypeError("batched solves need an operator with apply_into (em3d_b200.Operator / AcousticOperator)")
         self.lib = _lib.load()
 
     def vec(self):
@@ -190,33 +225,39 @@ class _Engine:
 
     def apply(self, x, out, adjoint=False):
         if self.native_op:
-            self.op.apply_into(x, out, adjoint=adjoint, skip_ptr=self.state.status_ptr)
+            self.op.apply_into(x, out, adjoint=adjoint, skip_ptr=self.state.done_ptr)
         else:
             import torch
 
             y = self.op.rmatvec(x) if adjoint else self.op.matvec(x)
             out.copy_(torch.as_tensor(y, device=out.device).reshape(out.shape))
 
+    def norms(self, x) -> np.ndarray:
+        _lib.call("em3d_vec_dots", self.dt, self.n, self.batch, x.data_ptr(), x.data_ptr(), None, None,
+                  self.state.ptr, self.state.stride, self.stream())
+        return np.array([np.sqrt(max(d0.real, 0.0)) for d0, _ in self.state.dots()])
+
     def norm(self, x) -> float:
-        _lib.call("em3d_vec_dots", self.dt, self.n, x.data_ptr(), x.data_ptr(), None, None, self.state.ptr,
-                  self.stream())
-        d0, _ = self.state.dots()
-        return float(np.sqrt(max(d0.real, 0.0)))
+        return float(self.norms(x)[0])
 
     def step(self, name, *ptrs):
         fn = getattr(self.lib, name)
-        status = fn(self.dt, ctypes.c_size_t(self.n), ctypes.c_void_p(self.state.ptr),
-                    *[ctypes.c_void_p(p) for p in ptrs], ctypes.c_void_p(self.stream()))
+        status = fn(self.dt, ctypes.c_size_t(self.n), self.batch, ctypes.c_void_p(self.state.ptr),
+                    ctypes.c_size_t(self.state.stride), *[ctypes.c_void_p(p) for p in ptrs],
+                    ctypes.c_void_p(self.stream()))
         _lib.check(status, name)
         _lib.count_launches(name)
 
     def run(self, iteration, chunk: int, use_graph: bool):
-        """Launch ``iteration`` until the device status says stop.  With a native
-        operator the iterations are replayed ``chunk`` at a time from a CUDA graph."""
+        """Launch ``iteration`` until every right-hand side has stopped.  With a
+        native operator the iterations are replayed ``chunk`` at a time from a
+        CUDA graph."""
         import torch
 
+        if self.state.done():
+            return
         iteration()
-        if self.state.status() != 0:
+        if self.state.done():
             return
         graph = None
         per_replay = 0
@@ -234,7 +275,7 @@ class _Engine:
                 graph = None
             per_replay = _lib.launch_count - before
             _lib.launch_count = before  # captured, not launched
-        while self.state.status() == 0:
+        while not self.state.done():
             if graph is not None:
                 graph.replay()
                 _lib.launch_count += per_replay
@@ -255,7 +296,7 @@ def _log(tag, history, counts, label="iter"):
         print(f"[{tag}] {label}={i}, actions={c}, rel_res={r:.3e}")
 
 
-def _result(u, st, hist, counts, rmv=0) -> SolverResult:
+def _result(u, st, hist, counts) -> SolverResult:
     status = _status_name(st.status)
     return SolverResult(u=u, iterations=int(st.iter), residual_history=[float(h) for h in hist],
                         converged=status == "converged", matvec_count=int(st.matvecs),
@@ -263,10 +304,7 @@ def _result(u, st, hist, counts, rmv=0) -> SolverResult:
                         status=status, true_final_residual=float(hist[-1]) if hist else float("inf"))
 
 
-def _trivial(rhs, x0=None) -> SolverResult:
-    import torch
-
-    u = torch.zeros_like(rhs) if x0 is None else x0.clone()
+def _trivial_result(u) -> SolverResult:
     return SolverResult(u=u, iterations=0, residual_history=[0.0], converged=True, matvec_count=0,
                         residual_action_counts=[0], status="converged", true_final_residual=0.0)
 
@@ -288,7 +326,47 @@ def _init_u(eng, x0):
     return x.to(device=eng.rhs.device, dtype=eng.rhs.dtype).reshape(eng.rhs.shape).clone()
 
 
-class BiCGStab:
+def _batch_of(operator, rhs) -> int:
+    """Number of right-hand sides stacked in front of the operator's field shape."""
+    fs = operator._field_shape() if hasattr(operator, "_field_shape") else None
+    if fs is None:
+        return 1
+    lead = tuple(rhs.shape[: len(rhs.shape) - len(fs)])
+    if tuple(rhs.shape[len(lead):]) != tuple(fs):
+        raise ValueError(f"rhs.shape {tuple(rhs.shape)} != expected (..., {', '.join(map(str, fs))})")
+    return int(np.prod(lead)) if lead else 1
+
+
+class _KrylovSolver:
+    """``solve(operator, rhs)`` for one right-hand side (the reference's API) and
+    ``solve_batch(operator, rhs)`` for a stack of them sharing the operator."""
+
+    def solve(self, operator, rhs, x0=None) -> SolverResult:
+        import torch
+
+        t = rhs if isinstance(rhs, torch.Tensor) else torch.as_tensor(np.asarray(rhs))
+        return self._solve(operator, t, x0, batch=1)[0]
+
+    def solve_batch(self, operator, rhs, x0=None) -> list:
+        import torch
+
+        t = rhs if isinstance(rhs, torch.Tensor) else torch.as_tensor(np.asarray(rhs))
+        b = _batch_of(operator, t)
+        t = t.reshape((b,) + tuple(operator._field_shape()))
+        return self._solve(operator, t, x0, batch=b)
+
+    def _results(self, eng, u, trivial):
+        out = []
+        for b, (st, hist, counts) in enumerate(eng.state.download()):
+            ub = u if eng.batch == 1 else u[b]
+            if trivial[b]:
+                out.append(_trivial_result(ub))
+            else:
+                out.append(_result(ub, st, hist, counts))
+        return out
+
+
+class BiCGStab(_KrylovSolver):
     """BiCGStab (reference ``src/em3d/solvers/bicgstab.py``), device resident."""
 
     graph_chunk = 4
@@ -296,46 +374,48 @@ class BiCGStab:
     def __init__(self, config: SolverConfig):
         self.cfg = config
 
-    def solve(self, operator, rhs, x0=None) -> SolverResult:
+    def _solve(self, operator, rhs, x0, batch):
         cfg = self.cfg
-        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2)
+        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2, batch=batch)
         rhs = eng.rhs
-        rhs_norm = eng.norm(rhs)
-        if rhs_norm == 0.0:
-            return _trivial(rhs)
-        tol = max(float(cfg.rtol), float(cfg.atol) / rhs_norm)
+        rhs_norms = eng.norms(rhs)
         u = _init_u(eng, x0)
         r = eng.vec()
         eng.apply(u, r)
-        _lib.call("em3d_vec_axpby", eng.dt, eng.n, r.data_ptr(), 1.0, 0.0, rhs.data_ptr(), -1.0, 0.0, r.data_ptr(),
-                  eng.stream())
-        rr = eng.norm(r)
-        rel0 = rr / rhs_norm
-        st = eng.state.host
-        st.rhs_norm, st.tol, st.guard = rhs_norm, tol, _guard(cfg.divergence_guard)
-        st.matvecs, st.rmatvecs, st.iter = 1, 0, 0
-        st.max_iter, st.max_actions = int(cfg.max_iter), _budget(cfg.max_operator_actions)
-        st.last_rel = rel0
-        early = None
-        if not np.isfinite(rel0):
-            early = 4
-        elif rel0 < tol:
-            early = 1
-        elif cfg.max_operator_actions is not None and 1 >= int(cfg.max_operator_actions):
-            early = 3
-        elif int(cfg.max_iter) <= 0:
-            early = 2
-        if early is not None:
-            st.status = early
-            return _result(u, st, [rel0], [1])
+        _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, rhs.data_ptr(), -1.0, 0.0,
+                  r.data_ptr(), eng.stream())
+        rr = eng.norms(r)
+        trivial = [bool(nrm == 0.0) for nrm in rhs_norms]
+        hists, counts = [], []
+        for b, st in enumerate(eng.state.hosts):
+            nrm = rhs_norms[b] if rhs_norms[b] != 0.0 else 1.0
+            rel0 = rr[b] / nrm
+            st.rhs_norm, st.tol, st.guard = nrm, max(float(cfg.rtol), float(cfg.atol) / nrm), _guard(cfg.divergence_guard)
+            st.matvecs, st.rmatvecs, st.iter = 1, 0, 0
+            st.max_iter, st.max_actions = int(cfg.max_iter), _budget(cfg.max_operator_actions)
+            st.last_rel = rel0
+            st.rho_re, st.rho_im = rr[b] * rr[b], 0.0
+            st.rho_prev_re, st.rho_prev_im = 1.0, 0.0
+            st.alpha_re, st.alpha_im = 1.0, 0.0
+            st.omega_re, st.omega_im = 1.0, 0.0
+            st.pending = 0
+            if trivial[b]:
+                st.status = 1
+            elif not np.isfinite(rel0):
+                st.status = 4
+            elif rel0 < st.tol:
+                st.status = 1
+            elif cfg.max_operator_actions is not None and 1 >= int(cfg.max_operator_actions):
+                st.status = 3
+            elif int(cfg.max_iter) <= 0:
+                st.status = 2
+            else:
+                st.status = 0
+            hists.append([rel0])
+            counts.append([1])
+        eng.state.upload(hists, counts)
         r_hat = r.clone()
         p, v, s, t = eng.vec(), eng.vec(), eng.vec(), eng.vec()
-        st.rho_re, st.rho_im = rr * rr, 0.0
-        st.rho_prev_re, st.rho_prev_im = 1.0, 0.0
-        st.alpha_re, st.alpha_im = 1.0, 0.0
-        st.omega_re, st.omega_im = 1.0, 0.0
-        st.status, st.pending = 0, 0
-        eng.state.upload([rel0], [1])
 
         def iteration():
             eng.step("em3d_bicgstab_p", r.data_ptr(), p.data_ptr(), v.data_ptr())
@@ -349,13 +429,14 @@ class BiCGStab:
             eng.step("em3d_bicgstab_finalize", u.data_ptr(), p.data_ptr())
 
         eng.run(iteration, self.graph_chunk, use_graph=True)
-        stf, hist, counts = eng.state.download()
+        res = self._results(eng, u, trivial)
         if cfg.log:
-            _log("BiCGStab", hist, counts)
-        return _result(u, stf, hist, counts)
+            for rb in res:
+                _log("BiCGStab", rb.residual_history, rb.residual_action_counts)
+        return res
 
 
-class SIM:
+class SIM(_KrylovSolver):
     """Simple iteration ``u <- u - gamma (A u - f)`` (reference ``src/em3d/solvers/sim.py``)."""
 
     graph_chunk = 8
@@ -364,21 +445,22 @@ class SIM:
         config.require_gamma()
         self.cfg = config
 
-    def solve(self, operator, rhs, x0=None) -> SolverResult:
+    def _solve(self, operator, rhs, x0, batch):
         cfg = self.cfg
-        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2)
+        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2, batch=batch)
         rhs = eng.rhs
-        rhs_norm = eng.norm(rhs)
-        if rhs_norm == 0.0:
-            return _trivial(rhs)
+        rhs_norms = eng.norms(rhs)
         gamma = 1.0 / complex(cfg.mu)
-        st = eng.state.host
-        st.rhs_norm = rhs_norm
-        st.tol = max(float(cfg.rtol), float(cfg.atol) / rhs_norm)
-        st.guard = _guard(cfg.divergence_guard)
-        st.gamma_re, st.gamma_im = gamma.real, gamma.imag
-        st.max_iter, st.max_actions = int(cfg.max_iter), _budget(cfg.max_operator_actions)
-        st.status = st.iter = st.matvecs = st.rmatvecs = 0
+        trivial = [bool(nrm == 0.0) for nrm in rhs_norms]
+        for b, st in enumerate(eng.state.hosts):
+            nrm = rhs_norms[b] if rhs_norms[b] != 0.0 else 1.0
+            st.rhs_norm = nrm
+            st.tol = max(float(cfg.rtol), float(cfg.atol) / nrm)
+            st.guard = _guard(cfg.divergence_guard)
+            st.gamma_re, st.gamma_im = gamma.real, gamma.imag
+            st.max_iter, st.max_actions = int(cfg.max_iter), _budget(cfg.max_operator_actions)
+            st.iter = st.matvecs = st.rmatvecs = 0
+            st.status = 1 if trivial[b] else 0
         eng.state.upload()
         u = _init_u(eng, x0)
         res = eng.vec()
@@ -389,13 +471,14 @@ class SIM:
             eng.step("em3d_sim_update", u.data_ptr(), res.data_ptr())
 
         eng.run(iteration, self.graph_chunk, use_graph=True)
-        stf, hist, counts = eng.state.download()
+        out = self._results(eng, u, trivial)
         if cfg.log:
-            _log("SIM", hist, counts, "updates")
-        return _result(u, stf, hist, counts)
+            for rb in out:
+                _log("SIM", rb.residual_history, rb.residual_action_counts, "updates")
+        return out
 
 
-class TwoStep:
+class TwoStep(_KrylovSolver):
     """Two-step minimal-residual gradient method (reference ``src/em3d/solvers/twostep.py``)."""
 
     graph_chunk = 4
@@ -403,20 +486,21 @@ class TwoStep:
     def __init__(self, config: SolverConfig):
         self.cfg = config
 
-    def solve(self, operator, rhs, x0=None) -> SolverResult:
+    def _solve(self, operator, rhs, x0, batch):
         cfg = self.cfg
-        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2)
+        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2, batch=batch)
         rhs = eng.rhs
-        rhs_norm = eng.norm(rhs)
-        if rhs_norm == 0.0:
-            return _trivial(rhs)
-        st = eng.state.host
-        st.rhs_norm = rhs_norm
-        st.tol = max(float(cfg.rtol), float(cfg.atol) / rhs_norm)
-        st.guard = _guard(cfg.divergence_guard)
-        st.max_iter, st.max_actions = int(cfg.max_iter), _budget(cfg.max_operator_actions)
-        st.status = st.iter = st.matvecs = st.rmatvecs = 0
-        st.first = 1
+        rhs_norms = eng.norms(rhs)
+        trivial = [bool(nrm == 0.0) for nrm in rhs_norms]
+        for b, st in enumerate(eng.state.hosts):
+            nrm = rhs_norms[b] if rhs_norms[b] != 0.0 else 1.0
+            st.rhs_norm = nrm
+            st.tol = max(float(cfg.rtol), float(cfg.atol) / nrm)
+            st.guard = _guard(cfg.divergence_guard)
+            st.max_iter, st.max_actions = int(cfg.max_iter), _budget(cfg.max_operator_actions)
+            st.iter = st.matvecs = st.rmatvecs = 0
+            st.first = 1
+            st.status = 1 if trivial[b] else 0
         eng.state.upload()
         u = _init_u(eng, x0)
         up, r, rp, g, hg = eng.vec(), eng.vec(), eng.vec(), eng.vec(), eng.vec()
@@ -430,10 +514,11 @@ class TwoStep:
             eng.step("em3d_twostep_update", u.data_ptr(), up.data_ptr(), r.data_ptr(), rp.data_ptr(), g.data_ptr())
 
         eng.run(iteration, self.graph_chunk, use_graph=True)
-        stf, hist, counts = eng.state.download()
+        out = self._results(eng, u, trivial)
         if cfg.log:
-            _log("TwoStep", hist, counts, "updates")
-        return _result(u, stf, hist, counts)
+            for rb in out:
+                _log("TwoStep", rb.residual_history, rb.residual_action_counts, "updates")
+        return out
 
 
 def true_relative_residual(operator, solution, rhs) -> float:
@@ -481,6 +566,8 @@ class DefectCorrection:
     ``inner_rtol`` is the FP32 solve's tolerance for the first correction;
     later corrections only need to bring the remaining residual down to
     ``rtol`` (with a safety factor), never looser than ``inner_rtol_max``.
+    ``solve_batch`` corrects a stack of right-hand sides together (batched
+    operator applications, batched inner solves); each stops on its own.
     """
 
     def __init__(self, config: SolverConfig, *, inner: str = "bicgstab", inner_rtol: float = 1e-4,
@@ -497,64 +584,95 @@ class DefectCorrection:
         self.safety = float(safety)
 
     def solve(self, operator, rhs, x0=None, *, operator_low=None) -> DefectCorrectionResult:
+        import torch
+
+        t = rhs if isinstance(rhs, torch.Tensor) else torch.as_tensor(np.asarray(rhs))
+        return self._solve(operator, t, x0, 1, operator_low)[0]
+
+    def solve_batch(self, operator, rhs, x0=None, *, operator_low=None) -> list:
+        import torch
+
+        t = rhs if isinstance(rhs, torch.Tensor) else torch.as_tensor(np.asarray(rhs))
+        b = _batch_of(operator, t)
+        t = t.reshape((b,) + tuple(operator._field_shape()))
+        return self._solve(operator, t, x0, b, operator_low)
+
+    def _solve(self, operator, rhs, x0, batch, operator_low):
+        import torch
+
         from .backend import Precision
 
         cfg = self.cfg
         op_lo = operator_low if operator_low is not None else operator.with_precision(Precision.SINGLE)
-        eng = _Engine(operator, rhs, hist_cap=4)
+        eng = _Engine(operator, rhs, hist_cap=4, batch=batch)
         f = eng.rhs
-        fn = eng.norm(f)
-        if fn == 0.0:
-            base = _trivial(f)
-            return DefectCorrectionResult(**base.__dict__)
-        tol = max(float(cfg.rtol), float(cfg.atol) / fn)
+        fn = eng.norms(f)
+        fs = np.where(fn == 0.0, 1.0, fn)
+        tol = np.maximum(float(cfg.rtol), float(cfg.atol) / fs)
         u = _init_u(eng, x0)
         r = eng.vec()
-        lo_dt = _lib.EM3D_C64
-        import torch
-
         r_lo = torch.empty(f.shape, dtype=torch.complex64, device=f.device)
-        hist, counts = [], []
-        mv64 = mv32 = rmv32 = 0
-        inner_its = []
-        status = "max_iter"
+        hist = [[] for _ in range(batch)]
+        counts = [[] for _ in range(batch)]
+        status = [("converged" if fn[b] == 0.0 else None) for b in range(batch)]
+        mv64 = 0
+        mv32 = np.zeros(batch, dtype=int)
+        rmv32 = np.zeros(batch, dtype=int)
+        inner_its = [[] for _ in range(batch)]
         inner_cls = BiCGStab if self.inner == "bicgstab" else TwoStep
         budget_inner = int(self.inner_max_iter or cfg.max_iter)
         for outer in range(self.max_outer + 1):
             operator.apply_into(u, r)
             mv64 += 1
-            _lib.call("em3d_vec_axpby", eng.dt, eng.n, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0, r.data_ptr(),
+            _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0,
+                      r.data_ptr(), eng.stream())
+            rel = eng.norms(r) / fs
+            for b in range(batch):
+                if status[b] is not None:
+                    continue
+                hist[b].append(float(rel[b]))
+                counts[b].append(int(mv64 + mv32[b] + rmv32[b]))
+                if cfg.log:
+                    print(f"[DefectCorrection] rhs={b}, outer={outer}, actions={counts[b][-1]}, rel_res={rel[b]:.3e}")
+                if not np.isfinite(rel[b]):
+                    status[b] = "nonfinite"
+                elif rel[b] < tol[b]:
+                    status[b] = "converged"
+                elif cfg.divergence_guard is not None and rel[b] > float(cfg.divergence_guard):
+                    status[b] = "divergence_guard"
+                elif outer == self.max_outer:
+                    status[b] = "max_iter"
+            running = [b for b in range(batch) if status[b] is None]
+            if not running:
+                break
+            target = min(min(self.inner_rtol_max, max(self.inner_rtol, self.safety * tol[b] / rel[b]))
+                         for b in running)
+            _lib.call("em3d_vec_convert", eng.n * batch, eng.dt, r.data_ptr(), _lib.EM3D_C64, r_lo.data_ptr(), 0,
                       eng.stream())
-            rel = eng.norm(r) / fn
-            hist.append(rel)
-            counts.append(mv64 + mv32 + rmv32)
-            if cfg.log:
-                print(f"[DefectCorrection] outer={outer}, actions={counts[-1]}, rel_res={rel:.3e}")
-            if not np.isfinite(rel):
-                status = "nonfinite"
-                break
-            if rel < tol:
-                status = "converged"
-                break
-            if cfg.divergence_guard is not None and rel > float(cfg.divergence_guard):
-                status = "divergence_guard"
-                break
-            if outer == self.max_outer:
-                status = "max_iter"
-                break
-            target = min(self.inner_rtol_max, max(self.inner_rtol, self.safety * tol / rel))
-            _lib.call("em3d_vec_convert", eng.n, eng.dt, r.data_ptr(), lo_dt, r_lo.data_ptr(), 0, eng.stream())
-            res = inner_cls(SolverConfig(max_iter=budget_inner, rtol=target)).solve(op_lo, r_lo)
-            mv32 += res.matvec_count
-            rmv32 += res.rmatvec_count
-            inner_its.append(res.iterations)
-            if res.status in ("nonfinite",):
-                status = "nonfinite"
-                break
-            d = res.u.contiguous()
-            _lib.call("em3d_vec_convert", eng.n, lo_dt, d.data_ptr(), eng.dt, u.data_ptr(), 1, eng.stream())
-        return DefectCorrectionResult(
-            u=u, iterations=sum(inner_its), residual_history=hist, converged=status == "converged",
-            matvec_count=mv64 + mv32, rmatvec_count=rmv32, residual_action_counts=counts, status=status,
-            true_final_residual=float(hist[-1]), outer_iterations=len(inner_its), inner_iterations=inner_its,
-            fp64_matvecs=mv64, fp32_matvecs=mv32, fp32_rmatvecs=rmv32)
+            if len(running) < batch:
+                for b in range(batch):
+                    if status[b] is not None:
+                        r_lo[b].zero_()
+            solver = inner_cls(SolverConfig(max_iter=budget_inner, rtol=target))
+            res = solver.solve(op_lo, r_lo) if batch == 1 else solver.solve_batch(op_lo, r_lo)
+            for b in running:
+                mv32[b] += res[b].matvec_count if batch > 1 else res.matvec_count
+                rmv32[b] += res[b].rmatvec_count if batch > 1 else res.rmatvec_count
+                inner_its[b].append(res[b].iterations if batch > 1 else res.iterations)
+            d = (res.u if batch == 1 else res[0].u._base if res[0].u._base is not None else res[0].u).contiguous()
+            if d.numel() != r_lo.numel():
+                d = torch.stack([rb.u for rb in res]).contiguous()
+            _lib.call("em3d_vec_convert", eng.n * batch, _lib.EM3D_C64, d.data_ptr(), eng.dt, u.data_ptr(), 1,
+                      eng.stream())
+        out = []
+        for b in range(batch):
+            ub = u if batch == 1 else u[b]
+            h = hist[b] if hist[b] else [0.0]
+            out.append(DefectCorrectionResult(
+                u=ub, iterations=int(sum(inner_its[b])), residual_history=h, converged=status[b] == "converged",
+                matvec_count=int(mv64 + mv32[b]), rmatvec_count=int(rmv32[b]),
+                residual_action_counts=counts[b] if counts[b] else [0], status=status[b] or "max_iter",
+                true_final_residual=float(h[-1]), outer_iterations=len(inner_its[b]),
+                inner_iterations=inner_its[b], fp64_matvecs=int(mv64), fp32_matvecs=int(mv32[b]),
+                fp32_rmatvecs=int(rmv32[b])))
+        return out

@@ -106,3 +106,42 @@ def acoustic_spheres(N: int = 256, precision: str = "double", k0: float = 20.0, 
         box = eta[sl[0], sl[1], sl[2]]
         box[m] = cdt(val)
     return AcousticCase(f"acoustic_{count}_spheres_{N}^3", Ns, L, c, k0, eta)
+
+
+def fibonacci_directions(n: int) -> np.ndarray:
+    """n unit vectors on a golden-angle (Fibonacci) spiral over the sphere."""
+    i = np.arange(n, dtype=np.float64)
+    z = 1.0 - 2.0 * (i + 0.5) / n
+    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    phi = i * np.pi * (3.0 - np.sqrt(5.0))
+    return np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=-1)
+
+
+def orthogonal_polarisations(direction) -> tuple:
+    """Two unit polarisations orthogonal to ``direction`` and to each other,
+    built from a fixed helper axis (z, or x when the direction is near z)."""
+    d = np.asarray(direction, dtype=np.float64)
+    d = d / np.linalg.norm(d)
+    helper = np.array([0.0, 0.0, 1.0]) if abs(d[2]) < 0.9 else np.array([1.0, 0.0, 0.0])
+    p1 = np.cross(helper, d)
+    p1 /= np.linalg.norm(p1)
+    p2 = np.cross(d, p1)
+    return p1, p2
+
+
+def plane_wave_batch(axes, k: float, n_directions: int, dtype=np.complex128) -> np.ndarray:
+    """(2 n_directions, 3, Nx, Ny, Nz): every Fibonacci direction with both
+    orthogonal polarisations, through ``flat_wave_vec``'s arithmetic."""
+    out = []
+    for d in fibonacci_directions(n_directions):
+        for p in orthogonal_polarisations(d):
+            out.append(_setup.flat_wave_vec_host(axes, k=k, orient=tuple(d), amplitude=tuple(p), dtype=dtype))
+    return np.stack(out)
+
+
+def multi_rhs_ellipsoid(N: int = 96, k0: float = 10.0, n_directions: int = 64, precision: str = "double"):
+    """The anisotropic ellipsoid at N^3 with 2 n_directions incident waves."""
+    case = aniso_ellipsoid_em(N, precision, k0=k0)
+    axes = _setup.grid_axes_host(case.N, case.L, case.center, precision)
+    waves = plane_wave_batch(axes, k0, n_directions, dtype=_setup.complex_dtype_of(precision))
+    return case, waves

@@ -147,14 +147,18 @@ int em3d_acoustic_rmatvec(const em3d_grid* g, int dtype, int batch, const void* 
 /* ------------------------------------------------------------------------
  * Device-resident Krylov solvers
  *
- * The solver scalars, counters, status and residual history live in one
- * device buffer (em3d_krylov_state followed by the history and the
- * reduction partials; size from em3d_krylov_state_bytes).  Inner products
- * and norms accumulate in FP64 whatever the vector dtype.  Every step kernel
- * returns at once when status != 0, and the operator entry points take
- * &state->status as their `skip` flag, so a sequence of iterations can be
- * launched (or replayed from a CUDA graph) without host round trips; the host
- * reads `status` once per chunk of iterations.
+ * The solver scalars, counters, status and residual history of one
+ * right-hand side live in one device block (em3d_krylov_state followed by
+ * the history and the reduction partials; size from
+ * em3d_krylov_state_bytes).  A batch of `batch` right-hand sides uses
+ * `batch` such blocks `state_stride` bytes apart and vectors stored batch
+ * after batch, each of length n; every right-hand side keeps its own
+ * scalars and stops on its own.  Inner products and norms accumulate in FP64
+ * whatever the vector dtype.  Step kernels skip right-hand sides whose
+ * status != 0, and the operator entry points take &state[0].batch_done as
+ * their `skip` flag, so a sequence of iterations can be launched (or
+ * replayed from a CUDA graph) without host round trips; the host reads
+ * batch_done once per chunk of iterations.
  * ------------------------------------------------------------------------ */
 
 enum em3d_solver_status {
@@ -190,7 +194,9 @@ typedef struct em3d_krylov_state {
   int32_t pending;             /* BiCGStab: 1 = u += alpha p still to apply    */
   int32_t first;               /* TwoStep: 1 before the first update           */
   uint32_t ticket;             /* last-block counter of the reductions         */
-  int32_t reserved;
+  int32_t batch_running;       /* state 0 only: right-hand sides still running */
+  int32_t batch_done;          /* state 0 only: 1 once all have stopped; the
+                                  operator's `skip` flag in a solve loop        */
 } em3d_krylov_state;
 
 /* sizeof(em3d_krylov_state) as compiled into the library (ABI check). */
@@ -204,11 +210,11 @@ size_t em3d_krylov_state_bytes(int hist_cap);
 size_t em3d_krylov_history_offset(int hist_cap);
 size_t em3d_krylov_counts_offset(int hist_cap);
 
-/* state->dots[0..1] = vdot(x0, y0); state->dots[2..3] = vdot(x1, y1) (when
- * x1 != NULL); FP64 accumulation.  Replaces xp.vdot / xp.linalg.norm of the
+/* Per right-hand side b: state[b].dots[0..1] = vdot(x0_b, y0_b) and
+ * state[b].dots[2..3] = vdot(x1_b, y1_b) (when x1 != NULL); FP64 accumulation.  Replaces xp.vdot / xp.linalg.norm of the
  * solvers (src/em3d/solvers/bicgstab.py:70,90). */
-int em3d_vec_dots(int dtype, size_t n, const void* x0, const void* y0, const void* x1, const void* y1,
-                  void* state, void* stream);
+int em3d_vec_dots(int dtype, size_t n, int batch, const void* x0, const void* y0, const void* x1, const void* y1,
+                  void* state, size_t state_stride, void* stream);
 /* out = a*x + b*y (scalars rounded to the vector dtype; y may be NULL). */
 int em3d_vec_axpby(int dtype, size_t n, void* out, double a_re, double a_im, const void* x, double b_re,
                    double b_im, const void* y, void* stream);
@@ -219,24 +225,24 @@ int em3d_vec_convert(size_t n, int src_dtype, const void* src, int dst_dtype, vo
 
 /* BiCGStab (src/em3d/solvers/bicgstab.py:12-211), one iteration =
  *   p -> [matvec v = A p] -> alpha -> s -> [matvec t = A s] -> omega -> update -> finalize */
-int em3d_bicgstab_p(int dtype, size_t n, void* state, const void* r, void* p, const void* v, void* stream);
-int em3d_bicgstab_alpha(int dtype, size_t n, void* state, const void* r_hat, const void* v, void* stream);
-int em3d_bicgstab_s(int dtype, size_t n, void* state, const void* r, const void* v, void* s, void* stream);
-int em3d_bicgstab_omega(int dtype, size_t n, void* state, const void* t, const void* s, void* stream);
-int em3d_bicgstab_update(int dtype, size_t n, void* state, void* u, const void* p, const void* s, const void* t,
+int em3d_bicgstab_p(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* r, void* p, const void* v, void* stream);
+int em3d_bicgstab_alpha(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* r_hat, const void* v, void* stream);
+int em3d_bicgstab_s(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* r, const void* v, void* s, void* stream);
+int em3d_bicgstab_omega(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* t, const void* s, void* stream);
+int em3d_bicgstab_update(int dtype, size_t n, int batch, void* state, size_t state_stride, void* u, const void* p, const void* s, const void* t,
                          void* r, const void* r_hat, void* stream);
-int em3d_bicgstab_finalize(int dtype, size_t n, void* state, void* u, const void* p, void* stream);
+int em3d_bicgstab_finalize(int dtype, size_t n, int batch, void* state, size_t state_stride, void* u, const void* p, void* stream);
 
 /* SIM (src/em3d/solvers/sim.py:13-91): [matvec res = A u] -> residual -> update */
-int em3d_sim_residual(int dtype, size_t n, void* state, void* res, const void* f, void* stream);
-int em3d_sim_update(int dtype, size_t n, void* state, void* u, const void* res, void* stream);
+int em3d_sim_residual(int dtype, size_t n, int batch, void* state, size_t state_stride, void* res, const void* f, void* stream);
+int em3d_sim_update(int dtype, size_t n, int batch, void* state, size_t state_stride, void* u, const void* res, void* stream);
 
 /* TwoStep (src/em3d/solvers/twostep.py:16-139):
  *   [matvec r = A u] -> residual -> [rmatvec g = A* r] -> [matvec hg = A g] -> coeffs -> update */
-int em3d_twostep_residual(int dtype, size_t n, void* state, void* r, const void* f, void* stream);
-int em3d_twostep_coeffs(int dtype, size_t n, void* state, const void* r, const void* r_prev, const void* g,
+int em3d_twostep_residual(int dtype, size_t n, int batch, void* state, size_t state_stride, void* r, const void* f, void* stream);
+int em3d_twostep_coeffs(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* r, const void* r_prev, const void* g,
                         const void* hg, void* stream);
-int em3d_twostep_update(int dtype, size_t n, void* state, void* u, void* u_prev, const void* r, void* r_prev,
+int em3d_twostep_update(int dtype, size_t n, int batch, void* state, size_t state_stride, void* u, void* u_prev, const void* r, void* r_prev,
                         const void* g, void* stream);
 
 #ifdef __cplusplus

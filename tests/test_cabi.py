@@ -67,7 +67,9 @@ def test_invalid_arguments_are_reported_not_launched():
     with pytest.raises(ValueError, match="dtype"):
         _lib.call("em3d_em_matvec", ctypes.byref(g), 7, 1, 1, 1, 1, 2, 1, 1 << 30, None, None)
     with pytest.raises(ValueError, match="state is NULL"):
-        _lib.call("em3d_bicgstab_p", _lib.EM3D_C64, 10, None, 1, 1, 1, None)
+        _lib.call("em3d_bicgstab_p", _lib.EM3D_C64, 10, 1, None, 0, 1, 1, 1, None)
+    with pytest.raises(ValueError, match="batch"):
+        _lib.call("em3d_bicgstab_p", _lib.EM3D_C64, 10, 0, 1, 0, 1, 1, 1, None)
 
 
 def test_krylov_state_layout_matches_library():

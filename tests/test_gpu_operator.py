@@ -248,3 +248,31 @@ def test_em_matvec_oracle_at_32_cubed_both_paths(monkeypatch):
         assert rel_err(be.to_host(op.rmatvec(u)), ref_a) < 1e-12
     _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 0)
     del g
+
+
+@pytest.mark.parametrize("N", [(16, 16, 16), (32, 16, 64)])
+@pytest.mark.parametrize("prec", ["double", "single"])
+def test_batched_matvec_equals_single_register_path(N, prec):
+    """Batched application on the register-FFT path (power-of-two axes)."""
+    import torch
+    import em3d_b200 as e
+    from em3d_b200 import acoustics as ea
+
+    be = _be(prec)
+    tc = be.precision.torch_complex
+    grid = e.Grid(N=N, L=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0), backend=be)
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    chi = (torch.randn((3, 3) + N, dtype=tc, device="cuda", generator=gen) * 0.3).contiguous()
+    U = torch.randn((7, 3) + N, dtype=tc, device="cuda", generator=gen)
+    op = e.Operator(e.Problem(grid=grid, eps_tensor=chi, wave=U[0], k0=5.0, volume=1.0))
+    tol = 1e-14 if prec == "double" else 1e-6
+    Y, Ya = op.matvec(U), op.rmatvec(U)
+    for b in range(7):
+        assert rel_err(be.to_host(Y[b]), be.to_host(op.matvec(U[b]))) < tol, b
+        assert rel_err(be.to_host(Ya[b]), be.to_host(op.rmatvec(U[b]))) < tol, b
+    eta = (1.0 + torch.rand(N, dtype=tc, device="cuda", generator=gen)).contiguous()
+    aop = ea.AcousticOperator(ea.make_acoustic_problem(grid, eta, k0=6.0))
+    V = torch.randn((5,) + N, dtype=tc, device="cuda", generator=gen)
+    Z = aop.matvec(V)
+    for b in range(5):
+        assert rel_err(be.to_host(Z[b]), be.to_host(aop.matvec(V[b]))) < tol, b
