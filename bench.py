@@ -39,12 +39,12 @@ RTOL = 1e-6
 METRIC = "em_solves_per_s_128^3_true_rtol1e-6"
 UNIT = "solves/s"
 # FP64 BiCGStab matvecs per solve of this workload to rtol 1e-6 (measured on
-# B200 by this script's fp64 leg; used only to convert CPU matvec timings).
-FP64_MATVECS_PER_SOLVE = None
-# dram__bytes_read.sum + dram__bytes_write.sum per FP32 EM matvec (all five
-# passes) from the ncu capture summarised in profiles/em_matvec_fp32_128.md;
-# None until that capture exists.
-NCU_TRAFFIC_BYTES = None
+# B200 by this script's fp64 leg: 24 iterations, 48 matvecs); used only by the
+# reference arm to convert a CPU matvec timing into solves/s.
+FP64_MATVECS_PER_SOLVE = 48
+# dram__bytes_read.sum + dram__bytes_write.sum per complex64 EM matvec (all
+# five passes) from the ncu launch list summarised in profiles/em_matvec_128.md.
+NCU_TRAFFIC_BYTES = 1495.4e6
 
 
 def byte_model(n: int, c: int) -> int:
