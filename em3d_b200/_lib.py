@@ -59,6 +59,30 @@ SIGNATURES = {
     "em3d_static_scratch_bytes": (c_size_t, []),
     "em3d_set_tuning": (c_int, [c_int, c_int]),
     "em3d_get_tuning": (c_int, [c_int]),
+    "em3d_fno_lift": (c_int, [c_int, c_int, c_size_t, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                              c_void_p]),
+    "em3d_fno_lift_bwd": (c_int, [c_int, c_size_t, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                  c_void_p]),
+    "em3d_fno_contract": (c_int, [c_int, c_int, c_size_t, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
+                                  c_void_p]),
+    "em3d_fno_modemix": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "em3d_fno_modemix_bwd": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_void_p]),
+    "em3d_fno_layer_out": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
+                                   c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "em3d_fno_layer_out_bwd": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                       c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "em3d_fno_pointwise_wgrad": (c_int, [c_int, c_int, c_size_t, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                         c_void_p]),
+    "em3d_fno_project": (c_int, [c_int, c_int, c_size_t, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_void_p]),
+    "em3d_fno_project_bwd": (c_int, [c_int, c_int, c_size_t, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_void_p]),
+    "em3d_fno_loss": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "em3d_fno_adam": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_float,
+                              ctypes.c_float, ctypes.c_float, ctypes.c_float, c_int, c_void_p, c_void_p]),
+    "em3d_fno_cast": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p]),
+    "em3d_fno_uncast": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p]),
     "em3d_krylov_state_size": (c_size_t, []),
     "em3d_krylov_state_bytes": (c_size_t, [c_int]),
     "em3d_krylov_history_offset": (c_size_t, [c_int]),

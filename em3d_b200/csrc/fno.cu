@@ -1,0 +1,722 @@
+// Fourier-neural-operator warm start: forward, backward and optimiser kernels.
+//
+// Activations and weights are stored in ACT (bf16, or float for gradient
+// checks); every product accumulates in FP32.  Layout of a channel tensor:
+// (B, C, X, Y, Z), C-contiguous.  Mode-space tensors are complex FP32.
+//
+// Network (one layer l of L):
+//   V_l   = DFT_trunc(v_l)            separable: z -> m modes, y -> 2m, x -> 2m
+//   U_l   = W_l[mode] V_l[mode]       per-mode complex width x width mixing
+//   s     = Re(IDFT_trunc(U_l))       weights c_kz / (X Y Z), c_0 = 1, c_kz>0 = 2
+//   pre_l = A_l v_l + a_l + s
+//   v_l+1 = GELU(pre_l)               (identity after the last layer)
+// Lift (24 features -> width) before, projection (width -> 6) after; the
+// prediction is u = f + (out_0 + i out_1, out_2 + i out_3, out_4 + i out_5).
+//
+// The truncated DFTs are small complex contractions along one axis,
+// Y[o][j][i] = sum_l X[o][l][i] M[l][j]; the adjoint of a contraction with M
+// is the contraction with conj(M)^T, so the backward pass reuses the same
+// kernel with the forward/inverse matrices swapped.
+#include <cuda_bf16.h>
+#include <math.h>
+
+#include "common.cuh"
+
+namespace em3d {
+namespace fno {
+
+constexpr int kMaxWidth = 32;
+constexpr int kFeat = 24;
+
+template <typename A> __device__ __forceinline__ float ld(const A* p) { return (float)(*p); }
+template <> __device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+template <typename A> __device__ __forceinline__ A st(float v) { return (A)v; }
+template <> __device__ __forceinline__ __nv_bfloat16 st<__nv_bfloat16>(float v) { return __float2bfloat16(v); }
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+// ---------------------------------------------------------------------------
+// lift: 24 features per cell -> width channels
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void cell_features(const float2* chi, const float2* wave, size_t ncell, int b, size_t cell,
+                                              float* f) {
+  const float2* c = chi + (size_t)b * 9 * ncell + cell;
+  const float2* w = wave + (size_t)b * 3 * ncell + cell;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) { const float2 v = c[(size_t)i * ncell]; f[2 * i] = v.x; f[2 * i + 1] = v.y; }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) { const float2 v = w[(size_t)i * ncell]; f[18 + 2 * i] = v.x; f[19 + 2 * i] = v.y; }
+}
+
+template <typename ACT>
+__global__ void k_lift(int B, size_t ncell, int W, const float2* chi, const float2* wave, const ACT* P, const float* pb,
+                       ACT* v0) {
+  __shared__ float sP[kMaxWidth * kFeat], sb[kMaxWidth];
+  for (int i = threadIdx.x; i < W * kFeat; i += blockDim.x) sP[i] = ld(P + i);
+  for (int i = threadIdx.x; i < W; i += blockDim.x) sb[i] = pb[i];
+  __syncthreads();
+  const size_t total = (size_t)B * ncell;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(t / ncell);
+    const size_t cell = t - (size_t)b * ncell;
+    float f[kFeat];
+    cell_features(chi, wave, ncell, b, cell, f);
+    for (int co = 0; co < W; ++co) {
+      float acc = sb[co];
+#pragma unroll
+      for (int k = 0; k < kFeat; ++k) acc += sP[co * kFeat + k] * f[k];
+      v0[((size_t)b * W + co) * ncell + cell] = st<ACT>(acc);
+    }
+  }
+}
+
+// dP[co][f] += sum dv0[co] feat[f];  dpb[co] += sum dv0[co]
+__global__ void k_lift_bwd(int B, size_t ncell, int W, const float2* chi, const float2* wave, const float* dv0,
+                           float* dP, float* dpb) {
+  __shared__ float acc[kMaxWidth * (kFeat + 1)];
+  for (int i = threadIdx.x; i < W * (kFeat + 1); i += blockDim.x) acc[i] = 0.0f;
+  __syncthreads();
+  const size_t total = (size_t)B * ncell;
+  float local[kFeat + 1];
+  for (int co = 0; co < W; ++co) {
+#pragma unroll
+    for (int k = 0; k <= kFeat; ++k) local[k] = 0.0f;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+      const int b = (int)(t / ncell);
+      const size_t cell = t - (size_t)b * ncell;
+      float f[kFeat];
+      cell_features(chi, wave, ncell, b, cell, f);
+      const float g = dv0[((size_t)b * W + co) * ncell + cell];
+#pragma unroll
+      for (int k = 0; k < kFeat; ++k) local[k] += g * f[k];
+      local[kFeat] += g;
+    }
+#pragma unroll
+    for (int k = 0; k <= kFeat; ++k) {
+      float v = local[k];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0) atomicAdd(&acc[co * (kFeat + 1) + k], v);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < W * (kFeat + 1); i += blockDim.x) {
+    const int co = i / (kFeat + 1), k = i - co * (kFeat + 1);
+    if (k < kFeat) atomicAdd(&dP[co * kFeat + k], acc[i]);
+    else atomicAdd(&dpb[co], acc[i]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// contractions along one axis: Y[o][j][i] = sum_l X[o][l][i] M[l][j]
+// ---------------------------------------------------------------------------
+
+template <typename ACT>
+__global__ void k_contract_r2c(size_t outer, int L, int J, int inner, const ACT* X, const float2* M, float2* Y) {
+  const size_t total = outer * J * inner;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % inner);
+    const int j = (int)((t / inner) % J);
+    const size_t o = t / ((size_t)inner * J);
+    const ACT* x = X + o * L * inner + i;
+    float re = 0.0f, im = 0.0f;
+    for (int l = 0; l < L; ++l) {
+      const float v = ld(x + (size_t)l * inner);
+      const float2 m = M[l * J + j];
+      re += v * m.x;
+      im += v * m.y;
+    }
+    Y[t] = make_float2(re, im);
+  }
+}
+
+__global__ void k_contract_c2c(size_t outer, int L, int J, int inner, const float2* X, const float2* M, float2* Y) {
+  const size_t total = outer * J * inner;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % inner);
+    const int j = (int)((t / inner) % J);
+    const size_t o = t / ((size_t)inner * J);
+    const float2* x = X + o * L * inner + i;
+    float re = 0.0f, im = 0.0f;
+    for (int l = 0; l < L; ++l) {
+      const float2 v = x[(size_t)l * inner];
+      const float2 m = M[l * J + j];
+      re += v.x * m.x - v.y * m.y;
+      im += v.x * m.y + v.y * m.x;
+    }
+    Y[t] = make_float2(re, im);
+  }
+}
+
+// Y[o][j][i] += Re(sum_l X[o][l][i] M[l][j])  (adjoint of a real-input DFT)
+__global__ void k_contract_c2r_acc(size_t outer, int L, int J, int inner, const float2* X, const float2* M, float* Y) {
+  const size_t total = outer * J * inner;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % inner);
+    const int j = (int)((t / inner) % J);
+    const size_t o = t / ((size_t)inner * J);
+    const float2* x = X + o * L * inner + i;
+    float re = 0.0f;
+    for (int l = 0; l < L; ++l) {
+      const float2 v = x[(size_t)l * inner];
+      const float2 m = M[l * J + j];
+      re += v.x * m.x - v.y * m.y;
+    }
+    Y[t] += re;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// per-mode channel mixing; W stored (ci, co, mode) as complex ACT pairs
+// ---------------------------------------------------------------------------
+
+template <typename ACT>
+__global__ void k_modemix(int B, int W, int nm, const float2* V, const ACT* Wre, const ACT* Wim, float2* U) {
+  const size_t total = (size_t)B * W * nm;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int mode = (int)(t % nm);
+    const int co = (int)((t / nm) % W);
+    const int b = (int)(t / ((size_t)nm * W));
+    float re = 0.0f, im = 0.0f;
+    for (int ci = 0; ci < W; ++ci) {
+      const float2 v = V[((size_t)b * W + ci) * nm + mode];
+      const size_t wi = ((size_t)ci * W + co) * nm + mode;
+      const float wr = ld(Wre + wi), wim = ld(Wim + wi);
+      re += v.x * wr - v.y * wim;
+      im += v.x * wim + v.y * wr;
+    }
+    U[t] = make_float2(re, im);
+  }
+}
+
+// dV[b][ci][mode] = sum_co dU[b][co][mode] conj(W[ci][co][mode])
+template <typename ACT>
+__global__ void k_modemix_bwd_v(int B, int W, int nm, const float2* dU, const ACT* Wre, const ACT* Wim, float2* dV) {
+  const size_t total = (size_t)B * W * nm;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int mode = (int)(t % nm);
+    const int ci = (int)((t / nm) % W);
+    const int b = (int)(t / ((size_t)nm * W));
+    float re = 0.0f, im = 0.0f;
+    for (int co = 0; co < W; ++co) {
+      const float2 g = dU[((size_t)b * W + co) * nm + mode];
+      const size_t wi = ((size_t)ci * W + co) * nm + mode;
+      const float wr = ld(Wre + wi), wim = ld(Wim + wi);
+      re += g.x * wr + g.y * wim;
+      im += g.y * wr - g.x * wim;
+    }
+    dV[t] = make_float2(re, im);
+  }
+}
+
+// dW[ci][co][mode] += sum_b conj(V[b][ci][mode]) dU[b][co][mode]
+__global__ void k_modemix_bwd_w(int B, int W, int nm, const float2* V, const float2* dU, float* dWre, float* dWim) {
+  const size_t total = (size_t)W * W * nm;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int mode = (int)(t % nm);
+    const int co = (int)((t / nm) % W);
+    const int ci = (int)(t / ((size_t)nm * W));
+    float re = 0.0f, im = 0.0f;
+    for (int b = 0; b < B; ++b) {
+      const float2 v = V[((size_t)b * W + ci) * nm + mode];
+      const float2 g = dU[((size_t)b * W + co) * nm + mode];
+      re += v.x * g.x + v.y * g.y;
+      im += v.x * g.y - v.y * g.x;
+    }
+    dWre[t] += re;
+    dWim[t] += im;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// inverse z transform + pointwise linear + GELU; one CTA per (b, x, y) row,
+// one thread per z
+// ---------------------------------------------------------------------------
+
+template <typename ACT>
+__global__ void k_layer_out(int W, int X, int Y, int Z, int m, const ACT* vin, const float2* Uxy, const ACT* A,
+                            const float* a, int apply_gelu, ACT* pre_out, ACT* vout) {
+  extern __shared__ float sh[];
+  float* sA = sh;                                   // W*W
+  float* sa = sA + W * W;                           // W
+  float2* sU = reinterpret_cast<float2*>(sa + W);   // W*m
+  const int row = blockIdx.x;                        // (b, x, y)
+  const int y = row % Y;
+  const int x = (row / Y) % X;
+  const int b = row / (X * Y);
+  const size_t ncell = (size_t)X * Y * Z;
+  for (int i = threadIdx.x; i < W * W; i += blockDim.x) sA[i] = ld(A + i);
+  for (int i = threadIdx.x; i < W; i += blockDim.x) sa[i] = a[i];
+  for (int i = threadIdx.x; i < W * m; i += blockDim.x) {
+    const int co = i / m, k = i - co * m;
+    sU[i] = Uxy[((((size_t)b * W + co) * X + x) * Y + y) * m + k];
+  }
+  __syncthreads();
+  const int z = threadIdx.x;
+  if (z >= Z) return;
+  const size_t base = (size_t)b * W * ncell + ((size_t)x * Y + y) * Z + z;
+  float v[kMaxWidth];
+  for (int ci = 0; ci < W; ++ci) v[ci] = ld(vin + base + (size_t)ci * ncell);
+  float cs[16], sn[16];
+  const float inv = 1.0f / (float)ncell;
+  for (int k = 0; k < m; ++k) {
+    float s, c;
+    sincospif(2.0f * (float)((k * z) % Z) / (float)Z, &s, &c);
+    const float w = (k == 0 ? 1.0f : 2.0f) * inv;
+    cs[k] = c * w;
+    sn[k] = s * w;
+  }
+  for (int co = 0; co < W; ++co) {
+    float acc = sa[co];
+    for (int ci = 0; ci < W; ++ci) acc += sA[co * W + ci] * v[ci];
+    for (int k = 0; k < m; ++k) {
+      const float2 u = sU[co * m + k];
+      acc += u.x * cs[k] - u.y * sn[k];
+    }
+    pre_out[base + (size_t)co * ncell] = st<ACT>(acc);
+    vout[base + (size_t)co * ncell] = st<ACT>(apply_gelu ? gelu(acc) : acc);
+  }
+}
+
+// Backward of k_layer_out for one (b, x, y) row:
+//   gpre = gout * GELU'(pre);  gin = A^T gpre (pointwise part);
+//   dUxy[co][k] = sum_z gpre[co][z] (c_k / XYZ) e^{-2 pi i k z / Z}
+template <typename ACT>
+__global__ void k_layer_out_bwd(int W, int X, int Y, int Z, int m, const float* gout, const ACT* pre, const ACT* A,
+                                int apply_gelu, float* gpre, float* gin, float2* dUxy) {
+  extern __shared__ float sh[];
+  float* sA = sh;                                         // W*W
+  float* sg = sA + W * W;                                 // W*Z gpre of the row
+  float2* stw = reinterpret_cast<float2*>(sg + W * Z);    // m*Z: e^{-2 pi i k z / Z}
+  const int row = blockIdx.x;
+  const int y = row % Y;
+  const int x = (row / Y) % X;
+  const int b = row / (X * Y);
+  const size_t ncell = (size_t)X * Y * Z;
+  for (int i = threadIdx.x; i < W * W; i += blockDim.x) sA[i] = ld(A + i);
+  for (int i = threadIdx.x; i < m * Z; i += blockDim.x) {
+    const int k = i / Z, zz = i - k * Z;
+    float s, c;
+    sincospif(2.0f * (float)((k * zz) % Z) / (float)Z, &s, &c);
+    stw[i] = make_float2(c, -s);
+  }
+  const int z = threadIdx.x;
+  const size_t base = (size_t)b * W * ncell + ((size_t)x * Y + y) * Z + z;
+  if (z < Z) {
+    for (int co = 0; co < W; ++co) {
+      float g = gout[base + (size_t)co * ncell];
+      if (apply_gelu) g *= gelu_grad(ld(pre + base + (size_t)co * ncell));
+      gpre[base + (size_t)co * ncell] = g;
+      sg[co * Z + z] = g;
+    }
+  }
+  __syncthreads();
+  if (z < Z) {
+    for (int ci = 0; ci < W; ++ci) {
+      float acc = 0.0f;
+      for (int co = 0; co < W; ++co) acc += sA[co * W + ci] * sg[co * Z + z];
+      gin[base + (size_t)ci * ncell] = acc;
+    }
+  }
+  // spectral gradient of the row: W*m complex sums over z
+  const float inv = 1.0f / (float)ncell;
+  for (int i = threadIdx.x; i < W * m; i += blockDim.x) {
+    const int co = i / m, k = i - co * m;
+    float re = 0.0f, im = 0.0f;
+    for (int zz = 0; zz < Z; ++zz) {
+      const float2 w = stw[k * Z + zz];
+      const float g = sg[co * Z + zz];
+      re += g * w.x;
+      im += g * w.y;
+    }
+    const float w = (k == 0 ? 1.0f : 2.0f) * inv;
+    dUxy[((((size_t)b * W + co) * X + x) * Y + y) * m + k] = make_float2(re * w, im * w);
+  }
+}
+
+// dA[co][ci] += sum_cells gpre[co] v[ci];  da[co] += sum gpre[co]
+// One CTA of W*W threads per chunk of cells; tiles staged in shared memory.
+template <typename ACT>
+__global__ void k_pointwise_wgrad(int B, size_t ncell, int W, const float* gpre, const ACT* v, float* dA, float* da,
+                                  size_t chunk) {
+  constexpr int T = 32;
+  __shared__ float sg[kMaxWidth][T + 1], sv[kMaxWidth][T + 1];
+  const int tid = threadIdx.x;
+  const int co = tid / W, ci = tid - (tid / W) * W;
+  const size_t total = (size_t)B * ncell;
+  const size_t begin = blockIdx.x * chunk;
+  const size_t end = begin + chunk < total ? begin + chunk : total;
+  float acc = 0.0f, accb = 0.0f;
+  for (size_t t0 = begin; t0 < end; t0 += T) {
+    for (int i = tid; i < W * T; i += blockDim.x) {
+      const int c = i / T, k = i - c * T;
+      const size_t t = t0 + k;
+      float g = 0.0f, vv = 0.0f;
+      if (t < end) {
+        const int b = (int)(t / ncell);
+        const size_t cell = t - (size_t)b * ncell;
+        g = gpre[((size_t)b * W + c) * ncell + cell];
+        vv = ld(v + ((size_t)b * W + c) * ncell + cell);
+      }
+      sg[c][k] = g;
+      sv[c][k] = vv;
+    }
+    __syncthreads();
+    if (tid < W * W) {
+#pragma unroll 8
+      for (int k = 0; k < T; ++k) acc += sg[co][k] * sv[ci][k];
+      if (ci == 0)
+        for (int k = 0; k < T; ++k) accb += sg[co][k];
+    }
+    __syncthreads();
+  }
+  if (tid < W * W) {
+    atomicAdd(&dA[co * W + ci], acc);
+    if (ci == 0) atomicAdd(&da[co], accb);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// projection width -> 6 and u = f + out
+// ---------------------------------------------------------------------------
+
+template <typename ACT>
+__global__ void k_project(int B, size_t ncell, int W, const ACT* v, const ACT* Q, const float* qb, const float2* wave,
+                          float2* u) {
+  __shared__ float sQ[6 * kMaxWidth], sq[6];
+  for (int i = threadIdx.x; i < 6 * W; i += blockDim.x) sQ[i] = ld(Q + i);
+  if (threadIdx.x < 6) sq[threadIdx.x] = qb[threadIdx.x];
+  __syncthreads();
+  const size_t total = (size_t)B * ncell;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(t / ncell);
+    const size_t cell = t - (size_t)b * ncell;
+    float o[6];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) o[j] = sq[j];
+    for (int ci = 0; ci < W; ++ci) {
+      const float vv = ld(v + ((size_t)b * W + ci) * ncell + cell);
+#pragma unroll
+      for (int j = 0; j < 6; ++j) o[j] += sQ[j * W + ci] * vv;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t idx = ((size_t)b * 3 + c) * ncell + cell;
+      const float2 f = wave[idx];
+      u[idx] = make_float2(f.x + o[2 * c], f.y + o[2 * c + 1]);
+    }
+  }
+}
+
+// du: gradient wrt u (dL/dRe + i dL/dIm).  gv = Q^T dout; dQ += dout v; dqb += dout
+template <typename ACT>
+__global__ void k_project_bwd(int B, size_t ncell, int W, const ACT* v, const ACT* Q, const float2* du, float* gv,
+                              float* dQ, float* dqb) {
+  __shared__ float sQ[6 * kMaxWidth];
+  __shared__ float acc[6 * (kMaxWidth + 1)];
+  for (int i = threadIdx.x; i < 6 * W; i += blockDim.x) sQ[i] = ld(Q + i);
+  for (int i = threadIdx.x; i < 6 * (W + 1); i += blockDim.x) acc[i] = 0.0f;
+  __syncthreads();
+  const size_t total = (size_t)B * ncell;
+  float lQ[6 * (kMaxWidth + 1)];
+  for (int i = 0; i < 6 * (W + 1); ++i) lQ[i] = 0.0f;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(t / ncell);
+    const size_t cell = t - (size_t)b * ncell;
+    float d[6];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float2 g = du[((size_t)b * 3 + c) * ncell + cell];
+      d[2 * c] = g.x;
+      d[2 * c + 1] = g.y;
+    }
+    for (int ci = 0; ci < W; ++ci) {
+      const float vv = ld(v + ((size_t)b * W + ci) * ncell + cell);
+      float g = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        g += sQ[j * W + ci] * d[j];
+        lQ[j * (W + 1) + ci] += d[j] * vv;
+      }
+      gv[((size_t)b * W + ci) * ncell + cell] = g;
+    }
+#pragma unroll
+    for (int j = 0; j < 6; ++j) lQ[j * (W + 1) + W] += d[j];
+  }
+  for (int i = 0; i < 6 * (W + 1); ++i) {
+    float val = lQ[i];
+    for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&acc[i], val);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 6 * (W + 1); i += blockDim.x) {
+    const int j = i / (W + 1), k = i - j * (W + 1);
+    if (k < W) atomicAdd(&dQ[j * W + k], acc[i]);
+    else atomicAdd(&dqb[j], acc[i]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// loss: mean_b ||pred_b - t_b||^2 / ||t_b||^2 and its gradient
+// ---------------------------------------------------------------------------
+
+__global__ void k_loss_terms(int B, size_t n, const float2* pred, const float2* target, double* terms) {
+  // terms[2b] = ||pred_b - t_b||^2, terms[2b+1] = ||t_b||^2  (atomic FP64 accumulation)
+  const int b = blockIdx.y;
+  double num = 0.0, den = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float2 p = pred[(size_t)b * n + i], t = target[(size_t)b * n + i];
+    const double dx = (double)p.x - t.x, dy = (double)p.y - t.y;
+    num += dx * dx + dy * dy;
+    den += (double)t.x * t.x + (double)t.y * t.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    num += __shfl_xor_sync(0xffffffffu, num, o);
+    den += __shfl_xor_sync(0xffffffffu, den, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&terms[2 * b], num);
+    atomicAdd(&terms[2 * b + 1], den);
+  }
+}
+
+__global__ void k_loss_grad(int B, size_t n, const float2* pred, const float2* target, const double* terms,
+                            float2* grad) {
+  const int b = blockIdx.y;
+  const float s = (float)(2.0 / (terms[2 * b + 1] * B));
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float2 p = pred[(size_t)b * n + i], t = target[(size_t)b * n + i];
+    grad[(size_t)b * n + i] = make_float2(s * (p.x - t.x), s * (p.y - t.y));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Adam on FP32 master weights, writing the ACT copy used by the kernels
+// ---------------------------------------------------------------------------
+
+template <typename ACT>
+__global__ void k_adam(size_t n, float* w, const float* g, float* m1, float* m2, float lr, float b1, float b2,
+                       float eps, float bc1, float bc2, ACT* wact) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.0f - b1) * gi;
+    const float v = b2 * m2[i] + (1.0f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = v;
+    const float upd = lr * (a / bc1) / (sqrtf(v / bc2) + eps);
+    const float nw = w[i] - upd;
+    w[i] = nw;
+    if (wact) wact[i] = st<ACT>(nw);
+  }
+}
+
+template <typename ACT> __global__ void k_cast(size_t n, const float* src, ACT* dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = st<ACT>(src[i]);
+}
+
+template <typename ACT> __global__ void k_uncast(size_t n, const ACT* src, float* dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = ld(src + i);
+}
+
+inline int blocks_for(size_t n, int threads = 256) {
+  size_t b = (n + threads - 1) / threads;
+  if (b > (size_t)148 * 32) b = (size_t)148 * 32;
+  return (int)(b ? b : 1);
+}
+
+}  // namespace fno
+}  // namespace em3d
+
+using namespace em3d;
+using namespace em3d::fno;
+
+enum { FNO_BF16 = 0, FNO_F32 = 1 };
+
+#define FNO_DISPATCH(act, CALL)                                                    \
+  do {                                                                             \
+    if ((act) == FNO_BF16) { using ACT = __nv_bfloat16; CALL; }                   \
+    else if ((act) == FNO_F32) { using ACT = float; CALL; }                       \
+    else { em3d_set_last_error("act dtype must be 0 (bf16) or 1 (float)"); return EM3D_ERR_INVALID; } \
+  } while (0)
+
+static int check_width(int W) {
+  if (W < 1 || W > kMaxWidth) { em3d_set_last_error("FNO width must be in [1, 32]"); return EM3D_ERR_INVALID; }
+  return EM3D_OK;
+}
+
+extern "C" {
+
+int em3d_fno_lift(int act, int B, size_t ncell, int W, const void* chi, const void* wave, const void* P,
+                  const float* pb, void* v0, void* stream) {
+  if (int rc = check_width(W)) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  FNO_DISPATCH(act, (k_lift<ACT><<<blocks_for((size_t)B * ncell), 256, 0, st>>>(
+                         B, ncell, W, (const float2*)chi, (const float2*)wave, (const ACT*)P, pb, (ACT*)v0)));
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_lift_bwd(int B, size_t ncell, int W, const void* chi, const void* wave, const float* dv0, float* dP,
+                      float* dpb, void* stream) {
+  if (int rc = check_width(W)) return rc;
+  k_lift_bwd<<<blocks_for((size_t)B * ncell) / 8 + 1, 256, 0, (cudaStream_t)stream>>>(
+      B, ncell, W, (const float2*)chi, (const float2*)wave, dv0, dP, dpb);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_contract(int kind, int act, size_t outer, int L, int J, int inner, const void* X, const void* M, void* Y,
+                      void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = outer * (size_t)J * inner;
+  if (kind == 0) {
+    FNO_DISPATCH(act, (k_contract_r2c<ACT><<<blocks_for(n), 256, 0, st>>>(outer, L, J, inner, (const ACT*)X,
+                                                                           (const float2*)M, (float2*)Y)));
+  } else if (kind == 1) {
+    k_contract_c2c<<<blocks_for(n), 256, 0, st>>>(outer, L, J, inner, (const float2*)X, (const float2*)M, (float2*)Y);
+  } else if (kind == 2) {
+    k_contract_c2r_acc<<<blocks_for(n), 256, 0, st>>>(outer, L, J, inner, (const float2*)X, (const float2*)M,
+                                                      (float*)Y);
+  } else {
+    em3d_set_last_error("contract kind must be 0 (real->complex), 1 (complex), 2 (complex->real, accumulate)");
+    return EM3D_ERR_INVALID;
+  }
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_modemix(int act, int B, int W, int nm, const void* V, const void* Wre, const void* Wim, void* U,
+                     void* stream) {
+  if (int rc = check_width(W)) return rc;
+  FNO_DISPATCH(act, (k_modemix<ACT><<<blocks_for((size_t)B * W * nm), 256, 0, (cudaStream_t)stream>>>(
+                         B, W, nm, (const float2*)V, (const ACT*)Wre, (const ACT*)Wim, (float2*)U)));
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_modemix_bwd(int act, int B, int W, int nm, const void* V, const void* dU, const void* Wre,
+                         const void* Wim, void* dV, float* dWre, float* dWim, void* stream) {
+  if (int rc = check_width(W)) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  FNO_DISPATCH(act, (k_modemix_bwd_v<ACT><<<blocks_for((size_t)B * W * nm), 256, 0, st>>>(
+                         B, W, nm, (const float2*)dU, (const ACT*)Wre, (const ACT*)Wim, (float2*)dV)));
+  EM3D_LAUNCH_CHECK();
+  k_modemix_bwd_w<<<blocks_for((size_t)W * W * nm), 256, 0, st>>>(B, W, nm, (const float2*)V, (const float2*)dU,
+                                                                   dWre, dWim);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_layer_out(int act, int B, int W, int X, int Y, int Z, int m, const void* vin, const void* Uxy,
+                       const void* A, const float* a, int apply_gelu, void* pre, void* vout, void* stream) {
+  if (int rc = check_width(W)) return rc;
+  if (Z > 1024 || m > 16 || m < 1) { em3d_set_last_error("FNO needs Z <= 1024 and 1 <= modes <= 16"); return EM3D_ERR_INVALID; }
+  const size_t smem = (size_t)(W * W + W) * sizeof(float) + (size_t)W * m * sizeof(float2);
+  const int threads = ((Z + 31) / 32) * 32;
+  FNO_DISPATCH(act, (k_layer_out<ACT><<<B * X * Y, threads, smem, (cudaStream_t)stream>>>(
+                         W, X, Y, Z, m, (const ACT*)vin, (const float2*)Uxy, (const ACT*)A, a, apply_gelu,
+                         (ACT*)pre, (ACT*)vout)));
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_layer_out_bwd(int act, int B, int W, int X, int Y, int Z, int m, const float* gout, const void* pre,
+                           const void* A, int apply_gelu, float* gpre, float* gin, void* dUxy, void* stream) {
+  if (int rc = check_width(W)) return rc;
+  if (Z > 1024 || m > 16 || m < 1) { em3d_set_last_error("FNO needs Z <= 1024 and 1 <= modes <= 16"); return EM3D_ERR_INVALID; }
+  const size_t smem = (size_t)(W * W + W * Z) * sizeof(float) + (size_t)m * Z * sizeof(float2);
+  if (smem > 200 * 1024) { em3d_set_last_error("FNO row too long for shared memory"); return EM3D_ERR_INVALID; }
+  const int threads = ((Z + 31) / 32) * 32;
+  if (act == FNO_BF16) {
+    auto kern = k_layer_out_bwd<__nv_bfloat16>;
+    EM3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    kern<<<B * X * Y, threads, smem, (cudaStream_t)stream>>>(W, X, Y, Z, m, gout, (const __nv_bfloat16*)pre,
+                                                              (const __nv_bfloat16*)A, apply_gelu, gpre, gin,
+                                                              (float2*)dUxy);
+  } else if (act == FNO_F32) {
+    auto kern = k_layer_out_bwd<float>;
+    EM3D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    kern<<<B * X * Y, threads, smem, (cudaStream_t)stream>>>(W, X, Y, Z, m, gout, (const float*)pre, (const float*)A,
+                                                              apply_gelu, gpre, gin, (float2*)dUxy);
+  } else {
+    em3d_set_last_error("act dtype must be 0 (bf16) or 1 (float)");
+    return EM3D_ERR_INVALID;
+  }
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_pointwise_wgrad(int act, int B, size_t ncell, int W, const float* gpre, const void* v, float* dA,
+                             float* da, void* stream) {
+  if (int rc = check_width(W)) return rc;
+  const size_t total = (size_t)B * ncell;
+  const size_t chunk = 4096;
+  const int grid = (int)((total + chunk - 1) / chunk);
+  const int threads = ((W * W + 31) / 32) * 32;
+  FNO_DISPATCH(act, (k_pointwise_wgrad<ACT><<<grid, threads, 0, (cudaStream_t)stream>>>(B, ncell, W, gpre,
+                                                                                         (const ACT*)v, dA, da,
+                                                                                         chunk)));
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_project(int act, int B, size_t ncell, int W, const void* v, const void* Q, const float* qb,
+                     const void* wave, void* u, void* stream) {
+  if (int rc = check_width(W)) return rc;
+  FNO_DISPATCH(act, (k_project<ACT><<<blocks_for((size_t)B * ncell), 256, 0, (cudaStream_t)stream>>>(
+                         B, ncell, W, (const ACT*)v, (const ACT*)Q, qb, (const float2*)wave, (float2*)u)));
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_project_bwd(int act, int B, size_t ncell, int W, const void* v, const void* Q, const void* du,
+                         float* gv, float* dQ, float* dqb, void* stream) {
+  if (int rc = check_width(W)) return rc;
+  FNO_DISPATCH(act, (k_project_bwd<ACT><<<blocks_for((size_t)B * ncell) / 8 + 1, 256, 0, (cudaStream_t)stream>>>(
+                         B, ncell, W, (const ACT*)v, (const ACT*)Q, (const float2*)du, gv, dQ, dqb)));
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_loss(int B, size_t n, const void* pred, const void* target, double* terms, void* grad, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  EM3D_CUDA_TRY(cudaMemsetAsync(terms, 0, sizeof(double) * 2 * B, st));
+  const dim3 grid(blocks_for(n) < 296 ? blocks_for(n) : 296, B);
+  k_loss_terms<<<grid, 256, 0, st>>>(B, n, (const float2*)pred, (const float2*)target, terms);
+  EM3D_LAUNCH_CHECK();
+  if (grad) {
+    const dim3 g2(blocks_for(n), B);
+    k_loss_grad<<<g2, 256, 0, st>>>(B, n, (const float2*)pred, (const float2*)target, terms, (float2*)grad);
+    EM3D_LAUNCH_CHECK();
+  }
+  return EM3D_OK;
+}
+
+int em3d_fno_adam(int act, size_t n, float* w, const float* g, float* m1, float* m2, float lr, float b1, float b2,
+                  float eps, int step, void* wact, void* stream) {
+  if (step < 1) { em3d_set_last_error("adam step counts from 1"); return EM3D_ERR_INVALID; }
+  const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
+  FNO_DISPATCH(act, (k_adam<ACT><<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(n, w, g, m1, m2, lr, b1, b2, eps,
+                                                                                  bc1, bc2, (ACT*)wact)));
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_cast(int act, size_t n, const float* src, void* dst, void* stream) {
+  FNO_DISPATCH(act, (k_cast<ACT><<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(n, src, (ACT*)dst)));
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_uncast(int act, size_t n, const void* src, float* dst, void* stream) {
+  FNO_DISPATCH(act, (k_uncast<ACT><<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(n, (const ACT*)src, dst)));
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+}  // extern "C"

@@ -205,7 +205,8 @@ class _Engine:
         if not isinstance(rhs, torch.Tensor):
             rhs = torch.as_tensor(np.asarray(rhs))
         tc = self.be.precision.torch_complex if hasattr(self.be, "precision") else rhs.dtype
-        self.rhs = rhs.to(device=self.be.torch_device, dtype=tc).contiguous()
+        self.rhs = torch.empty(rhs.shape, dtype=tc, device=self.be.torch_device)
+        self.rhs.copy_(rhs)
         self.batch = int(batch)
         self.n = int(self.rhs.numel()) // self.batch
         self.dt = _native_dtype(self.rhs)
@@ -214,6 +215,13 @@ class _Engine:
         if self.batch > 1 and not self.native_op:
             raise TypeError("batched solves need an operator with apply_into (em3d_b200.Operator / AcousticOperator)")
         self.lib = _lib.load()
+        self.graph = None
+        self.per_replay = 0
+        self.vectors = {}
+
+    def load_rhs(self, rhs):
+        """Reuse this engine (its buffers and captured graph) for a new right-hand side."""
+        self.rhs.copy_(rhs.reshape(self.rhs.shape))
 
     def vec(self):
         import torch
@@ -223,9 +231,12 @@ class _Engine:
     def stream(self):
         return _lib.stream_handle()
 
-    def apply(self, x, out, adjoint=False):
+    def apply(self, x, out, adjoint=False, skip=True):
+        """``out = A x`` (or ``A* x``).  Inside the iteration the batch-wide done
+        flag is the skip flag; set-up calls pass ``skip=False`` because the
+        state may still hold the previous solve's flags."""
         if self.native_op:
-            self.op.apply_into(x, out, adjoint=adjoint, skip_ptr=self.state.done_ptr)
+            self.op.apply_into(x, out, adjoint=adjoint, skip_ptr=self.state.done_ptr if skip else None)
         else:
             import torch
 
@@ -256,12 +267,10 @@ class _Engine:
 
         if self.state.done():
             return
-        iteration()
-        if self.state.done():
-            return
-        graph = None
-        per_replay = 0
-        if use_graph and self.native_op:
+        if self.graph is None and use_graph and self.native_op:
+            iteration()  # the first iteration runs eagerly (and loads the kernels)
+            if self.state.done():
+                return
             before = _lib.launch_count
             try:
                 graph = torch.cuda.CUDAGraph()
@@ -271,20 +280,18 @@ class _Engine:
                     for _ in range(chunk):
                         iteration()
                 torch.cuda.current_stream().wait_stream(side)
+                self.graph = graph
             except RuntimeError:
-                graph = None
-            per_replay = _lib.launch_count - before
+                self.graph = None
+            self.per_replay = _lib.launch_count - before
             _lib.launch_count = before  # captured, not launched
         while not self.state.done():
-            if graph is not None:
-                graph.replay()
-                _lib.launch_count += per_replay
+            if self.graph is not None:
+                self.graph.replay()
+                _lib.launch_count += self.per_replay
             else:
                 for _ in range(chunk if self.native_op else 1):
                     iteration()
-        if graph is not None:
-            torch.cuda.current_stream().synchronize()
-            del graph
 
 
 def _status_name(code: int) -> str:
@@ -317,13 +324,16 @@ def _budget(v):
     return -1 if v is None else int(v)
 
 
-def _init_u(eng, x0):
+def _load_u(buf, x0):
+    """Initial iterate in a reused buffer: zero, or a copy of ``x0``."""
     import torch
 
     if x0 is None:
-        return eng.vec()
-    x = x0 if isinstance(x0, torch.Tensor) else torch.as_tensor(np.asarray(x0))
-    return x.to(device=eng.rhs.device, dtype=eng.rhs.dtype).reshape(eng.rhs.shape).clone()
+        buf.zero_()
+    else:
+        x = x0 if isinstance(x0, torch.Tensor) else torch.as_tensor(np.asarray(x0))
+        buf.copy_(x.to(device=buf.device, dtype=buf.dtype).reshape(buf.shape))
+    return buf
 
 
 def _batch_of(operator, rhs) -> int:
@@ -339,7 +349,35 @@ def _batch_of(operator, rhs) -> int:
 
 class _KrylovSolver:
     """``solve(operator, rhs)`` for one right-hand side (the reference's API) and
-    ``solve_batch(operator, rhs)`` for a stack of them sharing the operator."""
+    ``solve_batch(operator, rhs)`` for a stack of them sharing the operator.
+
+    Repeated solves with the same operator and shape reuse the device buffers
+    and the captured CUDA graph of the iteration (the solver configuration is
+    re-read at every solve)."""
+
+    def _engine(self, operator, rhs, hist_cap, batch):
+        import weakref
+
+        if not hasattr(self, "_engines"):
+            self._engines = {}
+        key = (id(operator), tuple(rhs.shape), str(rhs.dtype), batch, hist_cap)
+        hit = self._engines.get(key)
+        if hit is not None and hit[0]() is operator:
+            eng = hit[1]
+            eng.load_rhs(rhs)
+            return eng
+        eng = _Engine(operator, rhs, hist_cap=hist_cap, batch=batch)
+        if hasattr(operator, "apply_into"):
+            self._engines = {k: v for k, v in self._engines.items() if v[0]() is not None}
+            self._engines[key] = (weakref.ref(operator), eng)
+        return eng
+
+    def _vec(self, eng, name):
+        v = eng.vectors.get(name)
+        if v is None:
+            v = eng.vec()
+            eng.vectors[name] = v
+        return v
 
     def solve(self, operator, rhs, x0=None) -> SolverResult:
         import torch
@@ -357,6 +395,7 @@ class _KrylovSolver:
 
     def _results(self, eng, u, trivial):
         out = []
+        u = u.clone()  # the engine's buffer is reused by the next solve
         for b, (st, hist, counts) in enumerate(eng.state.download()):
             ub = u if eng.batch == 1 else u[b]
             if trivial[b]:
@@ -376,12 +415,12 @@ class BiCGStab(_KrylovSolver):
 
     def _solve(self, operator, rhs, x0, batch):
         cfg = self.cfg
-        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2, batch=batch)
+        eng = self._engine(operator, rhs, int(cfg.max_iter) + 2, batch)
         rhs = eng.rhs
         rhs_norms = eng.norms(rhs)
-        u = _init_u(eng, x0)
-        r = eng.vec()
-        eng.apply(u, r)
+        u = _load_u(self._vec(eng, "u"), x0)
+        r = self._vec(eng, "r")
+        eng.apply(u, r, skip=False)
         _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, rhs.data_ptr(), -1.0, 0.0,
                   r.data_ptr(), eng.stream())
         rr = eng.norms(r)
@@ -414,8 +453,9 @@ class BiCGStab(_KrylovSolver):
             hists.append([rel0])
             counts.append([1])
         eng.state.upload(hists, counts)
-        r_hat = r.clone()
-        p, v, s, t = eng.vec(), eng.vec(), eng.vec(), eng.vec()
+        r_hat = self._vec(eng, "r_hat")
+        r_hat.copy_(r)
+        p, v, s, t = (self._vec(eng, k) for k in ("p", "v", "s", "t"))
 
         def iteration():
             eng.step("em3d_bicgstab_p", r.data_ptr(), p.data_ptr(), v.data_ptr())
@@ -447,7 +487,7 @@ class SIM(_KrylovSolver):
 
     def _solve(self, operator, rhs, x0, batch):
         cfg = self.cfg
-        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2, batch=batch)
+        eng = self._engine(operator, rhs, int(cfg.max_iter) + 2, batch)
         rhs = eng.rhs
         rhs_norms = eng.norms(rhs)
         gamma = 1.0 / complex(cfg.mu)
@@ -462,8 +502,8 @@ class SIM(_KrylovSolver):
             st.iter = st.matvecs = st.rmatvecs = 0
             st.status = 1 if trivial[b] else 0
         eng.state.upload()
-        u = _init_u(eng, x0)
-        res = eng.vec()
+        u = _load_u(self._vec(eng, "u"), x0)
+        res = self._vec(eng, "res")
 
         def iteration():
             eng.apply(u, res)
@@ -488,7 +528,7 @@ class TwoStep(_KrylovSolver):
 
     def _solve(self, operator, rhs, x0, batch):
         cfg = self.cfg
-        eng = _Engine(operator, rhs, hist_cap=int(cfg.max_iter) + 2, batch=batch)
+        eng = self._engine(operator, rhs, int(cfg.max_iter) + 2, batch)
         rhs = eng.rhs
         rhs_norms = eng.norms(rhs)
         trivial = [bool(nrm == 0.0) for nrm in rhs_norms]
@@ -502,8 +542,8 @@ class TwoStep(_KrylovSolver):
             st.first = 1
             st.status = 1 if trivial[b] else 0
         eng.state.upload()
-        u = _init_u(eng, x0)
-        up, r, rp, g, hg = eng.vec(), eng.vec(), eng.vec(), eng.vec(), eng.vec()
+        u = _load_u(self._vec(eng, "u"), x0)
+        up, r, rp, g, hg = (self._vec(eng, k) for k in ("up", "r", "rp", "g", "hg"))
 
         def iteration():
             eng.apply(u, r)
@@ -597,21 +637,43 @@ class DefectCorrection:
         t = t.reshape((b,) + tuple(operator._field_shape()))
         return self._solve(operator, t, x0, b, operator_low)
 
-    def _solve(self, operator, rhs, x0, batch, operator_low):
+    def _buffers(self, operator, rhs, batch, operator_low):
+        """Engine, buffers, FP32 operator and inner solver, reused across solves
+        with the same operator and shape."""
+        import weakref
+
         import torch
 
         from .backend import Precision
 
-        cfg = self.cfg
-        op_lo = operator_low if operator_low is not None else operator.with_precision(Precision.SINGLE)
+        if not hasattr(self, "_cache"):
+            self._cache = {}
+        key = (id(operator), tuple(rhs.shape), batch)
+        hit = self._cache.get(key)
+        if hit is not None and hit["op"]() is operator and (operator_low is None or hit["op_lo"] is operator_low):
+            hit["eng"].load_rhs(rhs)
+            return hit
         eng = _Engine(operator, rhs, hist_cap=4, batch=batch)
+        op_lo = operator_low if operator_low is not None else operator.with_precision(Precision.SINGLE)
+        inner_cls = BiCGStab if self.inner == "bicgstab" else TwoStep
+        hit = {"op": weakref.ref(operator), "op_lo": op_lo, "eng": eng, "u": eng.vec(), "r": eng.vec(),
+               "r_lo": torch.empty(eng.rhs.shape, dtype=torch.complex64, device=eng.rhs.device),
+               "inner": inner_cls(SolverConfig())}
+        self._cache = {k: v for k, v in self._cache.items() if v["op"]() is not None}
+        self._cache[key] = hit
+        return hit
+
+    def _solve(self, operator, rhs, x0, batch, operator_low):
+        cfg = self.cfg
+        buf = self._buffers(operator, rhs, batch, operator_low)
+        eng, op_lo, inner = buf["eng"], buf["op_lo"], buf["inner"]
         f = eng.rhs
         fn = eng.norms(f)
         fs = np.where(fn == 0.0, 1.0, fn)
         tol = np.maximum(float(cfg.rtol), float(cfg.atol) / fs)
-        u = _init_u(eng, x0)
-        r = eng.vec()
-        r_lo = torch.empty(f.shape, dtype=torch.complex64, device=f.device)
+        u = _load_u(buf["u"], x0)
+        r = buf["r"]
+        r_lo = buf["r_lo"]
         hist = [[] for _ in range(batch)]
         counts = [[] for _ in range(batch)]
         status = [("converged" if fn[b] == 0.0 else None) for b in range(batch)]
@@ -619,7 +681,6 @@ class DefectCorrection:
         mv32 = np.zeros(batch, dtype=int)
         rmv32 = np.zeros(batch, dtype=int)
         inner_its = [[] for _ in range(batch)]
-        inner_cls = BiCGStab if self.inner == "bicgstab" else TwoStep
         budget_inner = int(self.inner_max_iter or cfg.max_iter)
         for outer in range(self.max_outer + 1):
             operator.apply_into(u, r)
@@ -653,8 +714,8 @@ class DefectCorrection:
                 for b in range(batch):
                     if status[b] is not None:
                         r_lo[b].zero_()
-            solver = inner_cls(SolverConfig(max_iter=budget_inner, rtol=target))
-            res = solver.solve(op_lo, r_lo) if batch == 1 else solver.solve_batch(op_lo, r_lo)
+            inner.cfg = SolverConfig(max_iter=budget_inner, rtol=target)
+            res = inner.solve(op_lo, r_lo) if batch == 1 else inner.solve_batch(op_lo, r_lo)
             for b in running:
                 mv32[b] += res[b].matvec_count if batch > 1 else res.matvec_count
                 rmv32[b] += res[b].rmatvec_count if batch > 1 else res.rmatvec_count
@@ -665,6 +726,7 @@ class DefectCorrection:
             _lib.call("em3d_vec_convert", eng.n * batch, _lib.EM3D_C64, d.data_ptr(), eng.dt, u.data_ptr(), 1,
                       eng.stream())
         out = []
+        u = u.clone()  # the cached buffer is reused by the next solve
         for b in range(batch):
             ub = u if batch == 1 else u[b]
             h = hist[b] if hist[b] else [0.0]

@@ -245,6 +245,39 @@ int em3d_twostep_coeffs(int dtype, size_t n, int batch, void* state, size_t stat
 int em3d_twostep_update(int dtype, size_t n, int batch, void* state, size_t state_stride, void* u, void* u_prev, const void* r, void* r_prev,
                         const void* g, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Fourier-neural-operator warm start (no counterpart in the reference: the
+ * learned initial guess for the solvers).  Activations/weights in `act`
+ * (0 = bf16, 1 = float), FP32 accumulation; channel tensors (B, C, X, Y, Z);
+ * mode-space tensors complex64.  See em3d_b200/csrc/fno.cu for the network.
+ * ------------------------------------------------------------------------ */
+int em3d_fno_lift(int act, int B, size_t ncell, int W, const void* chi, const void* wave, const void* P,
+                  const float* pb, void* v0, void* stream);
+int em3d_fno_lift_bwd(int B, size_t ncell, int W, const void* chi, const void* wave, const float* dv0, float* dP,
+                      float* dpb, void* stream);
+/* kind 0: real(act) -> complex; 1: complex -> complex; 2: complex -> real, += Re(.) */
+int em3d_fno_contract(int kind, int act, size_t outer, int L, int J, int inner, const void* X, const void* M, void* Y,
+                      void* stream);
+int em3d_fno_modemix(int act, int B, int W, int nm, const void* V, const void* Wre, const void* Wim, void* U,
+                     void* stream);
+int em3d_fno_modemix_bwd(int act, int B, int W, int nm, const void* V, const void* dU, const void* Wre,
+                         const void* Wim, void* dV, float* dWre, float* dWim, void* stream);
+int em3d_fno_layer_out(int act, int B, int W, int X, int Y, int Z, int m, const void* vin, const void* Uxy,
+                       const void* A, const float* a, int apply_gelu, void* pre, void* vout, void* stream);
+int em3d_fno_layer_out_bwd(int act, int B, int W, int X, int Y, int Z, int m, const float* gout, const void* pre,
+                           const void* A, int apply_gelu, float* gpre, float* gin, void* dUxy, void* stream);
+int em3d_fno_pointwise_wgrad(int act, int B, size_t ncell, int W, const float* gpre, const void* v, float* dA,
+                             float* da, void* stream);
+int em3d_fno_project(int act, int B, size_t ncell, int W, const void* v, const void* Q, const float* qb,
+                     const void* wave, void* u, void* stream);
+int em3d_fno_project_bwd(int act, int B, size_t ncell, int W, const void* v, const void* Q, const void* du,
+                         float* gv, float* dQ, float* dqb, void* stream);
+int em3d_fno_loss(int B, size_t n, const void* pred, const void* target, double* terms, void* grad, void* stream);
+int em3d_fno_adam(int act, size_t n, float* w, const float* g, float* m1, float* m2, float lr, float b1, float b2,
+                  float eps, int step, void* wact, void* stream);
+int em3d_fno_cast(int act, size_t n, const float* src, void* dst, void* stream);
+int em3d_fno_uncast(int act, size_t n, const void* src, float* dst, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,8 +58,8 @@ def test_batched_solver_matches_single_rhs_solves(solver):
         assert got.matvec_count == single.matvec_count and got.rmatvec_count == single.rmatvec_count
         assert got.residual_action_counts == single.residual_action_counts
         np.testing.assert_allclose(got.residual_history, single.residual_history, rtol=1e-9)
-        if float(torch.linalg.vector_norm(single.u)) > 0:
-            assert rel_err(be.to_host(got.u), be.to_host(single.u)) < 1e-9
+        if float(torch.linalg.vector_norm(single.u)) > 0:  # agreement at the solve tolerance
+            assert rel_err(be.to_host(got.u), be.to_host(single.u)) < 1e-8
     assert batch[-1].status == "converged" and float(torch.linalg.vector_norm(batch[-1].u)) == 0.0
 
 

@@ -174,3 +174,25 @@ def test_x0_warm_start_reaches_same_solution():
     warm = BiCGStab(SolverConfig(max_iter=200, rtol=1e-10)).solve(op, prob.wave, x0=x0)
     assert warm.converged and warm.iterations < cold.iterations
     assert rel_err(be.to_host(warm.u), be.to_host(cold.u)) < 1e-8
+
+
+def test_repeated_solves_reuse_buffers_and_return_fresh_results():
+    """Second and third solves reuse the captured graph and buffers; results
+    of earlier solves are not overwritten and match a fresh solver."""
+    import torch
+
+    from em3d_b200 import workloads
+    from em3d_b200.solvers import BiCGStab, SolverConfig
+
+    be, prob, op = _sphere16("double")
+    waves = torch.as_tensor(workloads.plane_wave_batch(prob.grid.host_axes, 4.0, 2), device="cuda")
+    s = BiCGStab(SolverConfig(max_iter=200, rtol=1e-9))
+    r0 = s.solve(op, waves[0])
+    u0 = r0.u.clone()
+    r1 = s.solve(op, waves[1])
+    r2 = s.solve(op, waves[0])
+    assert torch.equal(r0.u, u0)
+    fresh = BiCGStab(SolverConfig(max_iter=200, rtol=1e-9)).solve(op, waves[1])
+    assert r1.iterations == fresh.iterations and r1.residual_history == fresh.residual_history
+    assert torch.equal(r1.u, fresh.u)
+    assert r2.residual_history == r0.residual_history and torch.equal(r2.u, r0.u)
