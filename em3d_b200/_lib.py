@@ -57,6 +57,10 @@ SIGNATURES = {
     "em3d_em_matvec_static_scratch": (c_int, [_GRID, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                               c_void_p]),
     "em3d_static_scratch_bytes": (c_size_t, []),
+    "em3d_sample_ellipsoids": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int,
+                                       c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
+    "em3d_plane_wave": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_double, c_void_p,
+                                c_void_p, c_double, c_int, c_void_p, c_void_p]),
     "em3d_set_tuning": (c_int, [c_int, c_int]),
     "em3d_get_tuning": (c_int, [c_int]),
     "em3d_fno_lift": (c_int, [c_int, c_int, c_size_t, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
@@ -65,6 +69,9 @@ SIGNATURES = {
                                   c_void_p]),
     "em3d_fno_contract": (c_int, [c_int, c_int, c_size_t, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
                                   c_void_p]),
+    "em3d_fno_row_forward": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_void_p, c_void_p]),
     "em3d_fno_modemix": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "em3d_fno_modemix_bwd": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                      c_void_p, c_void_p, c_void_p]),

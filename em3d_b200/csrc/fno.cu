@@ -523,6 +523,239 @@ template <typename ACT> __global__ void k_uncast(size_t n, const ACT* src, float
     dst[i] = ld(src + i);
 }
 
+// ---------------------------------------------------------------------------
+// Fused z-row kernel of the forward pass (Z <= 128, W <= 32, m <= 16).
+//
+// One group of R = 128 / Z consecutive (b, x, y) rows per step, one thread per
+// cell.  Each thread keeps its cell's channels in registers:
+//   LIFT:  o = P feat + pb                              (feat: 24 per cell)
+//   layer: pre = A v + a + sum_k Re(U[k] (c_k/XYZ) e^{+2 pi i k z/Z});
+//          o = GELU(pre) (identity on the last layer)
+// and writes what the caller asks for: pre (training), o (the next layer's
+// input), the truncated z-DFT of o, Vz[k] = sum_z o[z] e^{-2 pi i k z/Z}
+// (computed from a shared-memory copy of the rows, so the next layer does not
+// re-read o from memory), and/or the projection u = f + Q o + qb.  o is
+// rounded to the activation type before the DFT and the projection, so they
+// see exactly the values a separate pass would read back.
+// ---------------------------------------------------------------------------
+
+constexpr int kMaxModes = 16;
+constexpr int kRowThreads = 128;
+
+template <typename ACT, bool LIFT>
+__global__ void __launch_bounds__(kRowThreads) k_row_fwd(
+    int B, int W, int X, int Y, int Z, int m, const float2* __restrict__ chi, const float2* __restrict__ wave,
+    const ACT* __restrict__ vin, const float2* __restrict__ Uxy, const ACT* __restrict__ Wt,
+    const float* __restrict__ bias, int apply_gelu, ACT* __restrict__ pre_out, ACT* __restrict__ vout,
+    float2* __restrict__ Vz, const ACT* __restrict__ Q, const float* __restrict__ qb, float2* __restrict__ u_out) {
+  constexpr int KIN = LIFT ? kFeat : kMaxWidth;
+  extern __shared__ float sh[];
+  float* sW = sh;                                        // kMaxWidth x KIN
+  float* sb = sW + kMaxWidth * KIN;                      // kMaxWidth
+  float* sQ = sb + kMaxWidth;                            // 6 x kMaxWidth
+  float* sqb = sQ + 6 * kMaxWidth;                       // 8
+  float2* stw = reinterpret_cast<float2*>(sqb + 8);      // m x (Z+1): e^{-2 pi i k z / Z}
+  const int R = kRowThreads / Z;
+  float2* sU = stw + m * (Z + 1);                        // R x kMaxWidth x kMaxModes
+  float* tile = reinterpret_cast<float*>(sU + R * kMaxWidth * kMaxModes);  // R x kMaxWidth x (Z+1)
+
+  const int kin = LIFT ? kFeat : W;
+  for (int i = threadIdx.x; i < kMaxWidth * KIN; i += blockDim.x) {
+    const int co = i / KIN, c = i - co * KIN;
+    sW[i] = (co < W && c < kin) ? ld(Wt + co * kin + c) : 0.0f;
+  }
+  for (int i = threadIdx.x; i < kMaxWidth; i += blockDim.x) sb[i] = i < W ? bias[i] : 0.0f;
+  for (int i = threadIdx.x; i < 6 * kMaxWidth; i += blockDim.x) {
+    const int j = i / kMaxWidth, c = i - j * kMaxWidth;
+    sQ[i] = (Q != nullptr && c < W) ? ld(Q + j * W + c) : 0.0f;
+  }
+  if (threadIdx.x < 8) sqb[threadIdx.x] = (qb != nullptr && threadIdx.x < 6) ? qb[threadIdx.x] : 0.0f;
+  for (int i = threadIdx.x; i < m * Z; i += blockDim.x) {
+    const int k = i / Z, zz = i - k * Z;
+    float s, c;
+    sincospif(2.0f * (float)((k * zz) % Z) / (float)Z, &s, &c);
+    stw[k * (Z + 1) + zz] = make_float2(c, -s);
+  }
+  __syncthreads();
+
+  const int z = threadIdx.x % Z;
+  const int rr = threadIdx.x / Z;
+  const bool lane_on = rr < R;
+  const size_t XY = (size_t)X * Y;
+  const size_t ncell = XY * Z;
+  const size_t nrows = (size_t)B * XY;
+  // inverse-DFT weights of this thread's z (loop invariant)
+  float cs[kMaxModes], sn[kMaxModes];
+  {
+    const float inv = 1.0f / (float)ncell;
+#pragma unroll
+    for (int k = 0; k < kMaxModes; ++k) {
+      const float2 t = k < m ? stw[k * (Z + 1) + z] : make_float2(0.0f, 0.0f);
+      const float w = (k == 0 ? 1.0f : 2.0f) * inv;
+      cs[k] = t.x * w;
+      sn[k] = -t.y * w;
+    }
+  }
+  const size_t ngroups = (nrows + R - 1) / R;
+  for (size_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+    const size_t row0 = g * R;
+    if (!LIFT) {
+      for (int i = threadIdx.x; i < R * W * m; i += blockDim.x) {
+        const int r = i / (W * m), rem = i - r * (W * m), co = rem / m, k = rem - co * m;
+        const size_t row = row0 + r;
+        if (row < nrows) {
+          const size_t b = row / XY, xy = row - b * XY;
+          sU[(r * kMaxWidth + co) * kMaxModes + k] = Uxy[((b * W + co) * XY + xy) * m + k];
+        }
+      }
+      __syncthreads();
+    }
+    const size_t row = row0 + rr;
+    const bool valid = lane_on && row < nrows;
+    if (valid) {
+      const size_t b = row / XY, xy = row - b * XY;
+      const size_t cell = xy * Z + z;
+      const size_t base = b * W * ncell + cell;
+      float o[kMaxWidth];
+      if (LIFT) {
+        float f[kFeat];
+        cell_features(chi, wave, ncell, (int)b, cell, f);
+#pragma unroll
+        for (int co = 0; co < kMaxWidth; ++co) {
+          float acc = sb[co];
+#pragma unroll
+          for (int c = 0; c < kFeat; ++c) acc += sW[co * KIN + c] * f[c];
+          o[co] = acc;
+        }
+      } else {
+        float v[kMaxWidth];
+#pragma unroll
+        for (int ci = 0; ci < kMaxWidth; ++ci) v[ci] = ci < W ? ld(vin + base + (size_t)ci * ncell) : 0.0f;
+        const float2* u = sU + rr * kMaxWidth * kMaxModes;
+#pragma unroll
+        for (int co = 0; co < kMaxWidth; ++co) {
+          float acc = sb[co];
+#pragma unroll
+          for (int ci = 0; ci < kMaxWidth; ++ci) acc += sW[co * KIN + ci] * v[ci];
+#pragma unroll
+          for (int k = 0; k < kMaxModes; ++k) {
+            if (k < m) {
+              const float2 uk = u[co * kMaxModes + k];
+              acc += uk.x * cs[k] - uk.y * sn[k];
+            }
+          }
+          o[co] = acc;
+        }
+      }
+#pragma unroll
+      for (int co = 0; co < kMaxWidth; ++co) {
+        if (co < W) {
+          if (pre_out) pre_out[base + (size_t)co * ncell] = st<ACT>(o[co]);
+          const ACT q = st<ACT>((!LIFT && apply_gelu) ? gelu(o[co]) : o[co]);
+          if (vout) vout[base + (size_t)co * ncell] = q;
+          o[co] = ld(&q);
+        } else {
+          o[co] = 0.0f;
+        }
+      }
+      if (u_out) {
+        float p[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+          float acc = sqb[j];
+#pragma unroll
+          for (int ci = 0; ci < kMaxWidth; ++ci) acc += sQ[j * kMaxWidth + ci] * o[ci];
+          p[j] = acc;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const size_t idx = (b * 3 + c) * ncell + cell;
+          const float2 fw = wave[idx];
+          u_out[idx] = make_float2(fw.x + p[2 * c], fw.y + p[2 * c + 1]);
+        }
+      }
+      if (Vz) {
+        float* t = tile + rr * kMaxWidth * (Z + 1);
+#pragma unroll
+        for (int co = 0; co < kMaxWidth; ++co)
+          if (co < W) t[co * (Z + 1) + z] = o[co];
+      }
+    }
+    if (Vz) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < R * W * m; i += blockDim.x) {
+        const int r = i / (W * m), rem = i - r * (W * m), co = rem / m, k = rem - co * m;
+        const size_t rw = row0 + r;
+        if (rw < nrows) {
+          const float* t = tile + (r * kMaxWidth + co) * (Z + 1);
+          const float2* w = stw + k * (Z + 1);
+          float re = 0.0f, im = 0.0f;
+          for (int zz = 0; zz < Z; ++zz) {
+            re += t[zz] * w[zz].x;
+            im += t[zz] * w[zz].y;
+          }
+          const size_t b = rw / XY, xy = rw - b * XY;
+          Vz[((b * W + co) * XY + xy) * m + k] = make_float2(re, im);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+inline size_t row_fwd_smem(bool lift, int Z, int m) {
+  const int KIN = lift ? kFeat : kMaxWidth;
+  const int R = kRowThreads / Z;
+  return sizeof(float) * (kMaxWidth * KIN + kMaxWidth + 6 * kMaxWidth + 8) + sizeof(float2) * (size_t)m * (Z + 1) +
+         sizeof(float2) * (size_t)R * kMaxWidth * kMaxModes + sizeof(float) * (size_t)R * kMaxWidth * (Z + 1);
+}
+
+// ---------------------------------------------------------------------------
+// Register-blocked contraction Y[o][j][i] (op)= sum_l X[o][l][i] M[l][j] with
+// M (L x J) in shared memory; each thread produces JB consecutive j of one
+// (o, i), so X is read once instead of once per output.
+// ---------------------------------------------------------------------------
+
+template <int JB, bool REAL_ACC>
+__global__ void k_contract_blk(size_t outer, int L, int J, int inner, const float2* __restrict__ Xin,
+                               const float2* __restrict__ M, void* __restrict__ Yout) {
+  extern __shared__ float2 sM[];
+  for (int i = threadIdx.x; i < L * J; i += blockDim.x) sM[i] = M[i];
+  __syncthreads();
+  const int nb = (J + JB - 1) / JB;
+  const size_t total = outer * (size_t)nb * inner;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % inner);
+    const int jb = (int)((t / inner) % nb);
+    const size_t o = t / ((size_t)inner * nb);
+    const float2* x = Xin + o * L * inner + i;
+    float re[JB], im[JB];
+#pragma unroll
+    for (int jj = 0; jj < JB; ++jj) re[jj] = im[jj] = 0.0f;
+    const int j0 = jb * JB;
+    for (int l = 0; l < L; ++l) {
+      const float2 v = x[(size_t)l * inner];
+      const float2* mr = sM + l * J + j0;
+#pragma unroll
+      for (int jj = 0; jj < JB; ++jj) {
+        if (j0 + jj < J) {
+          const float2 mm = mr[jj];
+          re[jj] += v.x * mm.x - v.y * mm.y;
+          im[jj] += v.x * mm.y + v.y * mm.x;
+        }
+      }
+    }
+#pragma unroll
+    for (int jj = 0; jj < JB; ++jj) {
+      if (j0 + jj < J) {
+        const size_t idx = (o * J + j0 + jj) * inner + i;
+        if (REAL_ACC) reinterpret_cast<float*>(Yout)[idx] += re[jj];
+        else reinterpret_cast<float2*>(Yout)[idx] = make_float2(re[jj], im[jj]);
+      }
+    }
+  }
+}
+
 inline int blocks_for(size_t n, int threads = 256) {
   size_t b = (n + threads - 1) / threads;
   if (b > (size_t)148 * 32) b = (size_t)148 * 32;
@@ -543,6 +776,34 @@ enum { FNO_BF16 = 0, FNO_F32 = 1 };
     else if ((act) == FNO_F32) { using ACT = float; CALL; }                       \
     else { em3d_set_last_error("act dtype must be 0 (bf16) or 1 (float)"); return EM3D_ERR_INVALID; } \
   } while (0)
+
+// Opt a kernel in to more than 48 KB of dynamic shared memory.
+static bool allow_dyn_smem(const void* fn, size_t bytes) {
+  if (bytes <= 48 * 1024) return true;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) { em3d_set_last_error(cudaGetErrorString(e)); return false; }
+  return true;
+}
+
+template <typename ACT>
+static int launch_row_fwd(bool lift, int grid, size_t smem, cudaStream_t st, int B, int W, int X, int Y, int Z, int m,
+                          const void* chi, const void* wave, const void* vin, const void* Uxy, const void* Wt,
+                          const float* bias, int apply_gelu, void* pre_out, void* vout, void* Vz, const void* Q,
+                          const float* qb, void* u_out) {
+  if (lift) {
+    if (!allow_dyn_smem((const void*)k_row_fwd<ACT, true>, smem)) return EM3D_ERR_CUDA;
+    k_row_fwd<ACT, true><<<grid, kRowThreads, smem, st>>>(
+        B, W, X, Y, Z, m, (const float2*)chi, (const float2*)wave, nullptr, nullptr, (const ACT*)Wt, bias, 0,
+        (ACT*)pre_out, (ACT*)vout, (float2*)Vz, (const ACT*)Q, qb, (float2*)u_out);
+  } else {
+    if (!allow_dyn_smem((const void*)k_row_fwd<ACT, false>, smem)) return EM3D_ERR_CUDA;
+    k_row_fwd<ACT, false><<<grid, kRowThreads, smem, st>>>(
+        B, W, X, Y, Z, m, (const float2*)chi, (const float2*)wave, (const ACT*)vin, (const float2*)Uxy,
+        (const ACT*)Wt, bias, apply_gelu, (ACT*)pre_out, (ACT*)vout, (float2*)Vz, (const ACT*)Q, qb,
+        (float2*)u_out);
+  }
+  return EM3D_OK;
+}
 
 static int check_width(int W) {
   if (W < 1 || W > kMaxWidth) { em3d_set_last_error("FNO width must be in [1, 32]"); return EM3D_ERR_INVALID; }
@@ -577,15 +838,58 @@ int em3d_fno_contract(int kind, int act, size_t outer, int L, int J, int inner, 
   if (kind == 0) {
     FNO_DISPATCH(act, (k_contract_r2c<ACT><<<blocks_for(n), 256, 0, st>>>(outer, L, J, inner, (const ACT*)X,
                                                                            (const float2*)M, (float2*)Y)));
-  } else if (kind == 1) {
-    k_contract_c2c<<<blocks_for(n), 256, 0, st>>>(outer, L, J, inner, (const float2*)X, (const float2*)M, (float2*)Y);
-  } else if (kind == 2) {
-    k_contract_c2r_acc<<<blocks_for(n), 256, 0, st>>>(outer, L, J, inner, (const float2*)X, (const float2*)M,
-                                                      (float*)Y);
+  } else if (kind == 1 || kind == 2) {
+    const size_t smem = sizeof(float2) * (size_t)L * J;
+    if (smem <= 48 * 1024) {
+      constexpr int JB = 8;
+      const size_t nthr = outer * (size_t)((J + JB - 1) / JB) * inner;
+      if (kind == 1)
+        k_contract_blk<JB, false><<<blocks_for(nthr), 256, smem, st>>>(outer, L, J, inner, (const float2*)X,
+                                                                       (const float2*)M, Y);
+      else
+        k_contract_blk<JB, true><<<blocks_for(nthr), 256, smem, st>>>(outer, L, J, inner, (const float2*)X,
+                                                                      (const float2*)M, Y);
+    } else if (kind == 1) {
+      k_contract_c2c<<<blocks_for(n), 256, 0, st>>>(outer, L, J, inner, (const float2*)X, (const float2*)M,
+                                                    (float2*)Y);
+    } else {
+      k_contract_c2r_acc<<<blocks_for(n), 256, 0, st>>>(outer, L, J, inner, (const float2*)X, (const float2*)M,
+                                                        (float*)Y);
+    }
   } else {
     em3d_set_last_error("contract kind must be 0 (real->complex), 1 (complex), 2 (complex->real, accumulate)");
     return EM3D_ERR_INVALID;
   }
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_row_forward(int act, int lift, int B, int W, int X, int Y, int Z, int m, const void* chi,
+                         const void* wave, const void* vin, const void* Uxy, const void* Wt, const float* bias,
+                         int apply_gelu, void* pre_out, void* vout, void* Vz, const void* Q, const float* qb,
+                         void* u_out, void* stream) {
+  if (int rc = check_width(W)) return rc;
+  if (Z < 1 || Z > kRowThreads || m < 1 || m > kMaxModes || 2 * m > Z || X < 1 || Y < 1 || B < 1) {
+    em3d_set_last_error("row_forward: needs 1 <= Z <= 128, 1 <= modes <= 16, 2 modes <= Z");
+    return EM3D_ERR_UNSUPPORTED;
+  }
+  if (lift ? (!chi || !wave) : (!vin || !Uxy)) {
+    em3d_set_last_error("row_forward: missing input");
+    return EM3D_ERR_INVALID;
+  }
+  if (u_out && (!Q || !qb || !wave)) {
+    em3d_set_last_error("row_forward: projection needs Q, qb and wave");
+    return EM3D_ERR_INVALID;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t smem = row_fwd_smem(lift != 0, Z, m);
+  const int R = kRowThreads / Z;
+  const size_t groups = ((size_t)B * X * Y + R - 1) / R;
+  const int grid = (int)(groups < (size_t)148 * 12 ? groups : (size_t)148 * 12);
+  int rc = EM3D_OK;
+  FNO_DISPATCH(act, (rc = launch_row_fwd<ACT>(lift != 0, grid, smem, st, B, W, X, Y, Z, m, chi, wave, vin, Uxy, Wt,
+                                              bias, apply_gelu, pre_out, vout, Vz, Q, qb, u_out)));
+  if (rc != EM3D_OK) return rc;
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }

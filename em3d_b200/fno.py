@@ -153,6 +153,62 @@ class FNO:
 
     def forward(self, chi, wave, train: bool = False):
         """u = network(chi, wave): chi (B,3,3,X,Y,Z), wave (B,3,X,Y,Z) complex64 device tensors."""
+        Z = wave.shape[-1]
+        if Z <= 128 and 2 * self.m <= Z and self.m <= 16:
+            return self._forward_rows(chi, wave, train)
+        return self._forward_passes(chi, wave, train)
+
+    def _spectral(self, l, B, N, buf, mats, V):
+        """Vz (truncated z-DFT of the layer input) -> Uxy (modes mixed, x and y inverted)."""
+        X, Y, Z = N
+        W, m = self.W, self.m
+        nm = 4 * m * m * m
+        st = _lib.stream_handle()
+        self._contract(1, 0, B * W * X, Y, 2 * m, m, buf["Vz"], mats["fy"], buf["Vy"])
+        self._contract(1, 0, B * W, X, 2 * m, 2 * m * m, buf["Vy"], mats["fx"], V)
+        _lib.call("em3d_fno_modemix", self.act, B, W, nm, V.data_ptr(), self._w(f"Wre{l}").data_ptr(),
+                  self._w(f"Wim{l}").data_ptr(), buf["U"].data_ptr(), st)
+        self._contract(1, 0, B * W, 2 * m, X, 2 * m * m, buf["U"], mats["ix"], buf["Ux"])
+        self._contract(1, 0, B * W * X, 2 * m, Y, m, buf["Ux"], mats["iy"], buf["Uxy"])
+
+    def _forward_rows(self, chi, wave, train):
+        """Forward with the fused z-row kernel: lift + first z-DFT, then per
+        layer the y/x contractions, mode mixing and inverse, and one row pass
+        that applies the layer and produces the next layer's z-DFT (or, after
+        the last layer, the projection)."""
+        B = wave.shape[0]
+        N = tuple(wave.shape[-3:])
+        X, Y, Z = N
+        W, m, Lyr = self.W, self.m, self.L
+        mats = self._matrices(N)
+        buf = self._buffers(B, N, train)
+        st = _lib.stream_handle()
+        chi = chi.contiguous()
+        wave = wave.contiguous()
+        v = buf["v"]
+
+        def ptr(t):
+            return None if t is None else t.data_ptr()
+
+        _lib.call("em3d_fno_row_forward", self.act, 1, B, W, X, Y, Z, m, chi.data_ptr(), wave.data_ptr(), None, None,
+                  self._w("P").data_ptr(), self.master["pb"].data_ptr(), 0, None, v[0].data_ptr(),
+                  buf["Vz"].data_ptr(), None, None, None, st)
+        for l in range(Lyr):
+            last = l == Lyr - 1
+            vin = v[l] if train else v[l % 2]
+            vout = v[l + 1] if train else (None if last else v[(l + 1) % 2])
+            V = buf["V"][l] if train else buf["V"][0]
+            self._spectral(l, B, N, buf, mats, V)
+            _lib.call("em3d_fno_row_forward", self.act, 0, B, W, X, Y, Z, m, None, wave.data_ptr(), vin.data_ptr(),
+                      buf["Uxy"].data_ptr(), self._w(f"A{l}").data_ptr(), self.master[f"a{l}"].data_ptr(),
+                      int(not last), ptr(buf["pre"][l]) if train else None, ptr(vout),
+                      None if last else buf["Vz"].data_ptr(), self._w("Q").data_ptr() if last else None,
+                      self.master["qb"].data_ptr() if last else None, buf["u"].data_ptr() if last else None, st)
+        self._last = (chi, wave, B, N)
+        return buf["u"]
+
+    def _forward_passes(self, chi, wave, train: bool = False):
+        """Forward as separate passes (any Z up to 1024)."""
         B = wave.shape[0]
         N = tuple(wave.shape[-3:])
         X, Y, Z = N

@@ -355,21 +355,26 @@ class _KrylovSolver:
     and the captured CUDA graph of the iteration (the solver configuration is
     re-read at every solve)."""
 
+    # Engines (device buffers + captured graph) kept per solver object; the
+    # oldest is dropped beyond this many, which releases its operator too.
+    max_cached_engines = 2
+
     def _engine(self, operator, rhs, hist_cap, batch):
-        import weakref
+        from collections import OrderedDict
 
         if not hasattr(self, "_engines"):
-            self._engines = {}
+            self._engines = OrderedDict()
         key = (id(operator), tuple(rhs.shape), str(rhs.dtype), batch, hist_cap)
         hit = self._engines.get(key)
-        if hit is not None and hit[0]() is operator:
-            eng = hit[1]
-            eng.load_rhs(rhs)
-            return eng
+        if hit is not None and hit.op is operator:
+            self._engines.move_to_end(key)
+            hit.load_rhs(rhs)
+            return hit
         eng = _Engine(operator, rhs, hist_cap=hist_cap, batch=batch)
         if hasattr(operator, "apply_into"):
-            self._engines = {k: v for k, v in self._engines.items() if v[0]() is not None}
-            self._engines[key] = (weakref.ref(operator), eng)
+            self._engines[key] = eng
+            while len(self._engines) > self.max_cached_engines:
+                self._engines.popitem(last=False)
         return eng
 
     def _vec(self, eng, name):
@@ -591,6 +596,7 @@ class DefectCorrectionResult(SolverResult):
     fp64_matvecs: int = 0
     fp32_matvecs: int = 0
     fp32_rmatvecs: int = 0
+    guess_rejected: bool = False
 
 
 class DefectCorrection:
@@ -608,11 +614,16 @@ class DefectCorrection:
     ``rtol`` (with a safety factor), never looser than ``inner_rtol_max``.
     ``solve_batch`` corrects a stack of right-hand sides together (batched
     operator applications, batched inner solves); each stops on its own.
+
+    An initial guess ``x0`` (a learned warm start, say) is judged by its true
+    residual: when ``||f - A x0|| >= ||f||`` (or is not finite) the solve
+    falls back to the zero guess (``guess_rejected`` in the result), so a bad
+    guess never costs more than one FP64 matvec.
     """
 
     def __init__(self, config: SolverConfig, *, inner: str = "bicgstab", inner_rtol: float = 1e-4,
                  inner_rtol_max: float = 1e-2, inner_max_iter: int | None = None, max_outer: int = 20,
-                 safety: float = 0.3):
+                 safety: float = 0.3, guess_fallback: bool = True):
         if inner not in ("bicgstab", "twostep"):
             raise ValueError(f"inner must be 'bicgstab' or 'twostep', got {inner!r}")
         self.cfg = config
@@ -622,6 +633,7 @@ class DefectCorrection:
         self.inner_max_iter = inner_max_iter
         self.max_outer = int(max_outer)
         self.safety = float(safety)
+        self.guess_fallback = bool(guess_fallback)
 
     def solve(self, operator, rhs, x0=None, *, operator_low=None) -> DefectCorrectionResult:
         import torch
@@ -637,30 +649,35 @@ class DefectCorrection:
         t = t.reshape((b,) + tuple(operator._field_shape()))
         return self._solve(operator, t, x0, b, operator_low)
 
+    max_cached = 2
+
     def _buffers(self, operator, rhs, batch, operator_low):
         """Engine, buffers, FP32 operator and inner solver, reused across solves
-        with the same operator and shape."""
-        import weakref
+        with the same operator and shape (a small LRU; evicting an entry
+        releases its operators)."""
+        from collections import OrderedDict
 
         import torch
 
         from .backend import Precision
 
         if not hasattr(self, "_cache"):
-            self._cache = {}
+            self._cache = OrderedDict()
         key = (id(operator), tuple(rhs.shape), batch)
         hit = self._cache.get(key)
-        if hit is not None and hit["op"]() is operator and (operator_low is None or hit["op_lo"] is operator_low):
+        if hit is not None and hit["op"] is operator and (operator_low is None or hit["op_lo"] is operator_low):
+            self._cache.move_to_end(key)
             hit["eng"].load_rhs(rhs)
             return hit
         eng = _Engine(operator, rhs, hist_cap=4, batch=batch)
         op_lo = operator_low if operator_low is not None else operator.with_precision(Precision.SINGLE)
         inner_cls = BiCGStab if self.inner == "bicgstab" else TwoStep
-        hit = {"op": weakref.ref(operator), "op_lo": op_lo, "eng": eng, "u": eng.vec(), "r": eng.vec(),
+        hit = {"op": operator, "op_lo": op_lo, "eng": eng, "u": eng.vec(), "r": eng.vec(),
                "r_lo": torch.empty(eng.rhs.shape, dtype=torch.complex64, device=eng.rhs.device),
                "inner": inner_cls(SolverConfig())}
-        self._cache = {k: v for k, v in self._cache.items() if v["op"]() is not None}
         self._cache[key] = hit
+        while len(self._cache) > self.max_cached:
+            self._cache.popitem(last=False)
         return hit
 
     def _solve(self, operator, rhs, x0, batch, operator_low):
@@ -682,12 +699,20 @@ class DefectCorrection:
         rmv32 = np.zeros(batch, dtype=int)
         inner_its = [[] for _ in range(batch)]
         budget_inner = int(self.inner_max_iter or cfg.max_iter)
+        rejected = [False] * batch
         for outer in range(self.max_outer + 1):
             operator.apply_into(u, r)
             mv64 += 1
             _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0,
                       r.data_ptr(), eng.stream())
             rel = eng.norms(r) / fs
+            if outer == 0 and x0 is not None and self.guess_fallback:
+                for b in range(batch):
+                    if status[b] is None and not rel[b] < 1.0:
+                        (u if batch == 1 else u[b]).zero_()
+                        (r if batch == 1 else r[b]).copy_(f if batch == 1 else f[b])
+                        rel[b] = 1.0
+                        rejected[b] = True
             for b in range(batch):
                 if status[b] is not None:
                     continue
@@ -736,5 +761,5 @@ class DefectCorrection:
                 residual_action_counts=counts[b] if counts[b] else [0], status=status[b] or "max_iter",
                 true_final_residual=float(h[-1]), outer_iterations=len(inner_its[b]),
                 inner_iterations=inner_its[b], fp64_matvecs=int(mv64), fp32_matvecs=int(mv32[b]),
-                fp32_rmatvecs=int(rmv32[b])))
+                fp32_rmatvecs=int(rmv32[b]), guess_rejected=rejected[b]))
         return out

@@ -275,8 +275,45 @@ int em3d_fno_project_bwd(int act, int B, size_t ncell, int W, const void* v, con
 int em3d_fno_loss(int B, size_t n, const void* pred, const void* target, double* terms, void* grad, void* stream);
 int em3d_fno_adam(int act, size_t n, float* w, const float* g, float* m1, float* m2, float lr, float b1, float b2,
                   float eps, int step, void* wact, void* stream);
+/* Fused forward z-row pass (Z <= 128, W <= 32, modes <= 16; EM3D_ERR_UNSUPPORTED
+ * otherwise): lift (lift = 1: o = P feat + pb from chi, wave) or one Fourier
+ * layer (o = act(A vin + a + Re IDFT_z(Uxy))), writing any of: pre (pre_out),
+ * o (vout), the truncated z-DFT of o (Vz, (B,W,X,Y,m) complex) and the
+ * projection u = wave + Q o + qb (u_out).  NULL outputs are skipped. */
+int em3d_fno_row_forward(int act, int lift, int B, int W, int X, int Y, int Z, int m, const void* chi,
+                         const void* wave, const void* vin, const void* Uxy, const void* Wt, const float* bias,
+                         int apply_gelu, void* pre_out, void* vout, void* Vz, const void* Q, const float* qb,
+                         void* u_out, void* stream);
 int em3d_fno_cast(int act, size_t n, const float* src, void* dst, void* stream);
 int em3d_fno_uncast(int act, size_t n, const void* src, float* dst, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Input builders on the device.
+ *
+ * em3d_sample_ellipsoids: a scene of `count` ellipsoids sampled at cell
+ * centres; replaces the host-side center_mask + sample_contrast_tensor
+ * (src/em3d/geometry.py:67-93, 203-252) and eta_sphere / eta_ellipsoid
+ * (src/em3d/acoustics/materials.py:44-83), extended to rotated ellipsoids and
+ * to several shapes painted in order (the last shape containing a cell wins).
+ *   x, y, z    DEVICE float64 cell-centre coordinates (nx, ny, nz values)
+ *   shapes     DEVICE float64 array, EM3D_SHAPE_DOUBLES per shape: centre[3],
+ *              radii[3], R[9] (row-major; columns = body axes, r = c + R p),
+ *              eps[18] (3x3 complex row-major, re/im interleaved; acoustic
+ *              uses eps[0][0] as eta)
+ *   tol        inside <=> sum (p_i / a_i)^2 <= 1 + tol (the reference EM
+ *              builder uses 64 eps_f64 max(1, |L|); the acoustic ones 0)
+ *   background HOST float64: 18 values (EM eps tensor) or 2 (acoustic eta)
+ *   out        EM: chi = eps - I (3,3,Nx,Ny,Nz); acoustic: eta (Nx,Ny,Nz)
+ * em3d_plane_wave: amplitude[c] exp(i sign (k orient.r + phi0)), (3,Nx,Ny,Nz);
+ * replaces flat_wave_vec (src/em3d/wave.py:9-37).  orient (3) and amplitude
+ * (3 complex = 6 doubles) are HOST arrays.
+ * ------------------------------------------------------------------------ */
+#define EM3D_SHAPE_DOUBLES 33
+int em3d_sample_ellipsoids(int kind, int dtype, int nx, int ny, int nz, const double* x, const double* y,
+                           const double* z, int count, const double* shapes, double tol, const double* background,
+                           void* out, void* stream);
+int em3d_plane_wave(int dtype, int nx, int ny, int nz, const double* x, const double* y, const double* z, double k,
+                    const double* orient, const double* amplitude, double phi0, int sign, void* out, void* stream);
 
 #ifdef __cplusplus
 }

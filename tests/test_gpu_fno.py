@@ -91,3 +91,31 @@ def test_fno_training_reduces_loss():
     losses = [net.train_step(chi, wave, target, lr=1e-2) for _ in range(60)]
     assert np.all(np.isfinite(losses))
     assert losses[-1] < 0.5 * losses[0], losses[::10]
+
+
+@pytest.mark.parametrize("act,tol", [("float", 2e-5), ("bf16", 3e-2)])
+@pytest.mark.parametrize("N,W,m", [((16, 12, 32), 32, 5), ((8, 10, 128), 7, 3), ((6, 6, 6), 32, 3)])
+def test_fused_row_forward_matches_separate_passes(act, tol, N, W, m):
+    """The fused z-row forward (lift + z-DFT, layer + next z-DFT, last layer +
+    projection) gives the same u and stored activations as the pass-by-pass
+    kernels, in inference and in training mode."""
+    import torch
+
+    from em3d_b200.fno import FNO
+
+    rng = np.random.default_rng(11)
+    B = 2
+    chi = torch.as_tensor((_rand(rng, (B, 3, 3) + N) * 0.3).astype(np.complex64), device="cuda")
+    wave = torch.as_tensor(_rand(rng, (B, 3) + N).astype(np.complex64), device="cuda")
+    net = FNO(width=W, modes=m, layers=3, act=act, seed=5)
+    for train in (False, True):
+        a = net._forward_rows(chi, wave, train).clone()
+        acts = [t.float().clone() for t in net._buffers(B, N, train)["v"]] if train else []
+        b = net._forward_passes(chi, wave, train).clone()
+        torch.cuda.synchronize()
+        err = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+        assert err < tol, (train, err)
+        if train:
+            for x, y in zip(acts, net._buffers(B, N, train)["v"]):
+                e = float(torch.linalg.vector_norm(x - y.float()) / torch.linalg.vector_norm(y.float()))
+                assert e < tol * 4, e

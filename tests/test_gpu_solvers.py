@@ -196,3 +196,43 @@ def test_repeated_solves_reuse_buffers_and_return_fresh_results():
     assert r1.iterations == fresh.iterations and r1.residual_history == fresh.residual_history
     assert torch.equal(r1.u, fresh.u)
     assert r2.residual_history == r0.residual_history and torch.equal(r2.u, r0.u)
+
+
+def test_solver_caches_release_old_operators():
+    """Solving a stream of different problems keeps a bounded number of cached
+    engines: operators of earlier problems are released."""
+    import gc
+    import weakref
+
+    import em3d_b200 as e
+    from em3d_b200.solvers import BiCGStab, DefectCorrection, SolverConfig
+
+    be, prob, _ = _sphere16("double")
+    bic = BiCGStab(SolverConfig(max_iter=200, rtol=1e-6))
+    dc = DefectCorrection(SolverConfig(max_iter=200, rtol=1e-6))
+    refs = []
+    for k in (3.0, 3.5, 4.0, 4.5, 5.0):
+        p = e.Problem(grid=prob.grid, eps_tensor=prob.eps_tensor, wave=prob.wave, k0=k, volume=1.0)
+        op = e.Operator(p)
+        assert bic.solve(op, p.wave).converged
+        assert dc.solve(op, p.wave).converged
+        refs.append(weakref.ref(op))
+        del op, p
+    gc.collect()
+    assert len(bic._engines) <= bic.max_cached_engines and len(dc._cache) <= dc.max_cached
+    assert all(r() is None for r in refs[:2])
+
+
+def test_defect_correction_rejects_a_bad_guess():
+    """A guess whose true residual exceeds ||f|| is replaced by the zero guess."""
+    from em3d_b200.solvers import DefectCorrection, SolverConfig
+
+    be, prob, op = _sphere16("double")
+    dc = DefectCorrection(SolverConfig(max_iter=200, rtol=1e-8))
+    cold = dc.solve(op, prob.wave)
+    bad = dc.solve(op, prob.wave, x0=prob.wave * 50.0)
+    assert bad.guess_rejected and bad.converged
+    assert bad.residual_history[0] == 1.0
+    assert rel_err(be.to_host(bad.u), be.to_host(cold.u)) < 1e-7
+    good = dc.solve(op, prob.wave, x0=cold.u * (1 + 1e-5))
+    assert not good.guess_rejected and good.residual_history[0] < 1e-3
