@@ -549,15 +549,16 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
     const float* __restrict__ bias, int apply_gelu, ACT* __restrict__ pre_out, ACT* __restrict__ vout,
     float2* __restrict__ Vz, const ACT* __restrict__ Q, const float* __restrict__ qb, float2* __restrict__ u_out) {
   constexpr int KIN = LIFT ? kFeat : kMaxWidth;
-  extern __shared__ float sh[];
+  extern __shared__ __align__(16) float sh[];
   float* sW = sh;                                        // kMaxWidth x KIN
   float* sb = sW + kMaxWidth * KIN;                      // kMaxWidth
   float* sQ = sb + kMaxWidth;                            // 6 x kMaxWidth
   float* sqb = sQ + 6 * kMaxWidth;                       // 8
-  float2* stw = reinterpret_cast<float2*>(sqb + 8);      // m x (Z+1): e^{-2 pi i k z / Z}
+  float2* stw = reinterpret_cast<float2*>(sqb + 8);      // Z x kMaxModes: e^{-2 pi i k z / Z} at [z][k]
   const int R = kRowThreads / Z;
-  float2* sU = stw + m * (Z + 1);                        // R x kMaxWidth x kMaxModes
-  float* tile = reinterpret_cast<float*>(sU + R * kMaxWidth * kMaxModes);  // R x kMaxWidth x (Z+1)
+  const int TS = ((Z + 3) & ~3) + 4;                     // tile row stride: a multiple of 4 floats (16-byte rows)
+  float2* sU = stw + Z * kMaxModes;                      // R x kMaxWidth x kMaxModes
+  float* tile = reinterpret_cast<float*>(sU + R * kMaxWidth * kMaxModes);  // R x kMaxWidth x TS
 
   const int kin = LIFT ? kFeat : W;
   for (int i = threadIdx.x; i < kMaxWidth * KIN; i += blockDim.x) {
@@ -570,11 +571,11 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
     sQ[i] = (Q != nullptr && c < W) ? ld(Q + j * W + c) : 0.0f;
   }
   if (threadIdx.x < 8) sqb[threadIdx.x] = (qb != nullptr && threadIdx.x < 6) ? qb[threadIdx.x] : 0.0f;
-  for (int i = threadIdx.x; i < m * Z; i += blockDim.x) {
-    const int k = i / Z, zz = i - k * Z;
-    float s, c;
-    sincospif(2.0f * (float)((k * zz) % Z) / (float)Z, &s, &c);
-    stw[k * (Z + 1) + zz] = make_float2(c, -s);
+  for (int i = threadIdx.x; i < Z * kMaxModes; i += blockDim.x) {
+    const int zz = i / kMaxModes, k = i - zz * kMaxModes;
+    float s = 0.0f, c = 0.0f;
+    if (k < m) sincospif(2.0f * (float)((k * zz) % Z) / (float)Z, &s, &c);
+    stw[i] = make_float2(c, -s);
   }
   __syncthreads();
 
@@ -584,29 +585,33 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
   const size_t XY = (size_t)X * Y;
   const size_t ncell = XY * Z;
   const size_t nrows = (size_t)B * XY;
-  // inverse-DFT weights of this thread's z (loop invariant)
+  // inverse-DFT weights of this thread's z (loop invariant; zero for k >= m)
   float cs[kMaxModes], sn[kMaxModes];
   {
     const float inv = 1.0f / (float)ncell;
 #pragma unroll
     for (int k = 0; k < kMaxModes; ++k) {
-      const float2 t = k < m ? stw[k * (Z + 1) + z] : make_float2(0.0f, 0.0f);
+      const float2 t = stw[z * kMaxModes + k];
       const float w = (k == 0 ? 1.0f : 2.0f) * inv;
       cs[k] = t.x * w;
       sn[k] = -t.y * w;
     }
   }
+  const int mb = (m + 3) / 4;  // mode blocks of 4 in the DFT phase
   const size_t ngroups = (nrows + R - 1) / R;
   for (size_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
     const size_t row0 = g * R;
     if (!LIFT) {
-      for (int i = threadIdx.x; i < R * W * m; i += blockDim.x) {
-        const int r = i / (W * m), rem = i - r * (W * m), co = rem / m, k = rem - co * m;
+      for (int i = threadIdx.x; i < R * kMaxWidth * kMaxModes; i += blockDim.x) {
+        const int r = i / (kMaxWidth * kMaxModes), rem = i - r * (kMaxWidth * kMaxModes);
+        const int co = rem / kMaxModes, k = rem - co * kMaxModes;
         const size_t row = row0 + r;
-        if (row < nrows) {
+        float2 val = make_float2(0.0f, 0.0f);
+        if (row < nrows && co < W && k < m) {
           const size_t b = row / XY, xy = row - b * XY;
-          sU[(r * kMaxWidth + co) * kMaxModes + k] = Uxy[((b * W + co) * XY + xy) * m + k];
+          val = Uxy[((b * W + co) * XY + xy) * m + k];
         }
+        sU[i] = val;
       }
       __syncthreads();
     }
@@ -622,26 +627,34 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
         cell_features(chi, wave, ncell, (int)b, cell, f);
 #pragma unroll
         for (int co = 0; co < kMaxWidth; ++co) {
+          const float4* w4 = reinterpret_cast<const float4*>(sW + co * KIN);
           float acc = sb[co];
 #pragma unroll
-          for (int c = 0; c < kFeat; ++c) acc += sW[co * KIN + c] * f[c];
+          for (int c4 = 0; c4 < kFeat / 4; ++c4) {
+            const float4 w = w4[c4];
+            acc += w.x * f[4 * c4] + w.y * f[4 * c4 + 1] + w.z * f[4 * c4 + 2] + w.w * f[4 * c4 + 3];
+          }
           o[co] = acc;
         }
       } else {
         float v[kMaxWidth];
 #pragma unroll
         for (int ci = 0; ci < kMaxWidth; ++ci) v[ci] = ci < W ? ld(vin + base + (size_t)ci * ncell) : 0.0f;
-        const float2* u = sU + rr * kMaxWidth * kMaxModes;
+        const float4* u4 = reinterpret_cast<const float4*>(sU + rr * kMaxWidth * kMaxModes);
 #pragma unroll
         for (int co = 0; co < kMaxWidth; ++co) {
+          const float4* w4 = reinterpret_cast<const float4*>(sW + co * KIN);
           float acc = sb[co];
 #pragma unroll
-          for (int ci = 0; ci < kMaxWidth; ++ci) acc += sW[co * KIN + ci] * v[ci];
+          for (int c4 = 0; c4 < kMaxWidth / 4; ++c4) {
+            const float4 w = w4[c4];
+            acc += w.x * v[4 * c4] + w.y * v[4 * c4 + 1] + w.z * v[4 * c4 + 2] + w.w * v[4 * c4 + 3];
+          }
 #pragma unroll
-          for (int k = 0; k < kMaxModes; ++k) {
-            if (k < m) {
-              const float2 uk = u[co * kMaxModes + k];
-              acc += uk.x * cs[k] - uk.y * sn[k];
+          for (int k2 = 0; k2 < kMaxModes / 2; ++k2) {
+            if (2 * k2 < m) {
+              const float4 uk = u4[co * (kMaxModes / 2) + k2];   // modes 2 k2 and 2 k2 + 1
+              acc += uk.x * cs[2 * k2] - uk.y * sn[2 * k2] + uk.z * cs[2 * k2 + 1] - uk.w * sn[2 * k2 + 1];
             }
           }
           o[co] = acc;
@@ -662,9 +675,13 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
         float p[6];
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
+          const float4* q4 = reinterpret_cast<const float4*>(sQ + j * kMaxWidth);
           float acc = sqb[j];
 #pragma unroll
-          for (int ci = 0; ci < kMaxWidth; ++ci) acc += sQ[j * kMaxWidth + ci] * o[ci];
+          for (int c4 = 0; c4 < kMaxWidth / 4; ++c4) {
+            const float4 w = q4[c4];
+            acc += w.x * o[4 * c4] + w.y * o[4 * c4 + 1] + w.z * o[4 * c4 + 2] + w.w * o[4 * c4 + 3];
+          }
           p[j] = acc;
         }
 #pragma unroll
@@ -675,27 +692,49 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
         }
       }
       if (Vz) {
-        float* t = tile + rr * kMaxWidth * (Z + 1);
+        float* t = tile + rr * kMaxWidth * TS;
 #pragma unroll
         for (int co = 0; co < kMaxWidth; ++co)
-          if (co < W) t[co * (Z + 1) + z] = o[co];
+          if (co < W) t[co * TS + z] = o[co];
       }
     }
     if (Vz) {
       __syncthreads();
-      for (int i = threadIdx.x; i < R * W * m; i += blockDim.x) {
-        const int r = i / (W * m), rem = i - r * (W * m), co = rem / m, k = rem - co * m;
+      // one (row, channel, block of 4 modes) per item; 4 cells per tile load
+      for (int i = threadIdx.x; i < R * W * mb; i += blockDim.x) {
+        const int r = i / (W * mb), rem = i - r * (W * mb), co = rem / mb, kb = rem - co * mb;
         const size_t rw = row0 + r;
         if (rw < nrows) {
-          const float* t = tile + (r * kMaxWidth + co) * (Z + 1);
-          const float2* w = stw + k * (Z + 1);
-          float re = 0.0f, im = 0.0f;
-          for (int zz = 0; zz < Z; ++zz) {
-            re += t[zz] * w[zz].x;
-            im += t[zz] * w[zz].y;
+          const float* t = tile + (r * kMaxWidth + co) * TS;
+          float re[4] = {0.0f, 0.0f, 0.0f, 0.0f}, im[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+          const int z4 = Z & ~3;
+          for (int zz = 0; zz < z4; zz += 4) {
+            const float4 tv = *reinterpret_cast<const float4*>(t + zz);
+            const float tz[4] = {tv.x, tv.y, tv.z, tv.w};
+#pragma unroll
+            for (int d = 0; d < 4; ++d) {
+              const float4* w4 = reinterpret_cast<const float4*>(stw + (zz + d) * kMaxModes + 4 * kb);
+              const float4 wa = w4[0], wb = w4[1];
+              re[0] += tz[d] * wa.x; im[0] += tz[d] * wa.y;
+              re[1] += tz[d] * wa.z; im[1] += tz[d] * wa.w;
+              re[2] += tz[d] * wb.x; im[2] += tz[d] * wb.y;
+              re[3] += tz[d] * wb.z; im[3] += tz[d] * wb.w;
+            }
+          }
+          for (int zz = z4; zz < Z; ++zz) {
+            const float tzz = t[zz];
+#pragma unroll
+            for (int d = 0; d < 4; ++d) {
+              const float2 w = stw[zz * kMaxModes + 4 * kb + d];
+              re[d] += tzz * w.x;
+              im[d] += tzz * w.y;
+            }
           }
           const size_t b = rw / XY, xy = rw - b * XY;
-          Vz[((b * W + co) * XY + xy) * m + k] = make_float2(re, im);
+          float2* dst = Vz + ((b * W + co) * XY + xy) * m;
+#pragma unroll
+          for (int d = 0; d < 4; ++d)
+            if (4 * kb + d < m) dst[4 * kb + d] = make_float2(re[d], im[d]);
         }
       }
     }
@@ -704,10 +743,12 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
 }
 
 inline size_t row_fwd_smem(bool lift, int Z, int m) {
+  (void)m;
   const int KIN = lift ? kFeat : kMaxWidth;
   const int R = kRowThreads / Z;
-  return sizeof(float) * (kMaxWidth * KIN + kMaxWidth + 6 * kMaxWidth + 8) + sizeof(float2) * (size_t)m * (Z + 1) +
-         sizeof(float2) * (size_t)R * kMaxWidth * kMaxModes + sizeof(float) * (size_t)R * kMaxWidth * (Z + 1);
+  return sizeof(float) * (kMaxWidth * KIN + kMaxWidth + 6 * kMaxWidth + 8) + sizeof(float2) * (size_t)Z * kMaxModes +
+         sizeof(float2) * (size_t)R * kMaxWidth * kMaxModes +
+         sizeof(float) * (size_t)R * kMaxWidth * (((Z + 3) & ~3) + 4);
 }
 
 // ---------------------------------------------------------------------------
@@ -883,6 +924,10 @@ int em3d_fno_row_forward(int act, int lift, int B, int W, int X, int Y, int Z, i
   }
   cudaStream_t st = (cudaStream_t)stream;
   const size_t smem = row_fwd_smem(lift != 0, Z, m);
+  if (smem > 200 * 1024) {
+    em3d_set_last_error("row_forward: rows too short (Z < 4) for the shared-memory tile");
+    return EM3D_ERR_UNSUPPORTED;
+  }
   const int R = kRowThreads / Z;
   const size_t groups = ((size_t)B * X * Y + R - 1) / R;
   const int grid = (int)(groups < (size_t)148 * 12 ? groups : (size_t)148 * 12);

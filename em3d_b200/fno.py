@@ -154,7 +154,7 @@ class FNO:
     def forward(self, chi, wave, train: bool = False):
         """u = network(chi, wave): chi (B,3,3,X,Y,Z), wave (B,3,X,Y,Z) complex64 device tensors."""
         Z = wave.shape[-1]
-        if Z <= 128 and 2 * self.m <= Z and self.m <= 16:
+        if 4 <= Z <= 128 and 2 * self.m <= Z and self.m <= 16:
             return self._forward_rows(chi, wave, train)
         return self._forward_passes(chi, wave, train)
 
