@@ -1,24 +1,32 @@
 """Benchmark of the em3d operator-and-Krylov path on B200.
 
-Workload (default): the absorbing anisotropic ellipsoid on a 128^3 grid, k0 = 12
-(radii 0.30/0.20/0.25, eps = R diag(2.5+0.1i, 3.0+0.2i, 2.0+0.05i) R^T, R a
-seeded uniform rotation), solved to a TRUE relative residual of 1e-6.
+Headline: time to a TRUE relative residual of 1e-6 at 128^3 with mixed
+precision plus the learned warm start, against plain FP64 BiCGStab on the same
+GPU and the same problems.
 
-One step = one full solve of A u = f: FP64 defect correction (true residual
-f - A u in FP64) around FP32 BiCGStab inner solves.  ``value`` is solves/s with
-inputs resident in HBM; ``e2e`` is the same through the public API with the
-right-hand side copied from pinned host memory and the solution copied back
-inside every step.  Extra keys report the plain FP64 BiCGStab solve on the
-same GPU, the matvec throughput and the roofline of the dominant kernel (the
-FP32 EM matvec).
+Workload: held-out warm-start scenes (seeds 10000..10007: 1-5 rotated
+ellipsoids, eps_r U[1.5,4] + i U[0,0.15], k0 U[4,10], random incidence) on a
+128^3 grid.  Before timing, the warm-start network (4 Fourier layers, width
+32, 12 modes, bf16) is trained on the GPU on solver-generated 64^3 scenes
+(``--train-scenes``, ``--epochs``; the full 4000-scene protocol is
+``python -m em3d_b200.warmstart``).  One step = one solve of the next scene:
+network forward (the guess) + FP64 defect correction around FP32 BiCGStab.
+``value`` is solves/s with the scene's operator resident in HBM; ``e2e`` is the
+same with the right-hand side copied from pinned host memory and the solution
+copied back inside every step.  The same steps are timed for FP64 BiCGStab
+from the zero guess (``fp64``) and for the mixed solve without the network
+(``mixed_zero``).  The anisotropic absorbing ellipsoid (128^3, k0 = 12) is
+reported under ``aniso_ellipsoid``, and the roofline of the dominant kernel
+(the FP32 EM matvec) under ``roofline``.
 
 Multi-GPU: the path does not shard (one problem per GPU); ``--gpus N`` runs N
 independent replicas (weak scaling) and reports the total solve rate.
 
 ``--impl reference`` times the reference's own NumPy CPU path (the installed
 copy in baseline/_ref when importable, otherwise the CPU oracle port) on the
-same 128^3 problem: each step is one complex128 ``Operator.matvec``, converted
-to solves/s with the matvec count of the FP64 BiCGStab solve.
+first scene: each step is one complex128 ``Operator.matvec``, converted to
+solves/s with the mean matvec count of the FP64 BiCGStab solves of these
+scenes measured on B200.
 """
 from __future__ import annotations
 
@@ -36,12 +44,14 @@ sys.path.insert(0, ROOT)
 
 N_GRID = 128
 RTOL = 1e-6
-METRIC = "em_solves_per_s_128^3_true_rtol1e-6"
+METRIC = "time_to_true_rtol1e-6_128^3_mixed+nn_solves_per_s"
 UNIT = "solves/s"
-# FP64 BiCGStab matvecs per solve of this workload to rtol 1e-6 (measured on
-# B200 by this script's fp64 leg: 24 iterations, 48 matvecs); used only by the
-# reference arm to convert a CPU matvec timing into solves/s.
-FP64_MATVECS_PER_SOLVE = 48
+SCENE_SEEDS = list(range(10000, 10008))
+# Mean FP64 BiCGStab matvecs per solve to true rtol 1e-6 of the scenes a
+# default run times (seeds 10000..10004; measured on B200 by this script's
+# fp64 leg); used only by the reference arm to convert a CPU matvec timing
+# into solves/s.
+FP64_MATVECS_PER_SOLVE = 29.6
 # dram__bytes_read.sum + dram__bytes_write.sum per complex64 EM matvec (all
 # five passes) from the ncu launch list summarised in profiles/em_matvec_128.md.
 NCU_TRAFFIC_BYTES = 1495.4e6
@@ -182,13 +192,29 @@ def reference_matvec_timer(case):
     return (lambda: oem.matvec(case.chi, case.wave, kh, case.N)), "port", build_s
 
 
+def scene_case(seed: int, n: int = N_GRID):
+    """A warm-start scene as host complex128 arrays (the oracle's restatement
+    of the device sampler, bit-exact with it), for the CPU legs."""
+    from em3d_b200 import setup, warmstart, workloads
+    from oracle import materials as om
+
+    sc = warmstart.random_scene(seed)
+    N, L, c = (n, n, n), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0)
+    axes = setup.grid_axes_host(N, L, c, "double")
+    import numpy as np
+
+    packed = np.stack([s.packed() for s in sc.shapes])
+    chi = om.sample_contrast(axes, packed, om.em_tol(L), 1.0, np.complex128)
+    wave = om.plane_wave(axes, sc.k0, sc.direction, sc.polarisation)
+    return workloads.EMCase(f"warmstart_scene_{seed}_{n}^3", N, L, c, sc.k0, chi, wave)
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
     import numpy as np
-    from em3d_b200 import workloads
 
-    case = workloads.aniso_ellipsoid_em(N_GRID, "double")
+    case = scene_case(SCENE_SEEDS[0])
     fn, kind, build_s = reference_matvec_timer(case)
     for _ in range(args.warmup):
         fn()
@@ -198,15 +224,17 @@ def run_reference(args, world, rank):
         fn()
         times.append(time.perf_counter() - t0)
     t_mv = float(np.median(times))
-    mps = FP64_MATVECS_PER_SOLVE or 1
+    mps = FP64_MATVECS_PER_SOLVE
     value = 1.0 / (t_mv * mps)
-    sample = (f"one complex128 Operator.matvec per step at {N_GRID}^3 (NumPy, single-threaded FFT), "
-              f"x {mps} matvecs per FP64 BiCGStab solve to rtol {RTOL}; kernel build {build_s:.1f} s excluded")
+    sample = (f"one complex128 Operator.matvec per step on scene {SCENE_SEEDS[0]} at {N_GRID}^3 (NumPy, "
+              f"single-threaded FFT), x {mps} matvecs per FP64 BiCGStab solve to true rtol {RTOL} (mean over "
+              f"the benchmark scenes, measured on B200); kernel build {build_s:.1f} s excluded")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mv * 1e3, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mv * 1e3 * mps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": case.name, "k0": case.k0, "rtol": RTOL, "precision": "complex128"},
+        "config": {"workload": f"warmstart_heldout_scenes_{N_GRID}^3", "scene": SCENE_SEEDS[0], "rtol_true": RTOL,
+                   "precision": "complex128", "solver": "reference NumPy matvec x FP64 BiCGStab matvec count"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_matvec_s": t_mv,
@@ -218,127 +246,183 @@ def run_reference(args, world, rank):
 # B200 leg
 # ---------------------------------------------------------------------------
 
+def _events_ms(fn):
+    """CUDA-event time (ms) of ``fn()`` on the current stream and its result."""
+    import torch
+
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    out = fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b), out
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
 
     import em3d_b200 as e
-    from em3d_b200 import _lib, workloads
+    from em3d_b200 import _lib, warmstart as ws, workloads
+    from em3d_b200.fno import FNO
     from em3d_b200.solvers import BiCGStab, DefectCorrection, SolverConfig, true_relative_residual
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    case = workloads.aniso_ellipsoid_em(N_GRID, "double")
-    be64 = e.Backend.b200(e.Precision.DOUBLE, device_index=local)
-    grid = e.Grid(N=case.N, L=case.L, center=case.center, backend=be64)
-    prob = e.Problem(grid=grid, eps_tensor=case.chi, wave=case.wave, k0=case.k0, volume=1.0)
-    op64 = e.Operator(prob)
-    op32 = op64.with_precision(e.Precision.SINGLE)
-    rhs = prob.wave
-    solver = DefectCorrection(SolverConfig(max_iter=2000, rtol=RTOL), inner="bicgstab")
 
-    def step(f):
-        return solver.solve(op64, f, operator_low=op32)
+    def log(msg):
+        if rank == 0:
+            print(f"[bench] {msg}", file=sys.stderr, flush=True)
 
-    # warm-up (also captures the CUDA graphs of the inner loops)
-    res = None
-    for _ in range(max(args.warmup, 1)):
-        res = step(rhs)
-    barrier(world)
+    # -- 1. the warm-start network, trained here on solver-generated 64^3 scenes (untimed set-up)
+    t0 = time.perf_counter()
+    data = ws.generate(range(args.train_scenes), 64, device_index=local)
+    gen_s = time.perf_counter() - t0
+    net = FNO(width=32, modes=12, layers=4, act="bf16", seed=0, device=dev)
+    t1 = time.perf_counter()
+    hist = ws.train(net, data, epochs=args.epochs, batch=4, lr=1e-3, device_index=local)
+    train_s = time.perf_counter() - t1
+    log(f"warm start: {args.train_scenes} scenes generated in {gen_s:.1f} s, {args.epochs} epochs in {train_s:.1f} s, "
+        f"loss {hist[0]:.4f} -> {hist[-1]:.4f}")
+    del data
+    torch.cuda.empty_cache()
+
+    # -- 2. the held-out scenes at 128^3, operators built once (FP64 spectrum, FP32 twin)
+    grid = ws.unit_grid(N_GRID, e.Precision.DOUBLE, local)
+    scenes = []
+    for seed in SCENE_SEEDS:
+        prob = ws.scene_problem(ws.random_scene(seed), grid)
+        op64 = e.Operator(prob)
+        scenes.append((prob, op64, op64.with_precision(e.Precision.SINGLE)))
+    K = len(scenes)
+    cfg = SolverConfig(max_iter=2000, rtol=RTOL)
+    dc = DefectCorrection(cfg)
+    dc.max_cached = K + 1
+    bic = BiCGStab(cfg)
+    bic.max_cached_engines = K + 1
+
+    def mixed_nn(i, f=None):
+        prob, op64, op32 = scenes[i]
+        f = prob.wave if f is None else f
+        return dc.solve(op64, f, x0=ws.guess(net, prob, wave=f), operator_low=op32)
+
+    def mixed_zero(i):
+        prob, op64, op32 = scenes[i]
+        return dc.solve(op64, prob.wave, operator_low=op32)
+
+    def fp64(i):
+        prob, op64, _ = scenes[i]
+        return bic.solve(op64, prob.wave)
+
+    # warm-up: every scene once per leg (captures the CUDA graphs), then W headline steps
+    for i in range(K):
+        mixed_nn(i)
+        mixed_zero(i)
+        fp64(i)
+    for w in range(max(args.warmup, 1)):
+        mixed_nn(w % K)
+
+    def timed(fn):
+        barrier(world)
+        ms, res = _events_ms(lambda: [fn(s % K) for s in range(args.steps)])
+        barrier(world)
+        return max_over_ranks(world, ms / args.steps), res
+
     sampler = ClockSampler(local)
     sampler.start()
     launches0 = _lib.launch_count
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record()
-    for _ in range(args.steps):
-        res = step(rhs)
-    t_end.record()
-    barrier(world)
-    clocks = sampler.stop()
+    ms, res_nn = timed(mixed_nn)
     launches = _lib.launch_count - launches0
-    ms = t_start.elapsed_time(t_end) / args.steps
-    ms = max_over_ranks(world, ms)
+    clocks = sampler.stop()
     value = world * 1000.0 / ms
-    true_res = true_relative_residual(op64, res.u, rhs)
+    fp64_ms, res64 = timed(fp64)
+    zero_ms, res0 = timed(mixed_zero)
 
-    # end to end through the public API: pinned host rhs in, solution out
-    host_rhs = torch.from_numpy(case.wave).pin_memory()
-    host_u = torch.empty(host_rhs.shape, dtype=host_rhs.dtype).pin_memory()
-    for _ in range(1):
-        d = host_rhs.to(dev, non_blocking=True)
-        host_u.copy_(step(d).u, non_blocking=True)
-    barrier(world)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        d = host_rhs.to(dev, non_blocking=True)
-        host_u.copy_(step(d).u, non_blocking=True)
-    e1.record()
-    barrier(world)
-    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1) / args.steps)
+    def true_max(results):
+        return max(float(true_relative_residual(scenes[s % K][1], r.u, scenes[s % K][0].wave))
+                   for s, r in enumerate(results))
 
-    # plain FP64 BiCGStab on the same GPU (the comparison path)
-    fp64 = BiCGStab(SolverConfig(max_iter=2000, rtol=RTOL))
-    r64 = fp64.solve(op64, rhs)
-    barrier(world)
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record()
-    r64 = fp64.solve(op64, rhs)
-    f1.record()
-    torch.cuda.synchronize()
-    fp64_ms = f0.elapsed_time(f1)
-    fp64_true = true_relative_residual(op64, r64.u, rhs)
+    # -- 3. end to end through the public API: pinned host rhs in, solution out
+    host_rhs = [torch.empty(p.wave.shape, dtype=p.wave.dtype).pin_memory() for p, _, _ in scenes]
+    for h, (p, _, _) in zip(host_rhs, scenes):
+        h.copy_(p.wave.cpu())
+    host_u = torch.empty(host_rhs[0].shape, dtype=host_rhs[0].dtype).pin_memory()
 
-    # matvec timing (dominant kernel): CUDA events on the launching stream
+    def e2e_step(i):
+        d = host_rhs[i].to(dev, non_blocking=True)
+        host_u.copy_(mixed_nn(i, d).u, non_blocking=True)
+
+    e2e_step(0)
+    barrier(world)
+    e2e_ms, _ = _events_ms(lambda: [e2e_step(s % K) for s in range(args.steps)])
+    e2e_ms = max_over_ranks(world, e2e_ms / args.steps)
+
+    # -- 4. the anisotropic absorbing ellipsoid (128^3, k0 = 12): mixed vs FP64, no network
+    case = workloads.aniso_ellipsoid_em(N_GRID, "double")
+    be64 = e.Backend.b200(e.Precision.DOUBLE, device_index=local)
+    g2 = e.Grid(N=case.N, L=case.L, center=case.center, backend=be64)
+    p2 = e.Problem(grid=g2, eps_tensor=case.chi, wave=case.wave, k0=case.k0, volume=1.0)
+    a64 = e.Operator(p2)
+    a32 = a64.with_precision(e.Precision.SINGLE)
+    dc2 = DefectCorrection(cfg)
+    bic2 = BiCGStab(cfg)
+    for _ in range(2):
+        r2 = dc2.solve(a64, p2.wave, operator_low=a32)
+        b2 = bic2.solve(a64, p2.wave)
+    aniso_mixed_ms, r2 = _events_ms(lambda: dc2.solve(a64, p2.wave, operator_low=a32))
+    aniso_fp64_ms, b2 = _events_ms(lambda: bic2.solve(a64, p2.wave))
+
+    # -- 5. matvec timing (dominant kernel): CUDA events on the launching stream
     def time_matvec(op, reps=20):
         x = op.problem.wave
         out = torch.empty_like(x)
         for _ in range(3):
             op.apply_into(x, out)
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(reps):
-            op.apply_into(x, out)
-        b.record()
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / reps
+        ms_, _ = _events_ms(lambda: [op.apply_into(x, out) for _ in range(reps)])
+        return ms_ / reps
 
-    mv32_ms = time_matvec(op32)
-    mv64_ms = time_matvec(op64)
+    mv32_ms = time_matvec(a32)
+    mv64_ms = time_matvec(a64)
     peak, peak_kind = load_peaks()
     bytes32 = byte_model(N_GRID, 8)
     bytes64 = byte_model(N_GRID, 16)
     ach32 = bytes32 / (mv32_ms * 1e-3) / 1e9
     ach64 = bytes64 / (mv64_ms * 1e-3) / 1e9
+    mv_per_solve = float(np.mean([r.matvec_count for r in res64]))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        fn, kind, build_s = reference_matvec_timer(workloads.aniso_ellipsoid_em(N_GRID, "double"))
+        fn, kind, build_s = reference_matvec_timer(scene_case(SCENE_SEEDS[0]))
         fn()
         t0 = time.perf_counter()
         fn()
         t_mv = time.perf_counter() - t0
-        mps = r64.matvec_count
-        cpu = {"value": 1.0 / (t_mv * mps), "unit": UNIT, "cores": 1, "kind": kind,
-               "sample": (f"one complex128 Operator.matvec at {N_GRID}^3 ({t_mv:.2f} s, NumPy single-threaded "
-                          f"FFT) x {mps} matvecs of the FP64 BiCGStab solve measured here; build {build_s:.1f} s "
-                          f"excluded")}
+        cpu = {"value": 1.0 / (t_mv * mv_per_solve), "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": (f"one complex128 Operator.matvec on scene {SCENE_SEEDS[0]} at {N_GRID}^3 ({t_mv:.2f} s, "
+                          f"NumPy single-threaded FFT) x {mv_per_solve:.1f} matvecs (mean FP64 BiCGStab solve of "
+                          f"the benchmark scenes, measured here); build {build_s:.1f} s excluded")}
     if rank != 0:
         return
+
+    def summary(results):
+        return {"iterations_mean": float(np.mean([r.iterations for r in results])),
+                "matvecs_mean": float(np.mean([r.matvec_count for r in results])),
+                "converged": int(sum(r.converged for r in results)), "true_residual_max": true_max(results)}
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64 inner / c128 outer", "data": "synthetic",
-        "config": {"workload": case.name, "k0": case.k0, "rtol_true": RTOL,
-                   "solver": "FP64 defect correction + FP32 BiCGStab", "parallelism": f"replicas x{world}",
-                   "l2": "inputs and workspaces (~2 GB per solve) exceed the 126 MB L2"},
+        "vs_baseline": None, "dtype": "c64 inner / c128 outer, bf16 network", "data": "synthetic",
+        "config": {"workload": f"warmstart_heldout_scenes_{N_GRID}^3", "scenes": SCENE_SEEDS, "rtol_true": RTOL,
+                   "solver": "network guess + FP64 defect correction around FP32 BiCGStab",
+                   "network": {"layers": 4, "width": 32, "modes": 12, "train_scenes": args.train_scenes,
+                               "train_grid": 64, "epochs": args.epochs, "loss_first_last": [hist[0], hist[-1]],
+                               "generate_s": gen_s, "train_s": train_s},
+                   "parallelism": f"replicas x{world}",
+                   "l2": "each solve's operator, fields and workspaces (~2 GB) exceed the 126 MB L2"},
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT,
-                "h2d_bytes_per_step": int(host_rhs.numel() * host_rhs.element_size()),
+                "h2d_bytes_per_step": int(host_rhs[0].numel() * host_rhs[0].element_size()),
                 "d2h_bytes_per_step": int(host_u.numel() * host_u.element_size())},
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
                      "traffic": NCU_TRAFFIC_BYTES, "kernel": "em3d_em_matvec FP32 (5 fused passes)",
@@ -346,14 +430,18 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
-        "solve": {"status": res.status, "outer": res.outer_iterations, "inner_iterations": res.inner_iterations,
-                  "fp32_matvecs": res.fp32_matvecs, "fp64_matvecs": res.fp64_matvecs, "true_residual": true_res},
-        "fp64_bicgstab": {"ms": fp64_ms, "status": r64.status, "iterations": r64.iterations,
-                          "matvecs": r64.matvec_count, "true_residual": fp64_true},
+        "mixed_nn": summary(res_nn),
+        "fp64": dict(summary(res64), ms=fp64_ms, solves_per_s=world * 1000.0 / fp64_ms),
+        "mixed_zero": dict(summary(res0), ms=zero_ms, solves_per_s=world * 1000.0 / zero_ms),
         "speedup_vs_fp64": fp64_ms / ms,
+        "speedup_mixed_zero_vs_fp64": fp64_ms / zero_ms,
+        "aniso_ellipsoid": {"workload": case.name, "k0": case.k0, "mixed_ms": aniso_mixed_ms,
+                            "fp64_ms": aniso_fp64_ms, "speedup": aniso_fp64_ms / aniso_mixed_ms,
+                            "mixed_inner_iterations": r2.inner_iterations, "fp64_iterations": b2.iterations,
+                            "mixed_true_residual": float(true_relative_residual(a64, r2.u, p2.wave)),
+                            "fp64_true_residual": float(true_relative_residual(a64, b2.u, p2.wave))},
         "matvec": {"fp32_ms": mv32_ms, "fp64_ms": mv64_ms, "fp32_gbs": ach32, "fp64_gbs": ach64,
-                   "fp32_per_s": 1000.0 / mv32_ms, "fp64_per_s": 1000.0 / mv64_ms,
-                   "fp64_frac": ach64 / peak},
+                   "fp32_per_s": 1000.0 / mv32_ms, "fp64_per_s": 1000.0 / mv64_ms, "fp64_frac": ach64 / peak},
     }
     print(json.dumps(line), flush=True)
 
@@ -365,6 +453,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--train-scenes", type=int, default=1000, help="warm-start training scenes (64^3)")
+    ap.add_argument("--epochs", type=int, default=4, help="warm-start training epochs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -187,12 +187,13 @@ def load(path: str, act: str = "bf16") -> FNO:
 
 
 # ----------------------------------------------------------- warm start
-def guess(net: FNO, problem: Problem):
-    """The network's u for ``problem``, in the problem's dtype (3, N, N, N)."""
+def guess(net: FNO, problem: Problem, wave=None):
+    """The network's u for ``problem`` (incident field ``wave``, default the
+    problem's own), in the problem's dtype (3, N, N, N)."""
     import torch
 
     chi = problem.eps_tensor.to(torch.complex64).unsqueeze(0)
-    wave = problem.wave.to(torch.complex64).unsqueeze(0)
+    wave = (problem.wave if wave is None else wave).to(torch.complex64).unsqueeze(0)
     return net.forward(chi, wave, train=False)[0].to(problem.wave.dtype)
 
 
