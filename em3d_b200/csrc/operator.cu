@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <unordered_set>
@@ -640,7 +641,7 @@ static int ac_kernel_hat_full(const em3d_grid* g, const Dims& d, double k0, int 
 
 // Tuning knobs (em3d_set_tuning / em3d_get_tuning).  They select among
 // equivalent implementations; results do not depend on them beyond rounding.
-static int g_tuning[EM3D_TUNE_COUNT] = {0, 0};
+static int g_tuning[EM3D_TUNE_COUNT] = {-1, 0};
 
 static bool generic_forced() {
   const char* v = getenv("EM3D_FFT_GENERIC");
@@ -720,6 +721,31 @@ static int go_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d,
   return EM3D_OK;
 }
 
+template <typename R, int L, int C, bool ADJ, int E, int NTT>
+static int go_xpipe(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
+                    cudaStream_t st) {
+  using G = XpipeGeom<L, E, C, NTT>;
+  auto kern = kf_xmul_pipe<R, L, C, ADJ, E, NTT>;
+  EM3D_CUDA_TRY(allow_smem(kern));
+  const size_t smem = (size_t)G::TOTAL * sizeof(cx<R>);
+  const int ntz = (2 * d.nz + G::P - 1) / G::P;
+  const long long ntiles = (long long)batch * 2 * d.ny * ntz;
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    EM3D_CUDA_TRY(cudaGetDevice(&dev));
+    EM3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  int per_sm = 0;
+  EM3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, G::NT, smem));
+  if (per_sm < 1) per_sm = 1;
+  const long long grid = std::min<long long>(ntiles, (long long)sms * per_sm);
+  if (grid <= 0) return EM3D_OK;
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, skip);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
 template <typename R, int L, bool ADJ, int E>
 static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
                      cudaStream_t st) {
@@ -736,17 +762,25 @@ static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& 
 
 // x-pass variant (tuning key EM3D_TUNE_XPASS_VARIANT): 0 = three components
 // in registers, 256-thread CTAs; 1 = the same with 128-thread CTAs (two per
-// SM); 2 = component-split threads (EM only).
-static int xmul_variant() { return g_tuning[EM3D_TUNE_XPASS_VARIANT]; }
+// SM); 2 = component-split threads (EM only); 3 = persistent CTAs with the
+// next tile's field and spectrum prefetched by cp.async, 256 threads; 4 = the
+// same with 128 threads.  -1 (the default) picks 3 for EM and 0 for the
+// scalar acoustic operator, the fastest of each on B200 at 128^3 / 256^3.
+static int xmul_variant(int C) {
+  const int v = g_tuning[EM3D_TUNE_XPASS_VARIANT];
+  return v >= 0 ? v : (C == 3 ? 3 : 0);
+}
 
 template <typename R, int C, bool ADJ, int L>
 static int launch_xmul_len(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
                            const int* skip, cudaStream_t st) {
   constexpr int EB = FastE<R>::E;
-  const int v = xmul_variant();
+  const int v = xmul_variant(C);
   if constexpr (C == 3) {
     if (v == 2) return go_xsplit<R, L, ADJ, EB>(T2, spec, tw, d, batch, skip, st);
   }
+  if (v == 3) return go_xpipe<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st);
+  if (v == 4) return go_xpipe<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st);
   if (v == 1) return go_xmul<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st);
   return go_xmul<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st);
 }
@@ -848,8 +882,8 @@ extern "C" {
 
 int em3d_set_tuning(int key, int value) {
   if (key < 0 || key >= EM3D_TUNE_COUNT) { em3d_set_last_error("unknown tuning key"); return EM3D_ERR_INVALID; }
-  if (key == EM3D_TUNE_XPASS_VARIANT && (value < 0 || value > 2)) {
-    em3d_set_last_error("x-pass variant must be 0, 1 or 2");
+  if (key == EM3D_TUNE_XPASS_VARIANT && (value < -1 || value > 4)) {
+    em3d_set_last_error("x-pass variant must be -1 (automatic) or 0 .. 4");
     return EM3D_ERR_INVALID;
   }
   g_tuning[key] = value;

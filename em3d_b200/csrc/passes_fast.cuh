@@ -339,6 +339,183 @@ kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg
 }
 
 // ---------------------------------------------------------------------------
+// Pipelined x pass: a persistent CTA loops over (batch, ky, kz-tile) tiles and
+// prefetches the next tile's field slab (C x Nx x P) and spectrum slab
+// (6 or 1 x (Nx+1) x P, octant-folded) into shared memory with cp.async while
+// it transforms the current tile, so the global loads overlap the FFTs.
+//
+// Per tile:  wait field(i) -> registers -> prefetch field(i+1) -> forward FFT
+//            -> wait spectrum(i) -> 3x3 multiply -> prefetch spectrum(i+1)
+//            -> reversed inverse FFT -> crop and store (in place; tiles are
+//            disjoint, so the prefetch never reads what another tile writes).
+// Exactly two cp.async groups are committed per tile (empty ones at the end),
+// so "wait until at most one group is pending" always targets the right one.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void cp_async_el(void* dst, const void* src, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (bytes == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+template <int L, int E, int C, int NTT> struct XpipeGeom {
+  static constexpr int TT = L / E;
+  static constexpr int P = (NTT / TT) > 32 ? 32 : ((NTT / TT) >= 2 ? (NTT / TT) : 2);
+  static constexpr int NT = P * TT;
+  static constexpr int S = (P & 1) ? P : P + 1;
+  static constexpr int NX = L / 2;
+  static constexpr int NSPEC = C == 3 ? 6 : 1;
+  static constexpr int TW = L;
+  static constexpr int EXCH = L * S;
+  static constexpr int FIELD = C * NX * P;
+  static constexpr int SPEC = NSPEC * (NX + 1) * P;
+  static constexpr int TOTAL = TW + EXCH + FIELD + SPEC;   // complex elements of shared memory
+};
+
+template <typename R, int L, int C, bool ADJ, int E, int NTT>
+__global__ void __launch_bounds__(XpipeGeom<L, E, C, NTT>::NT)
+kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
+             int nb, const int* skip) {
+  using T = cx<R>;
+  using G = XpipeGeom<L, E, C, NTT>;
+  using PL = RegPlan<L, E>;
+  constexpr int TT = G::TT, PP = G::P, S = G::S, NX = G::NX, NSP = G::NSPEC;
+  constexpr int R1 = PL::first(false), RL = PL::last(false);
+  constexpr int M1 = L / R1, ML = L / RL;
+  constexpr int EB = (int)sizeof(T);
+  if (skip_launch(skip)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tw = reinterpret_cast<T*>(smem_raw);
+  T* sm = tw + G::TW;
+  T* sfield = sm + G::EXCH;
+  T* sspec = sfield + G::FIELD;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
+  const int p = threadIdx.x % PP, t = threadIdx.x / PP;
+  const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
+  const size_t xstride = (size_t)Ny2 * Nz2;
+  const size_t ostride = (size_t)(NX + 1) * (Ny + 1) * (Nz + 1);
+  const int ntiles = nb * Ny2 * ntz;
+
+  auto decode = [&](int tile, int& b, int& ky, int& kz0) {
+    b = tile % nb;
+    const int idx = tile / nb;
+    kz0 = (idx % ntz) * PP;
+    ky = idx / ntz;
+  };
+  auto issue_field = [&](int tile) {
+    int b, ky, kz0;
+    decode(tile, b, ky, kz0);
+    const T* base = T2 + (size_t)b * C * NX * xstride + (size_t)ky * Nz2;
+    for (int i = threadIdx.x; i < G::FIELD; i += blockDim.x) {
+      const int q = i % PP, row = i / PP;   // row = c * NX + x
+      const int kz = kz0 + q;
+      if (kz < Nz2) cp_async_el(sfield + i, base + (size_t)row * xstride + kz, EB);
+      else sfield[i] = mk<R>(0, 0);
+    }
+  };
+  auto issue_spec = [&](int tile) {
+    int b, ky, kz0;
+    decode(tile, b, ky, kz0);
+    const int jy = kfold(ky, Ny);
+    const T* base = spec + (size_t)jy * (Nz + 1);
+    for (int i = threadIdx.x; i < G::SPEC; i += blockDim.x) {
+      const int q = i % PP, row = i / PP;   // row = component * (NX + 1) + ix
+      const int sc = row / (NX + 1), ix = row - sc * (NX + 1);
+      const int kz = kz0 + q;
+      if (kz < Nz2) cp_async_el(sspec + i, base + sc * ostride + (size_t)ix * (Ny + 1) * (Nz + 1) + kfold(kz, Nz), EB);
+      else sspec[i] = mk<R>(0, 0);
+    }
+  };
+
+  const int tile0 = blockIdx.x;
+  if (tile0 < ntiles) issue_field(tile0);
+  cp_async_commit();
+  if (tile0 < ntiles) issue_spec(tile0);
+  cp_async_commit();
+  const LayInter lay{p, S, 0};
+
+  for (int tile = tile0; tile < ntiles; tile += gridDim.x) {
+    int b, ky, kz0;
+    decode(tile, b, ky, kz0);
+    const int kz = kz0 + p;
+    const bool valid = kz < Nz2;
+    const int next = tile + gridDim.x;
+
+    cp_async_wait_one();  // this tile's field slab
+    __syncthreads();
+    T a[C][E];
+#pragma unroll
+    for (int q = 0; q < E / R1; ++q) {
+      const int j = t + q * TT;
+#pragma unroll
+      for (int r = 0; r < R1; ++r) {
+        const int x = j + r * M1;
+#pragma unroll
+        for (int c = 0; c < C; ++c) a[c][q * R1 + r] = r < R1 / 2 ? sfield[(c * NX + x) * PP + p] : mk<R>(0, 0);
+      }
+    }
+    __syncthreads();
+    if (next < ntiles) issue_field(next);
+    cp_async_commit();
+
+    reg_fft_x<L, E, false, false, true, C>(a, t, sm, tw, lay);
+
+    cp_async_wait_one();  // this tile's spectrum slab
+    __syncthreads();
+    const R sy = ky <= Ny ? (R)1 : (R)-1;
+    const R sz = kz <= Nz ? (R)1 : (R)-1;
+#pragma unroll
+    for (int q = 0; q < E / RL; ++q) {
+      const int j = t + q * TT;
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int kx = j + r * ML;
+        const T* s0 = sspec + kfold(kx, NX) * PP + p;
+        const int e = q * RL + r;
+        if constexpr (C == 1) {
+          const T k0 = s0[0];
+          a[0][e] = ADJ ? cmulcj(k0, a[0][e]) : cmul(k0, a[0][e]);
+        } else {
+          constexpr int OS = (NX + 1) * PP;
+          const R sx = kx <= NX ? (R)1 : (R)-1;
+          T kxx = s0[0], kyy = s0[OS], kzz = s0[2 * OS];
+          T kxy = cscale(s0[3 * OS], sx * sy);
+          T kxz = cscale(s0[4 * OS], sx * sz);
+          T kyz = cscale(s0[5 * OS], sy * sz);
+          if (ADJ) { kxx = cconj(kxx); kyy = cconj(kyy); kzz = cconj(kzz); kxy = cconj(kxy); kxz = cconj(kxz); kyz = cconj(kyz); }
+          const T X0 = a[0][e], X1 = a[1][e], X2 = a[2][e];
+          a[0][e] = cadd(cadd(cmul(kxx, X0), cmul(kxy, X1)), cmul(kxz, X2));
+          a[1][e] = cadd(cadd(cmul(kxy, X0), cmul(kyy, X1)), cmul(kyz, X2));
+          a[2][e] = cadd(cadd(cmul(kxz, X0), cmul(kyz, X1)), cmul(kzz, X2));
+        }
+      }
+    }
+    __syncthreads();
+    if (next < ntiles) issue_spec(next);
+    cp_async_commit();
+
+    reg_fft_x<L, E, true, true, true, C>(a, t, sm, tw, lay);
+    if (valid) {
+      T* col = T2 + (size_t)b * C * NX * xstride + (size_t)ky * Nz2 + kz;
+#pragma unroll
+      for (int q = 0; q < E / R1; ++q) {
+        const int j = t + q * TT;
+#pragma unroll
+        for (int r = 0; r < R1 / 2; ++r) {
+          const int x = j + r * M1;
+#pragma unroll
+          for (int c = 0; c < C; ++c) col[((size_t)c * NX + x) * xstride] = a[c][q * R1 + r];
+        }
+      }
+    }
+  }
+  cp_async_wait_all();
+}
+
+// ---------------------------------------------------------------------------
 // Component-split x pass (EM only): each thread transforms one component
 // pencil slice, so a thread holds E elements instead of 3E; the 3x3 dyadic
 // multiply reads the other two components of the same frequency through

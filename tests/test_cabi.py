@@ -94,3 +94,15 @@ def test_solver_config_mirrors_reference_defaults():
         SolverConfig(mu=0j, radius=1.0).require_gamma()
     r = SolverResult(u=None, iterations=1, residual_history=[1.0], converged=False, matvec_count=2, rmatvec_count=3)
     assert r.operator_action_count == 5
+
+
+def test_tuning_keys_validate_without_gpu():
+    from em3d_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT) == -1   # automatic by default
+    assert lib.em3d_set_tuning(_lib.EM3D_TUNE_XPASS_VARIANT, 5) == _lib.EM3D_ERR_INVALID
+    assert "variant" in _lib.last_error()
+    for v in (3, 4, 0, -1):
+        assert lib.em3d_set_tuning(_lib.EM3D_TUNE_XPASS_VARIANT, v) == 0
+        assert lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT) == v

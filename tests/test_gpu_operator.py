@@ -216,12 +216,12 @@ def test_register_fft_path_matches_generic_path(prec, kind, monkeypatch):
         _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 1)
         gen_mv, gen_rmv = op.matvec(u), op.rmatvec(u)
         _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 0)
-        for v in (0, 1, 2):
+        for v in (0, 1, 2, 3, 4):
             set_xpass_variant(v)
             fast_mv, fast_rmv = op.matvec(u), op.rmatvec(u)
             assert rel_err(be.to_host(fast_mv), be.to_host(gen_mv)) < tol, (N, v)
             assert rel_err(be.to_host(fast_rmv), be.to_host(gen_rmv)) < tol, (N, v)
-        set_xpass_variant(0)
+        set_xpass_variant(-1)
     del rng
 
 
@@ -266,10 +266,15 @@ def test_batched_matvec_equals_single_register_path(N, prec):
     U = torch.randn((7, 3) + N, dtype=tc, device="cuda", generator=gen)
     op = e.Operator(e.Problem(grid=grid, eps_tensor=chi, wave=U[0], k0=5.0, volume=1.0))
     tol = 1e-14 if prec == "double" else 1e-6
-    Y, Ya = op.matvec(U), op.rmatvec(U)
-    for b in range(7):
-        assert rel_err(be.to_host(Y[b]), be.to_host(op.matvec(U[b]))) < tol, b
-        assert rel_err(be.to_host(Ya[b]), be.to_host(op.rmatvec(U[b]))) < tol, b
+    from em3d_b200.tune import set_xpass_variant
+
+    for v in (0, 3, 4):
+        set_xpass_variant(v)
+        Y, Ya = op.matvec(U), op.rmatvec(U)
+        for b in range(7):
+            assert rel_err(be.to_host(Y[b]), be.to_host(op.matvec(U[b]))) < tol, (v, b)
+            assert rel_err(be.to_host(Ya[b]), be.to_host(op.rmatvec(U[b]))) < tol, (v, b)
+    set_xpass_variant(-1)
     eta = (1.0 + torch.rand(N, dtype=tc, device="cuda", generator=gen)).contiguous()
     aop = ea.AcousticOperator(ea.make_acoustic_problem(grid, eta, k0=6.0))
     V = torch.randn((5,) + N, dtype=tc, device="cuda", generator=gen)
