@@ -10,7 +10,9 @@ ellipsoids, eps_r U[1.5,4] + i U[0,0.15], k0 U[4,10], random incidence) on a
 32, 12 modes, bf16) is trained on the GPU on solver-generated 64^3 scenes
 (``--train-scenes``, ``--epochs``; the full 4000-scene protocol is
 ``python -m em3d_b200.warmstart``).  One step = one solve of the next scene:
-network forward (the guess) + FP64 defect correction around FP32 BiCGStab.
+network forward (the guess) + FP32 BiCGStab with FP64 reliable updates (the
+solution and the true residual f - A u in FP64, which is also the stopping
+test).
 ``value`` is solves/s with the scene's operator resident in HBM; ``e2e`` is the
 same with the right-hand side copied from pinned host memory and the solution
 copied back inside every step.  The same steps are timed for FP64 BiCGStab
@@ -139,23 +141,29 @@ def dist_setup(n_gpus: int):
 
 
 def barrier(world):
+    """Device synchronize plus a process-group barrier (N > 1)."""
     import torch
 
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
 
         dist.barrier()
-        torch.cuda.synchronize()
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
 
 
 def max_over_ranks(world, value: float) -> float:
+    """The maximum of ``value`` over the ranks (the job's time is the slowest
+    replica's); NCCL on the GPUs, or the CPU process group (gloo) in tests."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -266,7 +274,7 @@ def run_ours(args, world, rank, local):
     import em3d_b200 as e
     from em3d_b200 import _lib, warmstart as ws, workloads
     from em3d_b200.fno import FNO
-    from em3d_b200.solvers import BiCGStab, DefectCorrection, SolverConfig, true_relative_residual
+    from em3d_b200.solvers import BiCGStab, MixedBiCGStab, SolverConfig, true_relative_residual
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -297,7 +305,7 @@ def run_ours(args, world, rank, local):
         scenes.append((prob, op64, op64.with_precision(e.Precision.SINGLE)))
     K = len(scenes)
     cfg = SolverConfig(max_iter=2000, rtol=RTOL)
-    dc = DefectCorrection(cfg)
+    dc = MixedBiCGStab(cfg)
     dc.max_cached = K + 1
     bic = BiCGStab(cfg)
     bic.max_cached_engines = K + 1
@@ -365,7 +373,7 @@ def run_ours(args, world, rank, local):
     p2 = e.Problem(grid=g2, eps_tensor=case.chi, wave=case.wave, k0=case.k0, volume=1.0)
     a64 = e.Operator(p2)
     a32 = a64.with_precision(e.Precision.SINGLE)
-    dc2 = DefectCorrection(cfg)
+    dc2 = MixedBiCGStab(cfg)
     bic2 = BiCGStab(cfg)
     for _ in range(2):
         r2 = dc2.solve(a64, p2.wave, operator_low=a32)
@@ -415,7 +423,7 @@ def run_ours(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 inner / c128 outer, bf16 network", "data": "synthetic",
         "config": {"workload": f"warmstart_heldout_scenes_{N_GRID}^3", "scenes": SCENE_SEEDS, "rtol_true": RTOL,
-                   "solver": "network guess + FP64 defect correction around FP32 BiCGStab",
+                   "solver": "network guess + FP32 BiCGStab with FP64 reliable updates (true residual in FP64)",
                    "network": {"layers": 4, "width": 32, "modes": 12, "train_scenes": args.train_scenes,
                                "train_grid": 64, "epochs": args.epochs, "loss_first_last": [hist[0], hist[-1]],
                                "generate_s": gen_s, "train_s": train_s},
@@ -437,7 +445,8 @@ def run_ours(args, world, rank, local):
         "speedup_mixed_zero_vs_fp64": fp64_ms / zero_ms,
         "aniso_ellipsoid": {"workload": case.name, "k0": case.k0, "mixed_ms": aniso_mixed_ms,
                             "fp64_ms": aniso_fp64_ms, "speedup": aniso_fp64_ms / aniso_mixed_ms,
-                            "mixed_inner_iterations": r2.inner_iterations, "fp64_iterations": b2.iterations,
+                            "mixed_fp32_iterations_per_update": r2.inner_iterations,
+                            "fp64_iterations": b2.iterations,
                             "mixed_true_residual": float(true_relative_residual(a64, r2.u, p2.wave)),
                             "fp64_true_residual": float(true_relative_residual(a64, b2.u, p2.wave))},
         "matvec": {"fp32_ms": mv32_ms, "fp64_ms": mv64_ms, "fp32_gbs": ach32, "fp64_gbs": ach64,

@@ -249,7 +249,9 @@ __global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, 
 }
 
 // s = r - alpha v, ||s||; stopping checks on ||s|| (the update u += alpha p
-// of an early exit is applied by the finalize kernel).
+// of an early exit is applied by the finalize kernel).  state.first != 0
+// turns the convergence exit here off, so a run stops on full iterations
+// only (the reliable-update cycles continue the recurrence from there).
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_bicg_s(size_t n, void* state, size_t sstride, const cx<R>* r, const cx<R>* v, cx<R>* s) {
   StateView sv = view(state, sstride);
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_s(size_t n, void* state, size
     int stop = EM3D_RUNNING;
     if (!isfinite(srel)) stop = EM3D_NONFINITE;
     else if (st->guard >= 0.0 && srel > st->guard) stop = EM3D_DIVERGENCE_GUARD;
-    else if (srel < st->tol) stop = EM3D_CONVERGED;
+    else if (srel < st->tol && st->first == 0) stop = EM3D_CONVERGED;
     else if (st->max_actions >= 0 && st->matvecs + 1 > st->max_actions) stop = EM3D_MAX_OPERATOR_ACTIONS;
     st->last_rel = srel;
     if (stop != EM3D_RUNNING) {

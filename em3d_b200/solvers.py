@@ -763,3 +763,198 @@ class DefectCorrection:
                 inner_iterations=inner_its[b], fp64_matvecs=int(mv64), fp32_matvecs=int(mv32[b]),
                 fp32_rmatvecs=int(rmv32[b]), guess_rejected=rejected[b]))
         return out
+
+
+class MixedBiCGStab:
+    """BiCGStab in FP32 with reliable updates in FP64.
+
+    The iteration (vectors, operator applications, vector updates) runs on the
+    FP32 twin of the operator and accumulates a correction ``x32``.  Whenever
+    the FP32 recursive residual has dropped by ``delta`` since the last update
+    (or has reached the target), the correction is added to the FP64 solution,
+    the true residual ``f - A u`` is formed with the FP64 operator and FP64
+    norms, and it replaces the FP32 residual.  The search direction, the shadow
+    residual and the BiCGStab scalars carry over (``rho`` is recomputed against
+    the new residual), so, unlike restarted defect correction, the FP32 run
+    needs about as many iterations as FP64 BiCGStab; a cycle that ends inside
+    an iteration (the half-step exit) or on a breakdown restarts the
+    recurrence from the true residual (cycles run with BiCGStab's half-step
+    convergence exit turned off, so they end on full iterations unless the
+    half step breaks down).  The stopping test is the FP64 true
+    residual, as in :class:`DefectCorrection` (whose result type this returns:
+    ``outer_iterations`` counts updates, ``inner_iterations`` the FP32
+    iterations of each cycle).  Method: Sleijpen & van der Vorst, "Reliable
+    updated residuals in hybrid Bi-CG methods", Computing 56 (1996).
+
+    ``x0`` is judged like in :class:`DefectCorrection`: a guess whose true
+    residual is not below ``||f||`` is replaced by the zero guess.  One
+    right-hand side per solve (``DefectCorrection.solve_batch`` batches).
+    """
+
+    graph_chunk = 4
+    max_cached = 2
+
+    def __init__(self, config: SolverConfig, *, delta: float = 1e-3, safety: float = 0.5,
+                 guess_fallback: bool = True, max_cycles: int = 200):
+        if not 0.0 < delta < 1.0:
+            raise ValueError(f"delta must be in (0, 1), got {delta!r}")
+        self.cfg = config
+        self.delta = float(delta)
+        self.safety = float(safety)
+        self.guess_fallback = bool(guess_fallback)
+        self.max_cycles = int(max_cycles)
+
+    def _buffers(self, operator, rhs, operator_low):
+        from collections import OrderedDict
+
+        import torch
+
+        from .backend import Precision
+
+        if not hasattr(self, "_cache"):
+            self._cache = OrderedDict()
+        key = (id(operator), tuple(rhs.shape))
+        hit = self._cache.get(key)
+        if hit is not None and hit["op"] is operator and (operator_low is None or hit["op_lo"] is operator_low):
+            self._cache.move_to_end(key)
+            hit["eng"].load_rhs(rhs)
+            return hit
+        eng = _Engine(operator, rhs, hist_cap=4, batch=1)
+        op_lo = operator_low if operator_low is not None else operator.with_precision(Precision.SINGLE)
+        zero32 = torch.zeros(eng.rhs.shape, dtype=torch.complex64, device=eng.rhs.device)
+        e32 = _Engine(op_lo, zero32, hist_cap=int(self.cfg.max_iter) + 4, batch=1)
+        vec32 = {k: e32.vec() for k in ("u", "r", "r_hat", "p", "v", "s", "t")}
+        hit = {"op": operator, "op_lo": op_lo, "eng": eng, "u": eng.vec(), "r": eng.vec(), "e32": e32,
+               "v32": vec32}
+        self._cache[key] = hit
+        while len(self._cache) > self.max_cached:
+            self._cache.popitem(last=False)
+        return hit
+
+    def solve(self, operator, rhs, x0=None, *, operator_low=None) -> DefectCorrectionResult:
+        import torch
+
+        cfg = self.cfg
+        t = rhs if isinstance(rhs, torch.Tensor) else torch.as_tensor(np.asarray(rhs))
+        if _batch_of(operator, t) != 1:
+            raise NotImplementedError("MixedBiCGStab solves one right-hand side; use DefectCorrection.solve_batch")
+        buf = self._buffers(operator, t, operator_low)
+        eng, e32, V = buf["eng"], buf["e32"], buf["v32"]
+        f = eng.rhs
+        x = _load_u(buf["u"], x0)
+        r = buf["r"]
+        stream = eng.stream()
+        fn = eng.norm(f)
+        if fn == 0.0:
+            x.zero_()
+            return DefectCorrectionResult(u=x.clone(), iterations=0, residual_history=[0.0], converged=True,
+                                          matvec_count=0, residual_action_counts=[0], status="converged",
+                                          true_final_residual=0.0)
+        tol = max(float(cfg.rtol), float(cfg.atol) / fn)
+        mv64 = 0
+
+        def true_residual():
+            nonlocal mv64
+            operator.apply_into(x, r)
+            mv64 += 1
+            _lib.call("em3d_vec_axpby", eng.dt, eng.n, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0, r.data_ptr(),
+                      stream)
+            return eng.norm(r) / fn
+
+        rel = true_residual()
+        rejected = False
+        if x0 is not None and self.guess_fallback and not rel < 1.0:
+            x.zero_()
+            r.copy_(f)
+            rel = 1.0
+            rejected = True
+        hist, counts = [float(rel)], [mv64]
+        status = None
+        if not np.isfinite(rel):
+            status = "nonfinite"
+        elif rel < tol:
+            status = "converged"
+
+        u32, r32, rh, p, v, s, tt = (V[k] for k in ("u", "r", "r_hat", "p", "v", "s", "t"))
+
+        def iteration():
+            e32.step("em3d_bicgstab_p", r32.data_ptr(), p.data_ptr(), v.data_ptr())
+            e32.apply(p, v)
+            e32.step("em3d_bicgstab_alpha", rh.data_ptr(), v.data_ptr())
+            e32.step("em3d_bicgstab_s", r32.data_ptr(), v.data_ptr(), s.data_ptr())
+            e32.apply(s, tt)
+            e32.step("em3d_bicgstab_omega", tt.data_ptr(), s.data_ptr())
+            e32.step("em3d_bicgstab_update", u32.data_ptr(), p.data_ptr(), s.data_ptr(), tt.data_ptr(), r32.data_ptr(),
+                     rh.data_ptr())
+            e32.step("em3d_bicgstab_finalize", u32.data_ptr(), p.data_ptr())
+
+        st = e32.state.host
+        restart = True
+        total_its = 0
+        mv32 = 0
+        cycles = []
+        stalled = 0
+        budget = int(cfg.max_iter)
+        while status is None:
+            if total_its >= budget or len(cycles) >= self.max_cycles:
+                status = "max_iter"
+                break
+            _lib.call("em3d_vec_convert", eng.n, eng.dt, r.data_ptr(), _lib.EM3D_C64, r32.data_ptr(), 0, stream)
+            u32.zero_()
+            n0 = e32.norm(r32)
+            if restart:
+                rh.copy_(r32)
+                st.iter = 0
+                st.rho_re, st.rho_im = n0 * n0, 0.0
+                st.rho_prev_re, st.rho_prev_im = 1.0, 0.0
+                st.alpha_re, st.alpha_im = 1.0, 0.0
+                st.omega_re, st.omega_im = 1.0, 0.0
+            else:
+                _lib.call("em3d_vec_dots", _lib.EM3D_C64, e32.n, 1, rh.data_ptr(), r32.data_ptr(), None, None,
+                          e32.state.ptr, e32.state.stride, stream)
+                rho_new = e32.state.dots()[0][0]
+                st.rho_prev_re, st.rho_prev_im = st.rho_re, st.rho_im
+                st.rho_re, st.rho_im = rho_new.real, rho_new.imag
+            it0 = int(st.iter)
+            st.rhs_norm = n0
+            st.tol = max(self.delta, self.safety * tol * fn / n0)
+            st.guard = -1.0
+            st.status = 0
+            st.pending = 0
+            st.first = 1  # cycles end on full iterations only
+            st.max_iter = it0 + (budget - total_its)
+            st.max_actions = -1
+            st.last_rel = 1.0
+            mv_before = int(st.matvecs)
+            e32.state.upload([[1.0]], [[mv_before]])
+            e32.run(iteration, self.graph_chunk, use_graph=True)
+            got = e32.state.download()[0][0]
+            for name in ("rho_re", "rho_im", "rho_prev_re", "rho_prev_im", "alpha_re", "alpha_im", "omega_re",
+                         "omega_im", "iter", "matvecs", "status", "pending"):
+                setattr(st, name, getattr(got, name))
+            its = int(got.iter) - it0
+            total_its += its
+            mv32 += int(got.matvecs) - mv_before
+            cycles.append(its)
+            _lib.call("em3d_vec_convert", eng.n, _lib.EM3D_C64, u32.data_ptr(), eng.dt, x.data_ptr(), 1, stream)
+            rel = true_residual()
+            hist.append(float(rel))
+            counts.append(mv64 + mv32)
+            inner = _status_name(got.status)
+            if cfg.log:
+                print(f"[MixedBiCGStab] update={len(cycles)}, fp32_iterations={its} ({inner}), rel_res={rel:.3e}")
+            if not np.isfinite(rel):
+                status = "nonfinite"
+            elif rel < tol:
+                status = "converged"
+            elif cfg.divergence_guard is not None and rel > float(cfg.divergence_guard):
+                status = "divergence_guard"
+            stalled = stalled + 1 if its == 0 else 0
+            if status is None and stalled >= 2:
+                status = inner if inner not in ("converged", "running") else "max_iter"
+            restart = int(got.pending) != 0 or inner not in ("converged", "max_iter")
+        return DefectCorrectionResult(
+            u=x.clone(), iterations=int(total_its), residual_history=hist, converged=status == "converged",
+            matvec_count=int(mv64 + mv32), rmatvec_count=0, residual_action_counts=counts, status=status,
+            true_final_residual=float(hist[-1]), outer_iterations=len(cycles), inner_iterations=cycles,
+            fp64_matvecs=int(mv64), fp32_matvecs=int(mv32), guess_rejected=rejected)

@@ -194,7 +194,9 @@ typedef struct em3d_krylov_state {
   int32_t max_actions;         /* < 0 disables the action budget               */
   int32_t hist_len, hist_cap;  /* residual history entries used / capacity     */
   int32_t pending;             /* BiCGStab: 1 = u += alpha p still to apply    */
-  int32_t first;               /* TwoStep: 1 before the first update           */
+  int32_t first;               /* TwoStep: 1 before the first update; BiCGStab:
+                                  non-zero disables the half-step (||s||)
+                                  convergence exit                              */
   uint32_t ticket;             /* last-block counter of the reductions         */
   int32_t batch_running;       /* state 0 only: right-hand sides still running */
   int32_t batch_done;          /* state 0 only: 1 once all have stopped; the
