@@ -312,6 +312,27 @@ int em3d_fno_uncast(int act, size_t n, const void* src, float* dst, void* stream
  * replaces flat_wave_vec (src/em3d/wave.py:9-37).  orient (3) and amplitude
  * (3 complex = 6 doubles) are HOST arrays.
  * ------------------------------------------------------------------------ */
+/* ------------------------------------------------------------------------
+ * Far field.
+ *
+ * em3d_em_farfield: F[m][c] = dv sum_q (chi u)_c(q) exp(-i k0 dirs[m] . r_q)
+ * (replaces scatter_integral_direct, src/em3d/farfield/_core.py:8-71);
+ * em3d_acoustic_farfield: F[m] = k0^2 dv / (4 pi) sum_q chi(q) u(q)
+ * exp(-i k0 dirs[m] . r_q) (replaces farfield_amplitude,
+ * src/em3d/acoustics/farfield.py:29-60).  chi and u are the operator's device
+ * arrays (EM3D_C64 or EM3D_C128); x, y, z the DEVICE float64 cell-centre
+ * coordinates; dirs a DEVICE float64 (M, 3) array used as given (the callers
+ * normalise where the reference does); F a DEVICE complex128 (M, 3) / (M,)
+ * output.  Phases and sums are FP64.  Workspace: em3d_farfield_workspace_bytes.
+ * ------------------------------------------------------------------------ */
+size_t em3d_farfield_workspace_bytes(const em3d_grid* g, int M);
+int em3d_em_farfield(const em3d_grid* g, int dtype, const void* chi, const void* u, const double* x, const double* y,
+                     const double* z, double k0, double dv, int M, const double* dirs, void* F, void* workspace,
+                     size_t workspace_bytes, void* stream);
+int em3d_acoustic_farfield(const em3d_grid* g, int dtype, const void* chi, const void* u, const double* x,
+                           const double* y, const double* z, double k0, double dv, int M, const double* dirs, void* F,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
 #define EM3D_SHAPE_DOUBLES 33
 int em3d_sample_ellipsoids(int kind, int dtype, int nx, int ny, int nz, const double* x, const double* y,
                            const double* z, int count, const double* shapes, double tol, const double* background,

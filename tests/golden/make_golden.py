@@ -218,5 +218,64 @@ def main(ref_src: str) -> None:
     print("wrote solvers.json")
 
 
+def farfield_fixtures(ref_src: str) -> None:
+    """Far fields, RCS curves, the acoustic pattern and Mie comparisons of the
+    reference on the committed EM / acoustic golden inputs -> farfield.npz."""
+    sys.path.insert(0, ref_src)
+    import em3d
+    from em3d import Backend, Grid, Precision, Problem, farfield, mie
+    from em3d.acoustics import make_acoustic_problem
+    from em3d.acoustics import farfield as acff
+
+    be = {"double": Backend.numpy(Precision.DOUBLE), "single": Backend.numpy(Precision.SINGLE)}
+    out = {}
+    rng = np.random.default_rng(5)
+    dirs = rng.standard_normal((16, 3))
+    dirs /= np.linalg.norm(dirs, axis=1)[:, None]
+    out["em_dirs"] = dirs
+    for case, k in (("sphere16", 4.0), ("odd567", 3.3)):
+        g = np.load(os.path.join(HERE, f"em_{case}.npz"))
+        for prec in ("double", "single"):
+            grid = Grid(N=tuple(int(n) for n in g["N"]), L=tuple(float(v) for v in g["L"]), center=(0.0, 0.0, 0.0),
+                        backend=be[prec])
+            prob = Problem(grid=grid, eps_tensor=g[f"chi_{prec}"], wave=g[f"wave_{prec}"], k0=k,
+                           volume=grid.dv * int(np.prod(grid.N)))
+            out[f"em_{case}_F_{prec}"] = farfield.scatter_integral(g[f"u_{prec}"], prob, dirs)
+            phi, sig = farfield.rcs_plane(g[f"u_{prec}"], prob, n_phi=24, plane="xz")
+            out[f"em_{case}_rcs_xz_{prec}"] = sig
+            out[f"em_{case}_rcs_single_dir_{prec}"] = np.array(farfield.rcs(g[f"u_{prec}"], prob, dirs[3] * 2.0))
+    # the README sphere: the reference's own BiCGStab solution against Mie
+    g = np.load(os.path.join(HERE, "em_sphere16.npz"))
+    grid = Grid(N=(16, 16, 16), L=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0), backend=be["double"])
+    prob = Problem(grid=grid, eps_tensor=g["chi_double"], wave=g["wave_double"], k0=4.0, volume=1.0)
+    u = np.load(os.path.join(HERE, "sol_sphere16_bicgstab_double_u.npy"))
+    cmp = mie.compare_rcs_plane(u, prob, a=0.25, eps_r=2.0, n_phi=120, plane="xz")
+    for key in ("sigma_num", "sigma_mie", "shape_err", "scale_ratio", "abs_rel_err"):
+        out[f"mie_readme_{key}"] = np.asarray(cmp[key])
+    # the Mie series itself on a few parameter sets (lossless, lossy; all planes)
+    for tag, (a, eps, k0) in {"a": (0.25, 2.0, 4.0), "b": (0.3, 2.5 + 0.3j, 6.0), "c": (0.1, 4.0, 2.0)}.items():
+        co = mie.mie_coefficients(a, eps, k0)
+        out[f"mie_{tag}_an"], out[f"mie_{tag}_bn"] = co["a"], co["b"]
+        cs = mie.mie_cross_sections(a, eps, k0)
+        out[f"mie_{tag}_cross"] = np.array([cs["scat"], cs["ext"], cs["abs"]])
+        for plane in ("xy", "xz", "yz"):
+            out[f"mie_{tag}_rcs_{plane}"] = mie.mie_rcs_plane(a, eps, k0, n_phi=36, plane=plane)[1]
+    # acoustic far field on the spheres case
+    ga = np.load(os.path.join(HERE, "ac_spheres16.npz"))
+    adirs = rng.standard_normal((24, 3)) * 3.0   # not normalised: the reference normalises
+    out["ac_dirs"] = adirs
+    for prec in ("double", "single"):
+        grid = Grid(N=(16, 16, 16), L=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0), backend=be[prec])
+        prob = make_acoustic_problem(grid, ga[f"eta_{prec}"], k0=float(ga["k0"]))
+        out[f"ac_F_{prec}"] = acff.farfield_amplitude(ga[f"u_{prec}"], prob, adirs)
+        out[f"ac_pattern_xz_{prec}"] = acff.pattern_plane(ga[f"u_{prec}"], prob, plane="xz", n_angles=36)[1]
+    _save("farfield.npz", **out)
+    print("mie readme shape_err", float(cmp["shape_err"]), "scale", float(cmp["scale_ratio"]))
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) > 2 and sys.argv[2] == "farfield":
+        farfield_fixtures(sys.argv[1])
+    else:
+        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+        farfield_fixtures(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
