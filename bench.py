@@ -347,6 +347,11 @@ def run_ours(args, world, rank, local):
     fp64_ms, res64 = timed(fp64)
     zero_ms, res0 = timed(mixed_zero)
 
+    def sol_err_max(results):
+        """Max relative difference to the FP64 BiCGStab (complex128) solution of the same scene."""
+        return max(float(torch.linalg.vector_norm(r.u - res64[s].u) / torch.linalg.vector_norm(res64[s].u))
+                   for s, r in enumerate(results))
+
     def true_max(results):
         return max(float(true_relative_residual(scenes[s % K][1], r.u, scenes[s % K][0].wave))
                    for s, r in enumerate(results))
@@ -380,6 +385,45 @@ def run_ours(args, world, rank, local):
         b2 = bic2.solve(a64, p2.wave)
     aniso_mixed_ms, r2 = _events_ms(lambda: dc2.solve(a64, p2.wave, operator_low=a32))
     aniso_fp64_ms, b2 = _events_ms(lambda: bic2.solve(a64, p2.wave))
+    aniso_err = float(torch.linalg.vector_norm(r2.u - b2.u) / torch.linalg.vector_norm(b2.u))
+
+    # -- 4a. the README sphere (16^3, k0 = 4): RCS against Mie from this library's solve
+    from em3d_b200 import mie
+
+    sc1 = workloads.sphere_em(16, "double")
+    g1 = e.Grid(N=sc1.N, L=sc1.L, center=sc1.center, backend=be64)
+    p1 = e.Problem(grid=g1, eps_tensor=sc1.chi, wave=sc1.wave, k0=sc1.k0, volume=1.0)
+    r1 = BiCGStab(SolverConfig(max_iter=200, rtol=1e-8)).solve(e.Operator(p1), p1.wave)
+    cmp1 = mie.compare_rcs_plane(r1.u, p1, a=0.25, eps_r=2.0, n_phi=120, plane="xz")
+    readme = {"workload": sc1.name, "iterations": r1.iterations, "status": r1.status,
+              "mie_shape_err": cmp1["shape_err"], "mie_scale_ratio": cmp1["scale_ratio"],
+              "mie_abs_rel_err": cmp1["abs_rel_err"]}
+
+    # -- 4b. the acoustic scene: 200 spheres at 256^3, k0 = 20 (eta sampled on the device)
+    from em3d_b200 import acoustics as ea, farfield
+    from em3d_b200.solvers import TwoStep
+
+    gA = e.Grid(N=(256, 256, 256), L=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0), backend=be64)
+    pA = ea.make_acoustic_problem(gA, workloads.acoustic_spheres_device(gA, count=200, seed=0), k0=20.0)
+    oA64 = ea.AcousticOperator(pA)
+    oA32 = oA64.with_precision(e.Precision.SINGLE)
+    mxA, bA, tA = MixedBiCGStab(cfg), BiCGStab(cfg), TwoStep(cfg)
+    acoustic = {"workload": "acoustic_200_spheres_256^3", "k0": 20.0}
+    for name, fn in (("mixed", lambda: mxA.solve(oA64, pA.wave, operator_low=oA32)),
+                     ("fp64_bicgstab", lambda: bA.solve(oA64, pA.wave)),
+                     ("fp64_twostep", lambda: tA.solve(oA64, pA.wave))):
+        fn()
+        t_ms, rA = _events_ms(fn)
+        acoustic[name] = {"ms": t_ms, "iterations": rA.iterations, "status": rA.status,
+                          "true_residual": float(true_relative_residual(oA64, rA.u, pA.wave))}
+        if name == "mixed":
+            uA = rA.u
+    farfield.pattern_plane(uA, pA, plane="xz", n_angles=360)
+    pat_ms, _ = _events_ms(lambda: farfield.pattern_plane(uA, pA, plane="xz", n_angles=360))
+    acoustic["pattern_xz_360_ms"] = pat_ms
+    acoustic["speedup_mixed_vs_fp64_bicgstab"] = acoustic["fp64_bicgstab"]["ms"] / acoustic["mixed"]["ms"]
+    del oA64, oA32, mxA, bA, tA, uA
+    torch.cuda.empty_cache()
 
     # -- 5. matvec timing (dominant kernel): CUDA events on the launching stream
     def time_matvec(op, reps=20):
@@ -414,9 +458,12 @@ def run_ours(args, world, rank, local):
         return
 
     def summary(results):
-        return {"iterations_mean": float(np.mean([r.iterations for r in results])),
-                "matvecs_mean": float(np.mean([r.matvec_count for r in results])),
-                "converged": int(sum(r.converged for r in results)), "true_residual_max": true_max(results)}
+        out = {"iterations_mean": float(np.mean([r.iterations for r in results])),
+               "matvecs_mean": float(np.mean([r.matvec_count for r in results])),
+               "converged": int(sum(r.converged for r in results)), "true_residual_max": true_max(results)}
+        if results is not res64:
+            out["solution_rel_err_vs_fp64_max"] = sol_err_max(results)
+        return out
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -448,7 +495,10 @@ def run_ours(args, world, rank, local):
                             "mixed_fp32_iterations_per_update": r2.inner_iterations,
                             "fp64_iterations": b2.iterations,
                             "mixed_true_residual": float(true_relative_residual(a64, r2.u, p2.wave)),
+                            "mixed_solution_rel_err_vs_fp64": aniso_err,
                             "fp64_true_residual": float(true_relative_residual(a64, b2.u, p2.wave))},
+        "acoustic_spheres": acoustic,
+        "readme_sphere_mie": readme,
         "matvec": {"fp32_ms": mv32_ms, "fp64_ms": mv64_ms, "fp32_gbs": ach32, "fp64_gbs": ach64,
                    "fp32_per_s": 1000.0 / mv32_ms, "fp64_per_s": 1000.0 / mv64_ms, "fp64_frac": ach64 / peak},
     }

@@ -74,13 +74,11 @@ def aniso_ellipsoid_em(N: int = 128, precision: str = "double", k0: float = 12.0
     return EMCase(f"em_aniso_ellipsoid_{N}^3", Ns, L, c, k0, chi, wave)
 
 
-def acoustic_spheres(N: int = 256, precision: str = "double", k0: float = 20.0, count: int = 200,
-                     seed: int = 0) -> AcousticCase:
-    """Rejection-sampled non-overlapping spheres with centres in [-0.5+r, 0.5-r]^3."""
-    cdt = _setup.complex_dtype_of(precision)
+def acoustic_sphere_list(count: int = 200, seed: int = 0) -> list:
+    """Rejection-sampled non-overlapping spheres with centres in
+    [-0.5+r, 0.5-r]^3: [(centre, radius, eta)], radius U[0.02, 0.06],
+    eta U[1.2, 2.5] + i U[0, 0.1]."""
     rng = np.random.default_rng(seed)
-    Ns, L, c = (N, N, N), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0)
-    axes = _setup.grid_axes_host(Ns, L, c, precision)
     spheres = []
     tries = 0
     while len(spheres) < count:
@@ -92,20 +90,38 @@ def acoustic_spheres(N: int = 256, precision: str = "double", k0: float = 20.0, 
         if all(np.linalg.norm(ctr - c2) > r + r2 for c2, r2, _ in spheres):
             val = rng.uniform(1.2, 2.5) + 1j * rng.uniform(0.0, 0.1)
             spheres.append((ctr, r, val))
+    return spheres
+
+
+def acoustic_spheres(N: int = 256, precision: str = "double", k0: float = 20.0, count: int = 200,
+                     seed: int = 0) -> AcousticCase:
+    """eta of ``acoustic_sphere_list`` painted in order with the reference's
+    sphere test ``sum ((x_i - c_i) / r)^2 <= 1`` (``acoustics/materials.py:62-83``),
+    evaluated inside each sphere's bounding box."""
+    cdt = _setup.complex_dtype_of(precision)
+    Ns, L, c = (N, N, N), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0)
+    axes = _setup.grid_axes_host(Ns, L, c, precision)
     eta = np.ones(Ns, dtype=cdt)
     ax = [np.asarray(a, dtype=np.float64) for a in axes]
-    for ctr, r, val in spheres:
-        # cell-centre test inside the sphere's bounding box only
+    for ctr, r, val in acoustic_sphere_list(count, seed):
         sl = []
         for d in range(3):
             lo = int(np.searchsorted(ax[d], ctr[d] - r, side="left"))
             hi = int(np.searchsorted(ax[d], ctr[d] + r, side="right"))
-            sl.append(slice(lo, hi))
+            sl.append(slice(max(lo - 1, 0), min(hi + 1, N)))
         X, Y, Z = np.meshgrid(ax[0][sl[0]], ax[1][sl[1]], ax[2][sl[2]], indexing="ij")
-        m = ((X - ctr[0]) ** 2 + (Y - ctr[1]) ** 2 + (Z - ctr[2]) ** 2) <= r * r
+        m = (((X - ctr[0]) / r) ** 2 + ((Y - ctr[1]) / r) ** 2) + ((Z - ctr[2]) / r) ** 2 <= 1.0
         box = eta[sl[0], sl[1], sl[2]]
         box[m] = cdt(val)
     return AcousticCase(f"acoustic_{count}_spheres_{N}^3", Ns, L, c, k0, eta)
+
+
+def acoustic_spheres_device(grid, count: int = 200, seed: int = 0):
+    """The same eta sampled on the device (``em3d_sample_ellipsoids``)."""
+    from .scenes import EllipsoidShape, sample_scene_eta
+
+    shapes = [EllipsoidShape(tuple(ctr), (r, r, r), None, val) for ctr, r, val in acoustic_sphere_list(count, seed)]
+    return sample_scene_eta(grid, shapes, eta_outside=1.0, tol=0.0)
 
 
 def fibonacci_directions(n: int) -> np.ndarray:

@@ -194,3 +194,29 @@ def test_device_plane_wave_matches_reference(fixture, orient, amp):
                       backend=be)
         w = scenes.plane_wave(grid, k=float(d["k"]), orient=orient, amplitude=amp).cpu().numpy()
         assert np.abs(w - d[f"wave_{prec}"]).max() < tol
+
+
+def test_acoustic_sphere_workload_equals_oracle_scene():
+    """The 200-sphere acoustic workload's host builder paints exactly what the
+    scene restatement (reference sphere test, tol 0) gives."""
+    from em3d_b200 import setup, workloads
+    from oracle import materials as om
+
+    for N, count in ((32, 40), (64, 200)):
+        case = workloads.acoustic_spheres(N, count=count, seed=1)
+        axes = setup.grid_axes_host(case.N, case.L, case.center, "double")
+        shapes = np.stack([om.pack(c, (r,) * 3, None, v) for c, r, v in workloads.acoustic_sphere_list(count, 1)])
+        assert np.array_equal(case.eta, om.sample_eta(axes, shapes, 0.0, 1.0, np.complex128))
+
+
+@pytest.mark.gpu
+def test_device_acoustic_sphere_workload_equals_host():
+    import em3d_b200 as e
+    from em3d_b200 import workloads
+
+    for prec in ("double", "single"):
+        case = workloads.acoustic_spheres(64, prec, count=200, seed=0)
+        be = e.Backend.b200(e.Precision.DOUBLE if prec == "double" else e.Precision.SINGLE)
+        grid = e.Grid(N=case.N, L=case.L, center=case.center, backend=be)
+        eta = workloads.acoustic_spheres_device(grid, count=200, seed=0).cpu().numpy()
+        assert np.array_equal(eta, case.eta)
