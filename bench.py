@@ -56,7 +56,7 @@ SCENE_SEEDS = list(range(10000, 10008))
 FP64_MATVECS_PER_SOLVE = 29.6
 # dram__bytes_read.sum + dram__bytes_write.sum per complex64 EM matvec (all
 # five passes) from the ncu launch list summarised in profiles/em_matvec_128.md.
-NCU_TRAFFIC_BYTES = 1495.4e6
+NCU_TRAFFIC_BYTES = 1489.6e6
 
 
 def byte_model(n: int, c: int) -> int:
