@@ -23,6 +23,7 @@ EM3D_ACOUSTIC = 1
 EM3D_EM = 3
 EM3D_TUNE_XPASS_VARIANT = 0
 EM3D_TUNE_FFT_GENERIC = 1
+EM3D_TUNE_FNO_SIMT = 2
 
 
 class EmGrid(ctypes.Structure):

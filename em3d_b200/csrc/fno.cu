@@ -752,6 +752,317 @@ inline size_t row_fwd_smem(bool lift, int Z, int m) {
 }
 
 // ---------------------------------------------------------------------------
+// Tensor-core z-row kernel (bf16 activations, width 32, Z in {32, 64, 128}).
+//
+// Per row the layer is two small GEMMs on mma.sync m16n8k16 (bf16 in, FP32
+// accumulate), one warp per 32 cells of the row:
+//   O[co][z]  = sum_ci A[co][ci] v[ci][z] + sum_j Ucat[co][j] T[j][z]
+//               (Ucat = Re/Im of the row's mode coefficients, T the weighted
+//                inverse-DFT cos / -sin table), + a[co], GELU
+//   Vz[co][j] = sum_z O[co][z] F[z][j]   (F = cos / -sin: next layer's z-DFT)
+// The second GEMM takes its A operand straight from the first one's
+// accumulators (the m16n8 C layout of two neighbouring n-tiles is the m16k16 A
+// layout), after rounding O to bf16, so it sees exactly the stored values.
+// The lift uses the same path with A = P and the 24 cell features (padded to
+// 32) in place of v.  Twiddles and the mode coefficients enter the tensor
+// cores as bf16, like every other activation of the network.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ uint32_t pack_raw(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  __nv_bfloat162 v;
+  v.x = lo;
+  v.y = hi;
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+constexpr int kTcCols = 128;  // cells per CTA step (R rows of Z)
+
+inline size_t row_fwd_tc_smem() {
+  return sizeof(__nv_bfloat16) * 2 * 32 * kTcCols   // Vs, Os
+         + sizeof(float2) * 4 * 32 * kMaxModes      // sU (up to 4 rows)
+         + sizeof(float) * 4 * 32 * 32              // per-warp DFT partials
+         + sizeof(float) * (32 + 6 * 32 + 8);       // bias, Q, qb
+}
+
+template <bool LIFT>
+__global__ void __launch_bounds__(128) k_row_fwd_tc(
+    int B, int X, int Y, int Z, int m, const float2* __restrict__ chi, const float2* __restrict__ wave,
+    const __nv_bfloat16* __restrict__ vin, const float2* __restrict__ Uxy, const __nv_bfloat16* __restrict__ Wt,
+    const float* __restrict__ bias, int apply_gelu, __nv_bfloat16* __restrict__ pre_out,
+    __nv_bfloat16* __restrict__ vout, float2* __restrict__ Vz, const __nv_bfloat16* __restrict__ Q,
+    const float* __restrict__ qb, float2* __restrict__ u_out) {
+  constexpr int W = 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __nv_bfloat16* Vs = reinterpret_cast<__nv_bfloat16*>(smem_raw);   // [32][kTcCols]
+  __nv_bfloat16* Os = Vs + 32 * kTcCols;                            // [32][kTcCols]
+  float2* sU = reinterpret_cast<float2*>(Os + 32 * kTcCols);        // [4][32][kMaxModes]
+  float* red = reinterpret_cast<float*>(sU + 4 * 32 * kMaxModes);   // [4 warps][32][32]
+  float* sb = red + 4 * 32 * 32;
+  float* sQ = sb + 32;
+  float* sqb = sQ + 6 * 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tg = lane & 3;
+  const int WPR = Z / 32, R = 4 / WPR;
+  const int wr = warp / WPR, zs = (warp % WPR) * 32;
+  const int kin = LIFT ? kFeat : W;
+  const size_t XY = (size_t)X * Y, ncell = XY * Z, nrows = (size_t)B * XY;
+
+  for (int i = threadIdx.x; i < 32; i += blockDim.x) sb[i] = bias[i];
+  for (int i = threadIdx.x; i < 6 * 32; i += blockDim.x) sQ[i] = Q ? __bfloat162float(Q[i]) : 0.0f;
+  if (threadIdx.x < 8) sqb[threadIdx.x] = (qb && threadIdx.x < 6) ? qb[threadIdx.x] : 0.0f;
+
+  // constant fragments: weights (A), inverse-DFT table (B), forward-DFT table (B)
+  uint32_t Aw[2][2][4], Bt[2][4][2], Bf[2][4][2];
+  {
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+    auto wv = [&](int r, int c) { return c < kin ? Wt[r * kin + c] : zero; };
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks) {
+        const int r0 = mt * 16 + g, c0 = ks * 16 + tg * 2;
+        Aw[mt][ks][0] = pack_raw(wv(r0, c0), wv(r0, c0 + 1));
+        Aw[mt][ks][1] = pack_raw(wv(r0 + 8, c0), wv(r0 + 8, c0 + 1));
+        Aw[mt][ks][2] = pack_raw(wv(r0, c0 + 8), wv(r0, c0 + 9));
+        Aw[mt][ks][3] = pack_raw(wv(r0 + 8, c0 + 8), wv(r0 + 8, c0 + 9));
+      }
+    const float inv = 1.0f / (float)ncell;
+    // T[j][z]: j = 2k -> cos(theta) w_k, j = 2k+1 -> -sin(theta) w_k; F[z][j]: cos / -sin
+    auto tw = [&](int j, int z, bool weighted) {
+      if (j >= 2 * m) return 0.0f;
+      const int k = j >> 1;
+      float sn, cs;
+      sincospif(2.0f * (float)((k * z) % Z) / (float)Z, &sn, &cs);
+      const float w = weighted ? (k == 0 ? 1.0f : 2.0f) * inv : 1.0f;
+      return (j & 1) ? -sn * w : cs * w;
+    };
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int k0 = ks * 16 + tg * 2;
+        const int z = zs + nt * 8 + g;
+        Bt[ks][nt][0] = pack_bf16(tw(k0, z, true), tw(k0 + 1, z, true));
+        Bt[ks][nt][1] = pack_bf16(tw(k0 + 8, z, true), tw(k0 + 9, z, true));
+        // F: K = z (this warp's 32 cells, k-step ks), N = j
+        const int zk = zs + ks * 16 + tg * 2, j = nt * 8 + g;
+        Bf[ks][nt][0] = pack_bf16(tw(j, zk, false), tw(j, zk + 1, false));
+        Bf[ks][nt][1] = pack_bf16(tw(j, zk + 8, false), tw(j, zk + 9, false));
+      }
+  }
+  const int nt3 = (2 * m + 7) / 8;
+  __syncthreads();
+
+  const size_t ngroups = (nrows + R - 1) / R;
+  for (size_t gi = blockIdx.x; gi < ngroups; gi += gridDim.x) {
+    const size_t row0 = gi * R;
+    // ---- stage the rows' inputs
+    if (LIFT) {
+      for (int i = threadIdx.x; i < R * Z; i += blockDim.x) {
+        const int r = i / Z, z = i - r * Z;
+        const size_t row = row0 + r;
+        float f[kFeat];
+        if (row < nrows) {
+          const size_t b = row / XY, xy = row - b * XY;
+          cell_features(chi, wave, ncell, (int)b, xy * Z + z, f);
+        } else {
+#pragma unroll
+          for (int c = 0; c < kFeat; ++c) f[c] = 0.0f;
+        }
+#pragma unroll
+        for (int c = 0; c < 32; ++c) Vs[c * kTcCols + r * Z + z] = __float2bfloat16(c < kFeat ? f[c] : 0.0f);
+      }
+    } else {
+      const int chunks = Z / 8;
+      for (int i = threadIdx.x; i < R * 32 * chunks; i += blockDim.x) {
+        const int r = i / (32 * chunks), rem = i - r * 32 * chunks, ci = rem / chunks, q = rem - ci * chunks;
+        const size_t row = row0 + r;
+        uint4 val = make_uint4(0, 0, 0, 0);
+        if (row < nrows) {
+          const size_t b = row / XY, xy = row - b * XY;
+          val = *reinterpret_cast<const uint4*>(vin + (b * W + ci) * ncell + xy * Z + q * 8);
+        }
+        *reinterpret_cast<uint4*>(Vs + ci * kTcCols + r * Z + q * 8) = val;
+      }
+      for (int i = threadIdx.x; i < R * 32 * kMaxModes; i += blockDim.x) {
+        const int r = i / (32 * kMaxModes), rem = i - r * 32 * kMaxModes, co = rem / kMaxModes,
+                  k = rem - co * kMaxModes;
+        const size_t row = row0 + r;
+        float2 val = make_float2(0.0f, 0.0f);
+        if (row < nrows && k < m) {
+          const size_t b = row / XY, xy = row - b * XY;
+          val = Uxy[((b * W + co) * XY + xy) * m + k];
+        }
+        sU[i] = val;
+      }
+    }
+    __syncthreads();
+
+    // ---- GEMM 1 (+ inverse DFT) on this warp's 32 cells
+    float acc[2][4][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.0f;
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) {
+      uint32_t bv[4][2];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int col = wr * Z + zs + nt * 8 + g, k0 = ks * 16 + tg * 2;
+        bv[nt][0] = pack_raw(Vs[k0 * kTcCols + col], Vs[(k0 + 1) * kTcCols + col]);
+        bv[nt][1] = pack_raw(Vs[(k0 + 8) * kTcCols + col], Vs[(k0 + 9) * kTcCols + col]);
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[mt][nt], Aw[mt][ks], bv[nt]);
+    }
+    if (!LIFT) {
+      const float2* u = sU + wr * 32 * kMaxModes;
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks) {
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+          const int c0 = mt * 16 + g, j0 = ks * 16 + tg * 2;   // j0 even: (Re, Im) of mode j0 / 2
+          const float2 u00 = u[c0 * kMaxModes + (j0 >> 1)], u10 = u[(c0 + 8) * kMaxModes + (j0 >> 1)];
+          const float2 u01 = u[c0 * kMaxModes + (j0 >> 1) + 4], u11 = u[(c0 + 8) * kMaxModes + (j0 >> 1) + 4];
+          uint32_t au[4];
+          au[0] = pack_bf16(u00.x, u00.y);
+          au[1] = pack_bf16(u10.x, u10.y);
+          au[2] = pack_bf16(u01.x, u01.y);
+          au[3] = pack_bf16(u11.x, u11.y);
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[mt][nt], au, Bt[ks][nt]);
+        }
+      }
+    }
+
+    // ---- epilogue: bias, GELU, bf16; keep the rounded values for GEMM 2
+    const size_t row = row0 + wr;
+    const bool valid = row < nrows;
+    const size_t b = valid ? row / XY : 0, xy = valid ? row - b * XY : 0;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int co = mt * 16 + g + 8 * h;
+          const int z = zs + nt * 8 + tg * 2;
+          float o0 = acc[mt][nt][2 * h] + sb[co], o1 = acc[mt][nt][2 * h + 1] + sb[co];
+          if (pre_out && valid)
+            *reinterpret_cast<uint32_t*>(pre_out + (b * W + co) * ncell + xy * Z + z) = pack_bf16(o0, o1);
+          if (!LIFT && apply_gelu) { o0 = gelu(o0); o1 = gelu(o1); }
+          const uint32_t q = pack_bf16(o0, o1);
+          *reinterpret_cast<uint32_t*>(Os + co * kTcCols + wr * Z + z) = q;
+          const __nv_bfloat162 qq = *reinterpret_cast<const __nv_bfloat162*>(&q);
+          acc[mt][nt][2 * h] = __bfloat162float(qq.x);
+          acc[mt][nt][2 * h + 1] = __bfloat162float(qq.y);
+        }
+
+    // ---- GEMM 2: this warp's share of the next layer's z-DFT
+    if (Vz) {
+      float d[2][4][4];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) d[mt][nt][e] = 0.0f;
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks)
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+          uint32_t a[4];
+          a[0] = pack_bf16(acc[mt][2 * ks][0], acc[mt][2 * ks][1]);
+          a[1] = pack_bf16(acc[mt][2 * ks][2], acc[mt][2 * ks][3]);
+          a[2] = pack_bf16(acc[mt][2 * ks + 1][0], acc[mt][2 * ks + 1][1]);
+          a[3] = pack_bf16(acc[mt][2 * ks + 1][2], acc[mt][2 * ks + 1][3]);
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt)
+            if (nt < nt3) mma_bf16(d[mt][nt], a, Bf[ks][nt]);
+        }
+      float* rw = red + warp * 32 * 32;
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int co = mt * 16 + g + (e >= 2 ? 8 : 0), j = nt * 8 + tg * 2 + (e & 1);
+            rw[co * 32 + j] = d[mt][nt][e];
+          }
+    }
+    __syncthreads();
+    if (Vz) {
+      for (int i = threadIdx.x; i < R * 32 * m; i += blockDim.x) {
+        const int r = i / (32 * m), rem = i - r * 32 * m, co = rem / m, k = rem - co * m;
+        const size_t rw = row0 + r;
+        if (rw < nrows) {
+          float re = 0.0f, im = 0.0f;
+          for (int w = r * WPR; w < (r + 1) * WPR; ++w) {
+            re += red[(w * 32 + co) * 32 + 2 * k];
+            im += red[(w * 32 + co) * 32 + 2 * k + 1];
+          }
+          const size_t bb = rw / XY, xyy = rw - bb * XY;
+          Vz[((bb * W + co) * XY + xyy) * m + k] = make_float2(re, im);
+        }
+      }
+    }
+    if (vout) {
+      const int chunks = Z / 8;
+      for (int i = threadIdx.x; i < R * 32 * chunks; i += blockDim.x) {
+        const int r = i / (32 * chunks), rem = i - r * 32 * chunks, co = rem / chunks, q = rem - co * chunks;
+        const size_t rw = row0 + r;
+        if (rw < nrows) {
+          const size_t bb = rw / XY, xyy = rw - bb * XY;
+          *reinterpret_cast<uint4*>(vout + (bb * W + co) * ncell + xyy * Z + q * 8) =
+              *reinterpret_cast<const uint4*>(Os + co * kTcCols + r * Z + q * 8);
+        }
+      }
+    }
+    if (u_out) {
+      for (int i = threadIdx.x; i < R * Z; i += blockDim.x) {
+        const int r = i / Z, z = i - r * Z;
+        const size_t rw = row0 + r;
+        if (rw < nrows) {
+          float p[6];
+#pragma unroll
+          for (int j = 0; j < 6; ++j) p[j] = sqb[j];
+#pragma unroll 8
+          for (int co = 0; co < 32; ++co) {
+            const float o = __bfloat162float(Os[co * kTcCols + r * Z + z]);
+#pragma unroll
+            for (int j = 0; j < 6; ++j) p[j] += sQ[j * 32 + co] * o;
+          }
+          const size_t bb = rw / XY, xyy = rw - bb * XY;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const size_t idx = (bb * 3 + c) * ncell + xyy * Z + z;
+            const float2 fw = wave[idx];
+            u_out[idx] = make_float2(fw.x + p[2 * c], fw.y + p[2 * c + 1]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Register-blocked contraction Y[o][j][i] (op)= sum_l X[o][l][i] M[l][j] with
 // M (L x J) in shared memory; each thread produces JB consecutive j of one
 // (o, i), so X is read once instead of once per output.
@@ -931,6 +1242,27 @@ int em3d_fno_row_forward(int act, int lift, int B, int W, int X, int Y, int Z, i
   const int R = kRowThreads / Z;
   const size_t groups = ((size_t)B * X * Y + R - 1) / R;
   const int grid = (int)(groups < (size_t)148 * 12 ? groups : (size_t)148 * 12);
+  if (act == FNO_BF16 && W == 32 && Z % 32 == 0 && em3d_get_tuning(EM3D_TUNE_FNO_SIMT) == 0) {
+    const size_t tsm = row_fwd_tc_smem();
+    const int Rt = 128 / Z;
+    const size_t tgroups = ((size_t)B * X * Y + Rt - 1) / Rt;
+    const int tgrid = (int)(tgroups < (size_t)148 * 8 ? tgroups : (size_t)148 * 8);
+    using BF = __nv_bfloat16;
+    if (lift) {
+      if (!allow_dyn_smem((const void*)k_row_fwd_tc<true>, tsm)) return EM3D_ERR_CUDA;
+      k_row_fwd_tc<true><<<tgrid, 128, tsm, st>>>(B, X, Y, Z, m, (const float2*)chi, (const float2*)wave, nullptr,
+                                                    nullptr, (const BF*)Wt, bias, 0, (BF*)pre_out, (BF*)vout,
+                                                    (float2*)Vz, (const BF*)Q, qb, (float2*)u_out);
+    } else {
+      if (!allow_dyn_smem((const void*)k_row_fwd_tc<false>, tsm)) return EM3D_ERR_CUDA;
+      k_row_fwd_tc<false><<<tgrid, 128, tsm, st>>>(B, X, Y, Z, m, (const float2*)chi, (const float2*)wave,
+                                                     (const BF*)vin, (const float2*)Uxy, (const BF*)Wt, bias,
+                                                     apply_gelu, (BF*)pre_out, (BF*)vout, (float2*)Vz,
+                                                     (const BF*)Q, qb, (float2*)u_out);
+    }
+    EM3D_LAUNCH_CHECK();
+    return EM3D_OK;
+  }
   int rc = EM3D_OK;
   FNO_DISPATCH(act, (rc = launch_row_fwd<ACT>(lift != 0, grid, smem, st, B, W, X, Y, Z, m, chi, wave, vin, Uxy, Wt,
                                               bias, apply_gelu, pre_out, vout, Vz, Q, qb, u_out)));

@@ -641,7 +641,7 @@ static int ac_kernel_hat_full(const em3d_grid* g, const Dims& d, double k0, int 
 
 // Tuning knobs (em3d_set_tuning / em3d_get_tuning).  They select among
 // equivalent implementations; results do not depend on them beyond rounding.
-static int g_tuning[EM3D_TUNE_COUNT] = {-1, 0};
+static int g_tuning[EM3D_TUNE_COUNT] = {-1, 0, 0};
 
 static bool generic_forced() {
   const char* v = getenv("EM3D_FFT_GENERIC");
@@ -884,6 +884,10 @@ int em3d_set_tuning(int key, int value) {
   if (key < 0 || key >= EM3D_TUNE_COUNT) { em3d_set_last_error("unknown tuning key"); return EM3D_ERR_INVALID; }
   if (key == EM3D_TUNE_XPASS_VARIANT && (value < -1 || value > 4)) {
     em3d_set_last_error("x-pass variant must be -1 (automatic) or 0 .. 4");
+    return EM3D_ERR_INVALID;
+  }
+  if (key == EM3D_TUNE_FNO_SIMT && value != 0 && value != 1) {
+    em3d_set_last_error("FNO row-pass switch must be 0 or 1");
     return EM3D_ERR_INVALID;
   }
   g_tuning[key] = value;

@@ -60,7 +60,8 @@ enum em3d_tune_key {
                                    256-thread, 1 register 128-thread, 2 component-split, 3 persistent
                                    cp.async-pipelined 256-thread, 4 the same 128-thread */
   EM3D_TUNE_FFT_GENERIC = 1,   /* 1 = use the generic shared-memory FFT passes for every axis length */
-  EM3D_TUNE_COUNT = 2,
+  EM3D_TUNE_FNO_SIMT = 2,      /* 1 = FNO row pass on CUDA cores even where the tensor-core one applies */
+  EM3D_TUNE_COUNT = 3,
 };
 int em3d_set_tuning(int key, int value);
 int em3d_get_tuning(int key);

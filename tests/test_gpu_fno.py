@@ -119,3 +119,34 @@ def test_fused_row_forward_matches_separate_passes(act, tol, N, W, m):
             for x, y in zip(acts, net._buffers(B, N, train)["v"]):
                 e = float(torch.linalg.vector_norm(x - y.float()) / torch.linalg.vector_norm(y.float()))
                 assert e < tol * 4, e
+
+
+@pytest.mark.parametrize("N,m", [((10, 12, 32), 5), ((24, 26, 64), 12), ((24, 24, 128), 12), ((32, 33, 128), 16)])
+def test_tensor_core_row_pass_matches_cuda_core_pass(N, m):
+    """bf16, width 32: the mma.sync row kernel against the CUDA-core one (the
+    twiddles and mode coefficients enter the tensor cores as bf16)."""
+    import torch
+
+    from em3d_b200 import _lib
+    from em3d_b200.fno import FNO
+
+    rng = np.random.default_rng(12)
+    B = 2
+    chi = torch.as_tensor((_rand(rng, (B, 3, 3) + N) * 0.3).astype(np.complex64), device="cuda")
+    wave = torch.as_tensor(_rand(rng, (B, 3) + N).astype(np.complex64), device="cuda")
+    net = FNO(width=32, modes=m, layers=3, act="bf16", seed=2)
+    out = {}
+    for simt in (1, 0):
+        _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FNO_SIMT, simt)
+        for train in (False, True):
+            u = net.forward(chi, wave, train).clone()
+            acts = [t.float().clone() for t in net._buffers(B, N, train)["v"]] if train else []
+            out[(simt, train)] = (u, acts)
+    _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FNO_SIMT, 0)
+    torch.cuda.synchronize()
+    for train in (False, True):
+        a, b = out[(0, train)][0], out[(1, train)][0]
+        corr_a, corr_b = a - wave, b - wave   # the network's output proper
+        assert float(torch.linalg.vector_norm(corr_a - corr_b) / torch.linalg.vector_norm(corr_b)) < 3e-2
+        for x, y in zip(out[(0, train)][1], out[(1, train)][1]):
+            assert float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)) < 3e-2
