@@ -344,8 +344,16 @@ def run_ours(args, world, rank, local):
     launches = _lib.launch_count - launches0
     clocks = sampler.stop()
     value = world * 1000.0 / ms
+    # the comparison legs, each under its own clock record
+    leg_clocks = {}
+    sampler = ClockSampler(local)
+    sampler.start()
     fp64_ms, res64 = timed(fp64)
+    leg_clocks["fp64"] = sampler.stop()
+    sampler = ClockSampler(local)
+    sampler.start()
     zero_ms, res0 = timed(mixed_zero)
+    leg_clocks["mixed_zero"] = sampler.stop()
 
     def sol_err_max(results):
         """Max relative difference to the FP64 BiCGStab (complex128) solution of the same scene."""
@@ -398,6 +406,39 @@ def run_ours(args, world, rank, local):
     readme = {"workload": sc1.name, "iterations": r1.iterations, "status": r1.status,
               "mie_shape_err": cmp1["shape_err"], "mie_scale_ratio": cmp1["scale_ratio"],
               "mie_abs_rel_err": cmp1["abs_rel_err"]}
+
+    # -- 4c. 128 right-hand sides on one operator: the ellipsoid at 96^3, k0 = 10
+    from em3d_b200 import scenes as builders
+    from em3d_b200.solvers import DefectCorrection
+
+    c3 = workloads.aniso_ellipsoid_em(96, "double", k0=10.0)
+    g3 = e.Grid(N=c3.N, L=c3.L, center=c3.center, backend=be64)
+    p3 = e.Problem(grid=g3, eps_tensor=c3.chi, wave=c3.wave, k0=c3.k0, volume=1.0)
+    o64 = e.Operator(p3)
+    o32 = o64.with_precision(e.Precision.SINGLE)
+    dirs3 = workloads.fibonacci_directions(64)
+    waves3 = torch.empty((128, 3) + c3.N, dtype=torch.complex128, device=dev)
+    for i, d3 in enumerate(dirs3):
+        for j, pol in enumerate(workloads.orthogonal_polarisations(d3)):
+            builders.plane_wave(g3, k=c3.k0, orient=tuple(d3), amplitude=tuple(pol), out=waves3[2 * i + j])
+    chunk = 32
+    dcb = DefectCorrection(cfg)
+    dcb.solve_batch(o64, waves3[:chunk], operator_low=o32)
+    batch_ms, resb = _events_ms(lambda: [r for c0 in range(0, 128, chunk)
+                                         for r in dcb.solve_batch(o64, waves3[c0:c0 + chunk], operator_low=o32)])
+    mx3 = MixedBiCGStab(cfg)
+    mx3.solve(o64, waves3[0], operator_low=o32)
+    n_single = 8
+    single_ms, ress = _events_ms(lambda: [mx3.solve(o64, waves3[i], operator_low=o32) for i in range(n_single)])
+    multi_rhs = {"workload": "em_aniso_ellipsoid_96^3_k10_128_rhs", "rhs": 128, "batch": chunk,
+                 "batched_solves_per_s": 128 * 1000.0 / batch_ms, "batched_ms_total": batch_ms,
+                 "single_solves_per_s": n_single * 1000.0 / single_ms,
+                 "converged": int(sum(r.converged for r in resb)),
+                 "true_residual_max": max(float(r.true_final_residual) for r in resb),
+                 "outer_iterations_max": max(r.outer_iterations for r in resb)}
+    multi_rhs["batching_gain"] = multi_rhs["batched_solves_per_s"] / multi_rhs["single_solves_per_s"]
+    del o64, o32, waves3, dcb, mx3, resb, ress
+    torch.cuda.empty_cache()
 
     # -- 4b. the acoustic scene: 200 spheres at 256^3, k0 = 20 (eta sampled on the device)
     from em3d_b200 import acoustics as ea, farfield
@@ -484,6 +525,7 @@ def run_ours(args, world, rank, local):
                      "bytes_per_launch": bytes32, "ms_per_launch": mv32_ms, "peak_source": peak_kind},
         "cpu_baseline": cpu,
         "clocks": clocks,
+        "clocks_comparison_legs": leg_clocks,
         "gpu_launches": launches,
         "mixed_nn": summary(res_nn),
         "fp64": dict(summary(res64), ms=fp64_ms, solves_per_s=world * 1000.0 / fp64_ms),
@@ -498,6 +540,7 @@ def run_ours(args, world, rank, local):
                             "mixed_solution_rel_err_vs_fp64": aniso_err,
                             "fp64_true_residual": float(true_relative_residual(a64, b2.u, p2.wave))},
         "acoustic_spheres": acoustic,
+        "multi_rhs": multi_rhs,
         "readme_sphere_mie": readme,
         "matvec": {"fp32_ms": mv32_ms, "fp64_ms": mv64_ms, "fp32_gbs": ach32, "fp64_gbs": ach64,
                    "fp32_per_s": 1000.0 / mv32_ms, "fp64_per_s": 1000.0 / mv64_ms, "fp64_frac": ach64 / peak},
