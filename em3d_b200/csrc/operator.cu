@@ -764,18 +764,20 @@ static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& 
 // in registers, 256-thread CTAs; 1 = the same with 128-thread CTAs (two per
 // SM); 2 = component-split threads (EM only); 3 = persistent CTAs with the
 // next tile's field and spectrum prefetched by cp.async, 256 threads; 4 = the
-// same with 128 threads.  -1 (the default) picks 3 for EM and 0 for the
-// scalar acoustic operator, the fastest of each on B200 at 128^3 / 256^3.
-static int xmul_variant(int C) {
+// same with 128 threads.  -1 (the default) picks, per operator kind and
+// precision, the fastest measured on B200 at 128^3 (EM) / 256^3 (acoustic):
+// EM complex64 4, EM complex128 3, acoustic 0.
+static int xmul_variant(int C, bool fp64) {
   const int v = g_tuning[EM3D_TUNE_XPASS_VARIANT];
-  return v >= 0 ? v : (C == 3 ? 3 : 0);
+  if (v >= 0) return v;
+  return C == 3 ? (fp64 ? 3 : 4) : 0;
 }
 
 template <typename R, int C, bool ADJ, int L>
 static int launch_xmul_len(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
                            const int* skip, cudaStream_t st) {
   constexpr int EB = FastE<R>::E;
-  const int v = xmul_variant(C);
+  const int v = xmul_variant(C, sizeof(R) == 8);
   if constexpr (C == 3) {
     if (v == 2) return go_xsplit<R, L, ADJ, EB>(T2, spec, tw, d, batch, skip, st);
   }

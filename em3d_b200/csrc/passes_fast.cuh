@@ -405,28 +405,37 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     kz0 = (idx % ntz) * PP;
     ky = idx / ntz;
   };
+  // Prefetch loops: a thread always copies the kz lane p of its pencil and
+  // steps through the rows (component x position, or spectrum component x
+  // folded kx) with a constant stride, so the addresses are incremental.
+  constexpr int RSTEP = G::NT / PP;
   auto issue_field = [&](int tile) {
     int b, ky, kz0;
     decode(tile, b, ky, kz0);
-    const T* base = T2 + (size_t)b * C * NX * xstride + (size_t)ky * Nz2;
-    for (int i = threadIdx.x; i < G::FIELD; i += blockDim.x) {
-      const int q = i % PP, row = i / PP;   // row = c * NX + x
-      const int kz = kz0 + q;
-      if (kz < Nz2) cp_async_el(sfield + i, base + (size_t)row * xstride + kz, EB);
-      else sfield[i] = mk<R>(0, 0);
+    const bool ok = kz0 + p < Nz2;
+    int row = threadIdx.x / PP;                       // c * NX + x
+    const T* src = T2 + (size_t)b * C * NX * xstride + (size_t)ky * Nz2 + kz0 + p + (size_t)row * xstride;
+    T* dst = sfield + row * PP + p;
+    for (; row < C * NX; row += RSTEP, src += (size_t)RSTEP * xstride, dst += RSTEP * PP) {
+      if (ok) cp_async_el(dst, src, EB);
+      else *dst = mk<R>(0, 0);
     }
   };
   auto issue_spec = [&](int tile) {
     int b, ky, kz0;
     decode(tile, b, ky, kz0);
-    const int jy = kfold(ky, Ny);
-    const T* base = spec + (size_t)jy * (Nz + 1);
-    for (int i = threadIdx.x; i < G::SPEC; i += blockDim.x) {
-      const int q = i % PP, row = i / PP;   // row = component * (NX + 1) + ix
-      const int sc = row / (NX + 1), ix = row - sc * (NX + 1);
-      const int kz = kz0 + q;
-      if (kz < Nz2) cp_async_el(sspec + i, base + sc * ostride + (size_t)ix * (Ny + 1) * (Nz + 1) + kfold(kz, Nz), EB);
-      else sspec[i] = mk<R>(0, 0);
+    const int kz = kz0 + p;
+    const bool ok = kz < Nz2;
+    const T* base = spec + (size_t)kfold(ky, Ny) * (Nz + 1) + (ok ? kfold(kz, Nz) : 0);
+    const size_t xs = (size_t)(Ny + 1) * (Nz + 1);
+    int row = threadIdx.x / PP;                       // component * (NX + 1) + ix
+    int sc = row / (NX + 1), ix = row - sc * (NX + 1);
+    T* dst = sspec + row * PP + p;
+    for (; row < G::SPEC / PP; row += RSTEP, dst += RSTEP * PP) {
+      if (ok) cp_async_el(dst, base + sc * ostride + ix * xs, EB);
+      else *dst = mk<R>(0, 0);
+      ix += RSTEP;
+      while (ix > NX) { ix -= NX + 1; ++sc; }
     }
   };
 

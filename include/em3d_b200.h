@@ -56,7 +56,7 @@ const char* em3d_last_error(void);
  * in the reference, which has no native code to tune.
  * ------------------------------------------------------------------------ */
 enum em3d_tune_key {
-  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: 3 for EM, 0 acoustic), 0 register
+  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: EM complex64 4, complex128 3, acoustic 0), 0 register
                                    256-thread, 1 register 128-thread, 2 component-split, 3 persistent
                                    cp.async-pipelined 256-thread, 4 the same 128-thread */
   EM3D_TUNE_FFT_GENERIC = 1,   /* 1 = use the generic shared-memory FFT passes for every axis length */
