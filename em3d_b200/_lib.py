@@ -55,6 +55,14 @@ SIGNATURES = {
                                      c_size_t, c_void_p, c_void_p]),
     "em3d_acoustic_rmatvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                       c_size_t, c_void_p, c_void_p]),
+    "em3d_em_matvec_grouped": (c_int, [_GRID, c_int, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
+        c_void_p, c_size_t, c_void_p]),
+    "em3d_em_rmatvec_grouped": (c_int, [_GRID, c_int, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
+        c_void_p, c_size_t, c_void_p]),
+    "em3d_acoustic_matvec_grouped": (c_int, [_GRID, c_int, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
+        c_void_p, c_size_t, c_void_p]),
+    "em3d_acoustic_rmatvec_grouped": (c_int, [_GRID, c_int, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
+        c_void_p, c_size_t, c_void_p]),
     "em3d_em_matvec_static_scratch": (c_int, [_GRID, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                               c_void_p]),
     "em3d_static_scratch_bytes": (c_size_t, []),

@@ -40,6 +40,30 @@ template <typename R> __host__ __device__ __forceinline__ cx<R> from_c64(double2
 template <> __host__ __device__ __forceinline__ float2 from_c64<float>(double2 a) { return make_float2((float)a.x, (float)a.y); }
 template <> __host__ __device__ __forceinline__ double2 from_c64<double>(double2 a) { return a; }
 
+// Per-batch-entry addressing of an application.  chi / spec: element strides
+// between the entries' contrast and spectrum (zero when the whole batch shares
+// one operator; non-zero for a group of operators of one grid).  done
+// (nullable): entry b's stop flag at done + b * done_stride bytes (non-zero =
+// that entry's solve has stopped, its work is skipped); outer: pencil groups
+// per entry in the strided passes (C * Nx).
+struct BatchStrides {
+  size_t chi;
+  size_t spec;
+  const char* done;
+  size_t done_stride;
+  int outer;
+};
+
+__device__ __forceinline__ bool entry_done(const BatchStrides& bs, int b) {
+  return bs.done != nullptr && *(volatile const int*)(bs.done + (size_t)b * bs.done_stride) != 0;
+}
+__device__ __forceinline__ bool entries_done(const BatchStrides& bs, int b0, int b1) {
+  if (bs.done == nullptr) return false;
+  for (int b = b0; b <= b1; ++b)
+    if (!entry_done(bs, b)) return false;
+  return true;
+}
+
 // A kernel launched inside a device-resident solver loop returns at once when
 // the loop's status word says the solve has already stopped.
 __device__ __forceinline__ bool skip_launch(const int* flag) {

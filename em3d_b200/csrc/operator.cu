@@ -102,9 +102,19 @@ template <typename R, int C, int LD, int ST, bool INV>
 __global__ void __launch_bounds__(kThreads) k_rows(const cx<R>* in, const cx<R>* __restrict__ chi,
                                                    const cx<R>* base, cx<R>* out,
                                                    const cx<R>* __restrict__ twg, AxisPlan pl, int rows_pb,
-                                                   int nrows, int Lin, int Lout, int RPB, const int* skip) {
+                                                   int nrows, int Lin, int Lout, int RPB, BatchStrides bs,
+                                                   const int* skip) {
   using T = cx<R>;
   if (skip_launch(skip)) return;
+  // stop flags of the (usually one or two) entries this CTA's rows belong to, read once
+  const int gb0 = blockIdx.x * RPB, gb1 = min(gb0 + RPB, nrows) - 1;
+  const int eb0 = gb0 / rows_pb, eb1 = gb1 / rows_pb;
+  const bool d0 = entry_done(bs, eb0), d1 = entry_done(bs, eb1);
+  if (d0 && d1 && eb1 - eb0 <= 1) return;
+  auto row_done = [&](int g) {
+    const int bb = g / rows_pb;
+    return bb == eb0 ? d0 : (bb == eb1 ? d1 : entry_done(bs, bb));
+  };
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int L = pl.L;
   const int P = C * RPB, S = odd_stride(P);
@@ -120,7 +130,7 @@ __global__ void __launch_bounds__(kThreads) k_rows(const cx<R>* in, const cx<R>*
     T v[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) v[c] = mk<R>(0, 0);
-    if (g < nrows) {
+    if (g < nrows && !row_done(g)) {
       const int b = g / rows_pb, row = g - b * rows_pb;
       if constexpr (LD == LD_EM_CHI) {
         T uu[3];
@@ -130,11 +140,11 @@ __global__ void __launch_bounds__(kThreads) k_rows(const cx<R>* in, const cx<R>*
         for (int a = 0; a < 3; ++a) {
           T acc = mk<R>(0, 0);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) acc = cadd(acc, cmul(chi[((size_t)(a * 3 + c) * rows_pb + row) * Lin + k], uu[c]));
+          for (int c = 0; c < 3; ++c) acc = cadd(acc, cmul((chi + (size_t)b * bs.chi)[((size_t)(a * 3 + c) * rows_pb + row) * Lin + k], uu[c]));
           v[a] = acc;
         }
       } else if constexpr (LD == LD_AC_CHI) {
-        v[0] = cmul(chi[(size_t)row * Lin + k], in[((size_t)b * rows_pb + row) * Lin + k]);
+        v[0] = cmul((chi + (size_t)b * bs.chi)[(size_t)row * Lin + k], in[((size_t)b * rows_pb + row) * Lin + k]);
       } else {
 #pragma unroll
         for (int c = 0; c < C; ++c) v[c] = in[((size_t)(b * C + c) * rows_pb + row) * Lin + k];
@@ -153,7 +163,7 @@ __global__ void __launch_bounds__(kThreads) k_rows(const cx<R>* in, const cx<R>*
   for (int e = threadIdx.x; e < RPB * Lout; e += blockDim.x) {
     const int rl = e / Lout, k = e - rl * Lout;
     const int g = g0 + rl;
-    if (g >= nrows) continue;
+    if (g >= nrows || row_done(g)) continue;
     const int b = g / rows_pb, row = g - b * rows_pb;
     T y[C];
 #pragma unroll
@@ -172,14 +182,14 @@ __global__ void __launch_bounds__(kThreads) k_rows(const cx<R>* in, const cx<R>*
       for (int a = 0; a < 3; ++a) {
         T acc = mk<R>(0, 0);
 #pragma unroll
-        for (int c = 0; c < 3; ++c)  // (chi^H)[a][c] = conj(chi[c][a])
-          acc = cadd(acc, cmulcj(chi[((size_t)(c * 3 + a) * rows_pb + row) * Lout + k], y[c]));
+        for (int c = 0; c < 3; ++c)  // (chi^H)[a][c] = conj((chi + (size_t)b * bs.chi)[c][a])
+          acc = cadd(acc, cmulcj((chi + (size_t)b * bs.chi)[((size_t)(c * 3 + a) * rows_pb + row) * Lout + k], y[c]));
         const size_t o = ((size_t)(b * 3 + a) * rows_pb + row) * Lout + k;
         out[o] = csub(base[o], acc);
       }
     } else if constexpr (ST == ST_AC_ADJ) {
       const size_t o = ((size_t)b * rows_pb + row) * Lout + k;
-      out[o] = csub(base[o], cmulcj(chi[(size_t)row * Lout + k], y[0]));
+      out[o] = csub(base[o], cmulcj((chi + (size_t)b * bs.chi)[(size_t)row * Lout + k], y[0]));
     }
   }
 }
@@ -190,9 +200,10 @@ __global__ void __launch_bounds__(kThreads) k_rows(const cx<R>* in, const cx<R>*
 template <typename R, bool INV>
 __global__ void __launch_bounds__(kThreads) k_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg,
                                                       AxisPlan pl, int Lin, int Lout, int inner, int P, int ntiles,
-                                                      const int* skip) {
+                                                      BatchStrides bs, const int* skip) {
   using T = cx<R>;
   if (skip_launch(skip)) return;
+  if (bs.done && entry_done(bs, (int)(blockIdx.x / ntiles) / bs.outer)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int L = pl.L;
   const int S = odd_stride(P);
@@ -232,7 +243,8 @@ __device__ __forceinline__ int fsign(int k, int n) { return k <= n ? 1 : -1; }
 template <typename R, int C, bool ADJ>
 __global__ void __launch_bounds__(kThreads) k_xmul(cx<R>* T2, const cx<R>* __restrict__ spec,
                                                    const cx<R>* __restrict__ twg, AxisPlan pl, int Nx, int Ny,
-                                                   int Nz, int Pz, int ntz, int nb, const int* skip) {
+                                                   int Nz, int Pz, int ntz, int nb, BatchStrides bs,
+                                                   const int* skip) {
   using T = cx<R>;
   if (skip_launch(skip)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -248,6 +260,8 @@ __global__ void __launch_bounds__(kThreads) k_xmul(cx<R>* T2, const cx<R>* __res
   const int tile = idx % ntz;
   const int ky = idx / ntz;
   const int kz0 = tile * Pz;
+  if (entry_done(bs, b)) return;
+  spec += (size_t)b * bs.spec;
   const size_t xstride = (size_t)Ny2 * Nz2;
 
   for (int e = threadIdx.x; e < C * Nx * Pz; e += blockDim.x) {
@@ -459,7 +473,8 @@ template <typename R> static int tile_width(int L, int C) {
 
 template <typename R, int C, int LD, int ST, bool INV>
 static int launch_rows(const cx<R>* in, const cx<R>* chi, const cx<R>* base, cx<R>* out, const cx<R>* tw, int L,
-                       int rows_pb, int nrows, int Lin, int Lout, const int* skip, cudaStream_t st) {
+                       int rows_pb, int nrows, int Lin, int Lout, const int* skip, cudaStream_t st,
+                       BatchStrides bs = BatchStrides{}) {
   AxisPlan pl;
   make_axis_plan(L, &pl);
   const int rpb = rows_per_cta<R>(L, C, (size_t)nrows);
@@ -468,14 +483,14 @@ static int launch_rows(const cx<R>* in, const cx<R>* chi, const cx<R>* base, cx<
   auto kern = k_rows<R, C, LD, ST, INV>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const int grid = (nrows + rpb - 1) / rpb;
-  kern<<<grid, kThreads, smem, st>>>(in, chi, base, out, tw, pl, rows_pb, nrows, Lin, Lout, rpb, skip);
+  kern<<<grid, kThreads, smem, st>>>(in, chi, base, out, tw, pl, rows_pb, nrows, Lin, Lout, rpb, bs, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
 
 template <typename R, bool INV>
 static int launch_strided(const cx<R>* in, cx<R>* out, const cx<R>* tw, int L, int outer, int Lin, int Lout,
-                          int inner, const int* skip, cudaStream_t st) {
+                          int inner, const int* skip, cudaStream_t st, BatchStrides bs = BatchStrides{}) {
   AxisPlan pl;
   make_axis_plan(L, &pl);
   const int P = tile_width<R>(L, 1);
@@ -485,14 +500,14 @@ static int launch_strided(const cx<R>* in, cx<R>* out, const cx<R>* tw, int L, i
   EM3D_CUDA_TRY(allow_smem(kern));
   const size_t grid = (size_t)outer * ntiles;
   if (grid > 0x7fffffff) { em3d_set_last_error("grid too large"); return EM3D_ERR_INVALID; }
-  kern<<<(unsigned)grid, kThreads, smem, st>>>(in, out, tw, pl, Lin, Lout, inner, P, ntiles, skip);
+  kern<<<(unsigned)grid, kThreads, smem, st>>>(in, out, tw, pl, Lin, Lout, inner, P, ntiles, bs, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
 
 template <typename R, int C, bool ADJ>
 static int launch_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
-                       cudaStream_t st) {
+                       cudaStream_t st, BatchStrides bs) {
   AxisPlan pl;
   make_axis_plan(2 * d.nx, &pl);
   const int Pz = tile_width<R>(2 * d.nx, C);
@@ -502,7 +517,7 @@ static int launch_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims
   auto kern = k_xmul<R, C, ADJ>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const size_t grid = (size_t)batch * 2 * d.ny * ntz;
-  kern<<<(unsigned)grid, kThreads, smem, st>>>(T2, spec, tw, pl, d.nx, d.ny, d.nz, Pz, ntz, batch, skip);
+  kern<<<(unsigned)grid, kThreads, smem, st>>>(T2, spec, tw, pl, d.nx, d.ny, d.nz, Pz, ntz, batch, bs, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
@@ -654,26 +669,27 @@ static bool fast_len(int L) {
 
 template <typename R, int L, int C, int LD, int ST, bool INV>
 static int go_rows(const cx<R>* in, const cx<R>* chi, const cx<R>* base, cx<R>* out, const cx<R>* tw, int rows_pb,
-                   int nrows, const int* skip, cudaStream_t st) {
+                   int nrows, const int* skip, cudaStream_t st, BatchStrides bs) {
   using G = RowsGeom<L, FastE<R>::E, C>;
   auto kern = kf_rows<R, L, C, LD, ST, INV>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const size_t smem = (size_t)(L + C * G::RPB * G::PSTRIDE) * sizeof(cx<R>);
   const int grid = (nrows + G::RPB - 1) / G::RPB;
-  kern<<<grid, G::NT, smem, st>>>(in, chi, base, out, tw, rows_pb, nrows, skip);
+  kern<<<grid, G::NT, smem, st>>>(in, chi, base, out, tw, rows_pb, nrows, bs, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
 
 template <typename R, int C, int LD, int ST, bool INV>
 static int launch_rows_fast(int L, const cx<R>* in, const cx<R>* chi, const cx<R>* base, cx<R>* out,
-                            const cx<R>* tw, int rows_pb, int nrows, const int* skip, cudaStream_t st) {
+                            const cx<R>* tw, int rows_pb, int nrows, const int* skip, cudaStream_t st,
+                            BatchStrides bs) {
   switch (L) {
-    case 32: return go_rows<R, 32, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
-    case 64: return go_rows<R, 64, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
-    case 128: return go_rows<R, 128, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
-    case 256: return go_rows<R, 256, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
-    case 512: return go_rows<R, 512, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st);
+    case 32: return go_rows<R, 32, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
+    case 64: return go_rows<R, 64, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
+    case 128: return go_rows<R, 128, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
+    case 256: return go_rows<R, 256, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
+    case 512: return go_rows<R, 512, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
   }
   em3d_set_last_error("no register FFT for this length");
   return EM3D_ERR_UNSUPPORTED;
@@ -681,27 +697,27 @@ static int launch_rows_fast(int L, const cx<R>* in, const cx<R>* chi, const cx<R
 
 template <typename R, int L, bool INV>
 static int go_strided(const cx<R>* in, cx<R>* out, const cx<R>* tw, int outer, int inner, const int* skip,
-                      cudaStream_t st) {
+                      cudaStream_t st, BatchStrides bs) {
   using G = StridedGeom<L, FastE<R>::E>;
   auto kern = kf_strided<R, L, INV>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const int ntiles = (inner + G::P - 1) / G::P;
   const size_t smem = (size_t)(L + L * G::S) * sizeof(cx<R>);
   const size_t grid = (size_t)outer * ntiles;
-  kern<<<(unsigned)grid, G::NT, smem, st>>>(in, out, tw, inner, ntiles, skip);
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(in, out, tw, inner, ntiles, bs, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
 
 template <typename R, bool INV>
 static int launch_strided_fast(int L, const cx<R>* in, cx<R>* out, const cx<R>* tw, int outer, int inner,
-                               const int* skip, cudaStream_t st) {
+                               const int* skip, cudaStream_t st, BatchStrides bs) {
   switch (L) {
-    case 32: return go_strided<R, 32, INV>(in, out, tw, outer, inner, skip, st);
-    case 64: return go_strided<R, 64, INV>(in, out, tw, outer, inner, skip, st);
-    case 128: return go_strided<R, 128, INV>(in, out, tw, outer, inner, skip, st);
-    case 256: return go_strided<R, 256, INV>(in, out, tw, outer, inner, skip, st);
-    case 512: return go_strided<R, 512, INV>(in, out, tw, outer, inner, skip, st);
+    case 32: return go_strided<R, 32, INV>(in, out, tw, outer, inner, skip, st, bs);
+    case 64: return go_strided<R, 64, INV>(in, out, tw, outer, inner, skip, st, bs);
+    case 128: return go_strided<R, 128, INV>(in, out, tw, outer, inner, skip, st, bs);
+    case 256: return go_strided<R, 256, INV>(in, out, tw, outer, inner, skip, st, bs);
+    case 512: return go_strided<R, 512, INV>(in, out, tw, outer, inner, skip, st, bs);
   }
   em3d_set_last_error("no register FFT for this length");
   return EM3D_ERR_UNSUPPORTED;
@@ -709,21 +725,21 @@ static int launch_strided_fast(int L, const cx<R>* in, cx<R>* out, const cx<R>* 
 
 template <typename R, int L, int C, bool ADJ, int E, int NTT = 256>
 static int go_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
-                   cudaStream_t st) {
+                   cudaStream_t st, BatchStrides bs) {
   using G = XmulGeom<L, E, C, NTT>;
   auto kern = kf_xmul<R, L, C, ADJ, E, NTT>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const int ntz = (2 * d.nz + G::P - 1) / G::P;
   const size_t smem = (size_t)(L + G::REGIONS * L * G::S) * sizeof(cx<R>);
   const size_t grid = (size_t)batch * 2 * d.ny * ntz;
-  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, skip);
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, bs, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
 
 template <typename R, int L, int C, bool ADJ, int E, int NTT>
 static int go_xpipe(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
-                    cudaStream_t st) {
+                    cudaStream_t st, BatchStrides bs) {
   using G = XpipeGeom<L, E, C, NTT>;
   auto kern = kf_xmul_pipe<R, L, C, ADJ, E, NTT>;
   EM3D_CUDA_TRY(allow_smem(kern));
@@ -741,21 +757,21 @@ static int go_xpipe(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d
   if (per_sm < 1) per_sm = 1;
   const long long grid = std::min<long long>(ntiles, (long long)sms * per_sm);
   if (grid <= 0) return EM3D_OK;
-  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, skip);
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, bs, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
 
 template <typename R, int L, bool ADJ, int E>
 static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
-                     cudaStream_t st) {
+                     cudaStream_t st, BatchStrides bs) {
   using G = XsplitGeom<L, E>;
   auto kern = kf_xmul_split<R, L, ADJ, E>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const int ntz = (2 * d.nz + G::PZ - 1) / G::PZ;
   const size_t smem = (size_t)(L + 3 * G::REGION) * sizeof(cx<R>);
   const size_t grid = (size_t)batch * 2 * d.ny * ntz;
-  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, skip);
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, bs, skip);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
@@ -775,27 +791,27 @@ static int xmul_variant(int C, bool fp64) {
 
 template <typename R, int C, bool ADJ, int L>
 static int launch_xmul_len(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
-                           const int* skip, cudaStream_t st) {
+                           const int* skip, cudaStream_t st, BatchStrides bs) {
   constexpr int EB = FastE<R>::E;
   const int v = xmul_variant(C, sizeof(R) == 8);
   if constexpr (C == 3) {
-    if (v == 2) return go_xsplit<R, L, ADJ, EB>(T2, spec, tw, d, batch, skip, st);
+    if (v == 2) return go_xsplit<R, L, ADJ, EB>(T2, spec, tw, d, batch, skip, st, bs);
   }
-  if (v == 3) return go_xpipe<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st);
-  if (v == 4) return go_xpipe<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st);
-  if (v == 1) return go_xmul<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st);
-  return go_xmul<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st);
+  if (v == 3) return go_xpipe<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st, bs);
+  if (v == 4) return go_xpipe<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st, bs);
+  if (v == 1) return go_xmul<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st, bs);
+  return go_xmul<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st, bs);
 }
 
 template <typename R, int C, bool ADJ>
 static int launch_xmul_fast(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
-                            const int* skip, cudaStream_t st) {
+                            const int* skip, cudaStream_t st, BatchStrides bs) {
   switch (2 * d.nx) {
-    case 32: return launch_xmul_len<R, C, ADJ, 32>(T2, spec, tw, d, batch, skip, st);
-    case 64: return launch_xmul_len<R, C, ADJ, 64>(T2, spec, tw, d, batch, skip, st);
-    case 128: return launch_xmul_len<R, C, ADJ, 128>(T2, spec, tw, d, batch, skip, st);
-    case 256: return launch_xmul_len<R, C, ADJ, 256>(T2, spec, tw, d, batch, skip, st);
-    case 512: return launch_xmul_len<R, C, ADJ, 512>(T2, spec, tw, d, batch, skip, st);
+    case 32: return launch_xmul_len<R, C, ADJ, 32>(T2, spec, tw, d, batch, skip, st, bs);
+    case 64: return launch_xmul_len<R, C, ADJ, 64>(T2, spec, tw, d, batch, skip, st, bs);
+    case 128: return launch_xmul_len<R, C, ADJ, 128>(T2, spec, tw, d, batch, skip, st, bs);
+    case 256: return launch_xmul_len<R, C, ADJ, 256>(T2, spec, tw, d, batch, skip, st, bs);
+    case 512: return launch_xmul_len<R, C, ADJ, 512>(T2, spec, tw, d, batch, skip, st, bs);
   }
   em3d_set_last_error("no register FFT for this length");
   return EM3D_ERR_UNSUPPORTED;
@@ -805,12 +821,13 @@ static int launch_xmul_fast(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const
 // The five passes of one application.
 template <typename R, int C, bool ADJ>
 static int apply(const Dims& d, int batch, const void* spectrum, const void* chi, const void* u, void* out, void* ws,
-                 size_t wsb, const int* skip, cudaStream_t st) {
+                 size_t wsb, const int* skip, cudaStream_t st, BatchStrides bs = BatchStrides{}) {
   if (batch < 1) { em3d_set_last_error("batch must be >= 1"); return EM3D_ERR_INVALID; }
   if (!spectrum || !chi || !u || !out) { em3d_set_last_error("NULL array argument"); return EM3D_ERR_INVALID; }
   if (!ws || wsb < apply_ws_bytes<R>(d, C, batch)) { em3d_set_last_error("apply workspace too small"); return EM3D_ERR_INVALID; }
   if (out == u) { em3d_set_last_error("out must not alias the input field"); return EM3D_ERR_INVALID; }
   using T = cx<R>;
+  bs.outer = C * d.nx;
   SpecLayout<R> lay(d, C == 3 ? EM3D_EM : EM3D_ACOUSTIC);
   void* sp = const_cast<void*>(spectrum);
   const T* twx = lay.twx(sp, d);
@@ -833,32 +850,32 @@ static int apply(const Dims& d, int batch, const void* spectrum, const void* chi
   constexpr int FSTA = C == 3 ? FST_EM_ADJ : FST_AC_ADJ;
   // pass 1: rows along z, chi applied on load (matvec) or plain (rmatvec)
   if (fz) {
-    if (!ADJ) rc = launch_rows_fast<R, C, FLDF, FST_PLAIN, false>(Lz, uu, ch, nullptr, T1, twz, rows, nrows, skip, st);
-    else rc = launch_rows_fast<R, C, FLD_PLAIN, FST_PLAIN, false>(Lz, uu, nullptr, nullptr, T1, twz, rows, nrows, skip, st);
+    if (!ADJ) rc = launch_rows_fast<R, C, FLDF, FST_PLAIN, false>(Lz, uu, ch, nullptr, T1, twz, rows, nrows, skip, st, bs);
+    else rc = launch_rows_fast<R, C, FLD_PLAIN, FST_PLAIN, false>(Lz, uu, nullptr, nullptr, T1, twz, rows, nrows, skip, st, bs);
   } else {
-    if (!ADJ) rc = launch_rows<R, C, LDF, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st);
-    else rc = launch_rows<R, C, LD_PLAIN, ST_PLAIN, false>(uu, nullptr, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st);
+    if (!ADJ) rc = launch_rows<R, C, LDF, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st, bs);
+    else rc = launch_rows<R, C, LD_PLAIN, ST_PLAIN, false>(uu, nullptr, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st, bs);
   }
   if (rc) return rc;
   // pass 2: (batch*C*Nx, Ny, 2Nz) -> (batch*C*Nx, 2Ny, 2Nz)
-  if (fy) rc = launch_strided_fast<R, false>(Ly, T1, T2, twy, batch * C * d.nx, Lz, skip, st);
-  else rc = launch_strided<R, false>(T1, T2, twy, Ly, batch * C * d.nx, d.ny, Ly, Lz, skip, st);
+  if (fy) rc = launch_strided_fast<R, false>(Ly, T1, T2, twy, batch * C * d.nx, Lz, skip, st, bs);
+  else rc = launch_strided<R, false>(T1, T2, twy, Ly, batch * C * d.nx, d.ny, Ly, Lz, skip, st, bs);
   if (rc) return rc;
   // pass 3
-  if (fx) rc = launch_xmul_fast<R, C, ADJ>(T2, oct, twx, d, batch, skip, st);
-  else rc = launch_xmul<R, C, ADJ>(T2, oct, twx, d, batch, skip, st);
+  if (fx) rc = launch_xmul_fast<R, C, ADJ>(T2, oct, twx, d, batch, skip, st, bs);
+  else rc = launch_xmul<R, C, ADJ>(T2, oct, twx, d, batch, skip, st, bs);
   if (rc) return rc;
   // pass 4: (batch*C*Nx, 2Ny, 2Nz) -> (batch*C*Nx, Ny, 2Nz)
-  if (fy) rc = launch_strided_fast<R, true>(Ly, T2, T1, twy, batch * C * d.nx, Lz, skip, st);
-  else rc = launch_strided<R, true>(T2, T1, twy, Ly, batch * C * d.nx, Ly, d.ny, Lz, skip, st);
+  if (fy) rc = launch_strided_fast<R, true>(Ly, T2, T1, twy, batch * C * d.nx, Lz, skip, st, bs);
+  else rc = launch_strided<R, true>(T2, T1, twy, Ly, batch * C * d.nx, Ly, d.ny, Lz, skip, st, bs);
   if (rc) return rc;
   // pass 5: rows along z, crop and combine
   if (fz) {
-    if (!ADJ) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_SUB, true>(Lz, T1, nullptr, uu, o, twz, rows, nrows, skip, st);
-    else rc = launch_rows_fast<R, C, FLD_PLAIN, FSTA, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st);
+    if (!ADJ) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_SUB, true>(Lz, T1, nullptr, uu, o, twz, rows, nrows, skip, st, bs);
+    else rc = launch_rows_fast<R, C, FLD_PLAIN, FSTA, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st, bs);
   } else {
-    if (!ADJ) rc = launch_rows<R, C, LD_PLAIN, ST_SUB, true>(T1, nullptr, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st);
-    else rc = launch_rows<R, C, LD_PLAIN, STA, true>(T1, ch, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st);
+    if (!ADJ) rc = launch_rows<R, C, LD_PLAIN, ST_SUB, true>(T1, nullptr, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st, bs);
+    else rc = launch_rows<R, C, LD_PLAIN, STA, true>(T1, ch, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st, bs);
   }
   return rc;
 }
@@ -874,6 +891,36 @@ static int apply_dispatch(const em3d_grid* g, int dtype, int batch, const void* 
   if (dtype == EM3D_C128) return apply<double, C, ADJ>(d, batch, spectrum, chi, u, out, ws, wsb, skip, st);
   em3d_set_last_error("dtype must be EM3D_C64 or EM3D_C128");
   return EM3D_ERR_INVALID;
+}
+
+// A group of operators on one grid: batch entry b has its own contrast
+// (chi + b * chi_stride elements) and spectrum (spectra + b * spectrum_stride
+// bytes); the twiddle tables of entry 0 serve all (they depend on the grid
+// only).  entry_done: optional per-entry stop flags (see BatchStrides).
+template <int C, bool ADJ>
+static int apply_grouped(const em3d_grid* g, int dtype, int batch, const void* spectra, size_t spectrum_stride,
+                         const void* chis, const void* u, void* out, void* ws, size_t wsb, const int* skip,
+                         const void* entry_done, size_t entry_done_stride, void* stream) {
+  Dims d;
+  int rc = check_grid(g, &d);
+  if (rc) return rc;
+  if (dtype != EM3D_C64 && dtype != EM3D_C128) { em3d_set_last_error("dtype must be EM3D_C64 or EM3D_C128"); return EM3D_ERR_INVALID; }
+  const int kind = C == 3 ? EM3D_EM : EM3D_ACOUSTIC;
+  const size_t esz = dtype == EM3D_C64 ? sizeof(float2) : sizeof(double2);
+  if (spectrum_stride < em3d_spectrum_bytes(g, kind, dtype) || spectrum_stride % esz != 0) {
+    em3d_set_last_error("spectrum_stride must be >= em3d_spectrum_bytes and a multiple of the element size");
+    return EM3D_ERR_INVALID;
+  }
+  if (entry_done && entry_done_stride < sizeof(int)) {
+    em3d_set_last_error("entry_done_stride must be at least sizeof(int)");
+    return EM3D_ERR_INVALID;
+  }
+  const size_t ncell = (size_t)d.nx * d.ny * d.nz;
+  const BatchStrides bs{(C == 3 ? 9 : 1) * ncell, spectrum_stride / esz, (const char*)entry_done,
+                        entry_done_stride, 0};
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == EM3D_C64) return apply<float, C, ADJ>(d, batch, spectra, chis, u, out, ws, wsb, skip, st, bs);
+  return apply<double, C, ADJ>(d, batch, spectra, chis, u, out, ws, wsb, skip, st, bs);
 }
 
 }  // namespace em3d
@@ -967,6 +1014,31 @@ int em3d_acoustic_kernel_hat_full(const em3d_grid* g, double k0, int dtype, int 
   if (dtype == EM3D_C128) return ac_kernel_hat_full<double>(g, d, k0, adjoint, out, ws, wsb, st);
   em3d_set_last_error("dtype must be EM3D_C64 or EM3D_C128");
   return EM3D_ERR_INVALID;
+}
+
+int em3d_em_matvec_grouped(const em3d_grid* g, int dtype, int batch, const void* spectra, size_t spectrum_stride,
+    const void* chis, const void* u, void* out, void* ws, size_t wsb, const int* skip, const void* entry_done,
+    size_t entry_done_stride, void* stream) {
+  return apply_grouped<3, false>(g, dtype, batch, spectra, spectrum_stride, chis, u, out, ws, wsb, skip, entry_done,
+                                 entry_done_stride, stream);
+}
+int em3d_em_rmatvec_grouped(const em3d_grid* g, int dtype, int batch, const void* spectra, size_t spectrum_stride,
+    const void* chis, const void* v, void* out, void* ws, size_t wsb, const int* skip, const void* entry_done,
+    size_t entry_done_stride, void* stream) {
+  return apply_grouped<3, true>(g, dtype, batch, spectra, spectrum_stride, chis, v, out, ws, wsb, skip, entry_done,
+                                 entry_done_stride, stream);
+}
+int em3d_acoustic_matvec_grouped(const em3d_grid* g, int dtype, int batch, const void* spectra, size_t spectrum_stride,
+    const void* chis, const void* u, void* out, void* ws, size_t wsb, const int* skip, const void* entry_done,
+    size_t entry_done_stride, void* stream) {
+  return apply_grouped<1, false>(g, dtype, batch, spectra, spectrum_stride, chis, u, out, ws, wsb, skip, entry_done,
+                                 entry_done_stride, stream);
+}
+int em3d_acoustic_rmatvec_grouped(const em3d_grid* g, int dtype, int batch, const void* spectra, size_t spectrum_stride,
+    const void* chis, const void* v, void* out, void* ws, size_t wsb, const int* skip, const void* entry_done,
+    size_t entry_done_stride, void* stream) {
+  return apply_grouped<1, true>(g, dtype, batch, spectra, spectrum_stride, chis, v, out, ws, wsb, skip, entry_done,
+                                 entry_done_stride, stream);
 }
 
 int em3d_em_matvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi, const void* u,

@@ -28,7 +28,7 @@ template <int L, int E, int C> struct RowsGeom {
 template <typename R, int L, int C, int LD, int ST, bool INV>
 __global__ void __launch_bounds__(RowsGeom<L, FastE<R>::E, C>::NT)
 kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>* out,
-        const cx<R>* __restrict__ twg, int rows_pb, int nrows, const int* skip) {
+        const cx<R>* __restrict__ twg, int rows_pb, int nrows, BatchStrides bs, const int* skip) {
   using T = cx<R>;
   constexpr int E = FastE<R>::E;
   using G = RowsGeom<L, E, C>;
@@ -39,6 +39,10 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
   constexpr int LIN = INV ? L : L / 2;
   constexpr int LOUT = INV ? L / 2 : L;
   if (skip_launch(skip)) return;
+  {
+    const int g0 = blockIdx.x * RPB, g1 = min(g0 + RPB, nrows) - 1;
+    if (entries_done(bs, g0 / rows_pb, g1 / rows_pb)) return;
+  }
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tw = reinterpret_cast<T*>(smem_raw);
   T* sm = tw + L;
@@ -47,9 +51,11 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
   const int pen = threadIdx.x / TT;
   const int c = pen / RPB, rl = pen - c * RPB;
   const int g = blockIdx.x * RPB + rl;
-  const bool valid = g < nrows;
+  // rows of stopped entries are treated like rows past the end (no loads, no stores)
+  const bool valid = g < nrows && !entry_done(bs, g / rows_pb);
   const int b = valid ? g / rows_pb : 0;
   const int row = valid ? g - b * rows_pb : 0;
+  const cx<R>* chb = chi ? chi + (size_t)b * bs.chi : nullptr;
 
   T a[1][E];
 #pragma unroll
@@ -65,9 +71,9 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
           const size_t cs = (size_t)rows_pb * LIN;
           const T* ub = in + (size_t)b * 3 * cs;
 #pragma unroll
-          for (int k = 0; k < 3; ++k) v = cadd(v, cmul(chi[(size_t)(c * 3 + k) * cs + o], ub[k * cs + o]));
+          for (int k = 0; k < 3; ++k) v = cadd(v, cmul(chb[(size_t)(c * 3 + k) * cs + o], ub[k * cs + o]));
         } else if constexpr (LD == FLD_AC_CHI) {
-          v = cmul(chi[(size_t)row * LIN + pos], in[((size_t)b * rows_pb + row) * LIN + pos]);
+          v = cmul(chb[(size_t)row * LIN + pos], in[((size_t)b * rows_pb + row) * LIN + pos]);
         } else {
           v = in[((size_t)(b * C + c) * rows_pb + row) * LIN + pos];
         }
@@ -102,7 +108,7 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           const T yk = sm[(k * RPB + rl) * G::PSTRIDE + pos + (pos >> 4)];
-          acc = cadd(acc, cmulcj(chi[(size_t)(k * 3 + c) * cs + o], yk));
+          acc = cadd(acc, cmulcj(chb[(size_t)(k * 3 + c) * cs + o], yk));
         }
         const size_t oo = (size_t)(b * 3 + c) * cs + o;
         out[oo] = csub(base[oo], acc);
@@ -122,7 +128,7 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
         const size_t oo = ((size_t)(b * C + c) * rows_pb + row) * LOUT + pos;
         if constexpr (ST == FST_PLAIN) out[oo] = y;
         else if constexpr (ST == FST_SUB) out[oo] = csub(base[oo], y);
-        else if constexpr (ST == FST_AC_ADJ) out[oo] = csub(base[oo], cmulcj(chi[(size_t)row * LOUT + pos], y));
+        else if constexpr (ST == FST_AC_ADJ) out[oo] = csub(base[oo], cmulcj(chb[(size_t)row * LOUT + pos], y));
       }
     }
   }
@@ -138,7 +144,8 @@ template <int L, int E> struct StridedGeom {
 // Pencils along y: in (outer, L/2 or L, inner) -> out (outer, L or L/2, inner).
 template <typename R, int L, bool INV>
 __global__ void __launch_bounds__(StridedGeom<L, FastE<R>::E>::NT)
-kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner, int ntiles, const int* skip) {
+kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner, int ntiles, BatchStrides bs,
+           const int* skip) {
   using T = cx<R>;
   constexpr int E = FastE<R>::E;
   using G = StridedGeom<L, E>;
@@ -149,6 +156,7 @@ kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner
   constexpr int LIN = INV ? L : L / 2;
   constexpr int LOUT = INV ? L / 2 : L;
   if (skip_launch(skip)) return;
+  if (bs.done && entry_done(bs, (int)(blockIdx.x / ntiles) / bs.outer)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tw = reinterpret_cast<T*>(smem_raw);
   T* sm = tw + L;
@@ -245,7 +253,7 @@ __device__ __forceinline__ int kfold(int k, int n) { return k <= n ? k : 2 * n -
 template <typename R, int L, int C, bool ADJ, int E, int NTT>
 __global__ void __launch_bounds__(XmulGeom<L, E, C, NTT>::NT)
 kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
-        int nb, const int* skip) {
+        int nb, BatchStrides bs, const int* skip) {
   using T = cx<R>;
   using G = XmulGeom<L, E, C, NTT>;
   using PL = RegPlan<L, E>;
@@ -265,6 +273,7 @@ kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg
   idx /= nb;
   const int tile = idx % ntz;
   const int ky = idx / ntz;
+  if (entry_done(bs, b)) return;
   const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
   const int kz = tile * PP + p;
   const bool valid = kz < Nz2;
@@ -291,7 +300,7 @@ kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg
   const int jy = kfold(ky, Ny);
   const int l = kfold(valid ? kz : 0, Nz);
   const size_t ostride = (size_t)(Nx + 1) * (Ny + 1) * (Nz + 1);
-  const T* sp = spec + (size_t)jy * (Nz + 1) + l;
+  const T* sp = spec + (size_t)b * bs.spec + (size_t)jy * (Nz + 1) + l;
   const R sy = ky <= Ny ? (R)1 : (R)-1;
   const R sz = kz <= Nz ? (R)1 : (R)-1;
 #pragma unroll
@@ -378,7 +387,7 @@ template <int L, int E, int C, int NTT> struct XpipeGeom {
 template <typename R, int L, int C, bool ADJ, int E, int NTT>
 __global__ void __launch_bounds__(XpipeGeom<L, E, C, NTT>::NT)
 kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
-             int nb, const int* skip) {
+             int nb, BatchStrides bs, const int* skip) {
   using T = cx<R>;
   using G = XpipeGeom<L, E, C, NTT>;
   using PL = RegPlan<L, E>;
@@ -412,6 +421,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   auto issue_field = [&](int tile) {
     int b, ky, kz0;
     decode(tile, b, ky, kz0);
+    if (entry_done(bs, b)) return;
     const bool ok = kz0 + p < Nz2;
     int row = threadIdx.x / PP;                       // c * NX + x
     const T* src = T2 + (size_t)b * C * NX * xstride + (size_t)ky * Nz2 + kz0 + p + (size_t)row * xstride;
@@ -424,9 +434,10 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   auto issue_spec = [&](int tile) {
     int b, ky, kz0;
     decode(tile, b, ky, kz0);
+    if (entry_done(bs, b)) return;
     const int kz = kz0 + p;
     const bool ok = kz < Nz2;
-    const T* base = spec + (size_t)kfold(ky, Ny) * (Nz + 1) + (ok ? kfold(kz, Nz) : 0);
+    const T* base = spec + (size_t)b * bs.spec + (size_t)kfold(ky, Ny) * (Nz + 1) + (ok ? kfold(kz, Nz) : 0);
     const size_t xs = (size_t)(Ny + 1) * (Nz + 1);
     int row = threadIdx.x / PP;                       // component * (NX + 1) + ix
     int sc = row / (NX + 1), ix = row - sc * (NX + 1);
@@ -452,6 +463,8 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     const int kz = kz0 + p;
     const bool valid = kz < Nz2;
     const int next = tile + gridDim.x;
+    // the same for every thread of the CTA, so the barriers below stay uniform
+    const bool live = !entry_done(bs, b);
 
     cp_async_wait_one();  // this tile's field slab
     __syncthreads();
@@ -470,7 +483,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     if (next < ntiles) issue_field(next);
     cp_async_commit();
 
-    reg_fft_x<L, E, false, false, true, C>(a, t, sm, tw, lay);
+    if (live) reg_fft_x<L, E, false, false, true, C>(a, t, sm, tw, lay);
 
     cp_async_wait_one();  // this tile's spectrum slab
     __syncthreads();
@@ -506,8 +519,8 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     if (next < ntiles) issue_spec(next);
     cp_async_commit();
 
-    reg_fft_x<L, E, true, true, true, C>(a, t, sm, tw, lay);
-    if (valid) {
+    if (live) reg_fft_x<L, E, true, true, true, C>(a, t, sm, tw, lay);
+    if (valid && live) {
       T* col = T2 + (size_t)b * C * NX * xstride + (size_t)ky * Nz2 + kz;
 #pragma unroll
       for (int q = 0; q < E / R1; ++q) {
@@ -542,7 +555,7 @@ template <int L, int E> struct XsplitGeom {
 template <typename R, int L, bool ADJ, int E>
 __global__ void __launch_bounds__(XsplitGeom<L, E>::NT, 2)
 kf_xmul_split(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
-              int nb, const int* skip) {
+              int nb, BatchStrides bs, const int* skip) {
   using T = cx<R>;
   using G = XsplitGeom<L, E>;
   using PL = RegPlan<L, E>;
@@ -564,6 +577,7 @@ kf_xmul_split(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict
   idx /= nb;
   const int tile = idx % ntz;
   const int ky = idx / ntz;
+  if (entry_done(bs, b)) return;
   const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
   const int kz = tile * PZ + p;
   const bool valid = kz < Nz2;
@@ -607,9 +621,10 @@ kf_xmul_split(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict
   const int l = kfold(valid ? kz : 0, Nz);
   const size_t ostride = (size_t)(Nx + 1) * (Ny + 1) * (Nz + 1);
   const size_t rowstride = (size_t)(Ny + 1) * (Nz + 1);
-  const T* spd = spec + bd * ostride + (size_t)jy * (Nz + 1) + l;
-  const T* sp1 = spec + b1 * ostride + (size_t)jy * (Nz + 1) + l;
-  const T* sp2 = spec + b2 * ostride + (size_t)jy * (Nz + 1) + l;
+  const T* sb0 = spec + (size_t)b * bs.spec;
+  const T* spd = sb0 + bd * ostride + (size_t)jy * (Nz + 1) + l;
+  const T* sp1 = sb0 + b1 * ostride + (size_t)jy * (Nz + 1) + l;
+  const T* sp2 = sb0 + b2 * ostride + (size_t)jy * (Nz + 1) + l;
 #pragma unroll
   for (int q = 0; q < E / RL; ++q) {
     const int j = t + q * TT;

@@ -236,7 +236,12 @@ class _Engine:
         flag is the skip flag; set-up calls pass ``skip=False`` because the
         state may still hold the previous solve's flags."""
         if self.native_op:
-            self.op.apply_into(x, out, adjoint=adjoint, skip_ptr=self.state.done_ptr if skip else None)
+            if skip and self.batch > 1 and getattr(self.op, "accepts_entry_skip", False):
+                # a group of problems: stopped entries skip their share of the work
+                self.op.apply_into(x, out, adjoint=adjoint, skip_ptr=self.state.done_ptr,
+                                   entry_done=(self.state.ptr + KrylovState.status.offset, self.state.stride))
+            else:
+                self.op.apply_into(x, out, adjoint=adjoint, skip_ptr=self.state.done_ptr if skip else None)
         else:
             import torch
 

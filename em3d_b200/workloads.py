@@ -161,3 +161,43 @@ def multi_rhs_ellipsoid(N: int = 96, k0: float = 10.0, n_directions: int = 64, p
     axes = _setup.grid_axes_host(case.N, case.L, case.center, precision)
     waves = plane_wave_batch(axes, k0, n_directions, dtype=_setup.complex_dtype_of(precision))
     return case, waves
+
+
+def uneven_sphere_params(count: int = 48, seed: int = 0, sizes=(32, 48, 64, 80)) -> list:
+    """A set of ``count`` independent single-sphere EM problems of uneven grid
+    sizes: N from ``sizes`` in turn, radius U[0.15, 0.3], eps_r U[1.5, 3.0] +
+    i U[0, 0.1], k0 U[4, 10], a unit propagation direction drawn uniformly and
+    a polarisation orthogonal to it.  Returns dicts (N, center, radius, eps,
+    k0, orient, amplitude)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        N = int(sizes[i % len(sizes)])
+        radius = float(rng.uniform(0.15, 0.3))
+        center = tuple(float(v) for v in rng.uniform(-0.1, 0.1, 3))
+        eps = complex(rng.uniform(1.5, 3.0), rng.uniform(0.0, 0.1))
+        k0 = float(rng.uniform(4.0, 10.0))
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        amp = orthogonal_polarisations(d)[0]
+        out.append(dict(N=N, center=center, radius=radius, eps=eps, k0=k0, orient=tuple(float(v) for v in d),
+                        amplitude=tuple(float(v) for v in amp)))
+    return out
+
+
+def uneven_sphere_problems(precision: str = "single", count: int = 48, seed: int = 0, sizes=(32, 48, 64, 80),
+                           device_index: int = 0) -> list:
+    """``uneven_sphere_params`` built on the device (contrast by the scene
+    sampler at the reference's tolerance, plane wave by the wave kernel)."""
+    from . import scenes
+    from .backend import Backend, Precision
+    from .problem import Grid, Problem
+
+    be = Backend.b200(Precision.SINGLE if precision == "single" else Precision.DOUBLE, device_index=device_index)
+    problems = []
+    for p in uneven_sphere_params(count, seed, sizes):
+        grid = Grid(N=(p["N"],) * 3, L=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0), backend=be)
+        chi = scenes.sample_scene(grid, [scenes.EllipsoidShape(p["center"], (p["radius"],) * 3, None, p["eps"])])
+        wave = scenes.plane_wave(grid, k=p["k0"], orient=p["orient"], amplitude=p["amplitude"])
+        problems.append(Problem(grid=grid, eps_tensor=chi, wave=wave, k0=p["k0"], volume=1.0))
+    return problems

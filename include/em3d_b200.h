@@ -139,6 +139,31 @@ int em3d_em_matvec_static_scratch(const em3d_grid* g, int dtype, const void* spe
 /* Size of that fixed workspace in bytes. */
 size_t em3d_static_scratch_bytes(void);
 
+/* Groups of operators on one grid (many problems of the same size, each with
+ * its own contrast and wave number): batch entry b of u / out is applied with
+ * the contrast at chis + b * (9 or 1) * Nx*Ny*Nz elements and the spectrum at
+ * spectra + b * spectrum_stride bytes (each built by em3d_*_spectrum_build;
+ * spectrum_stride >= em3d_spectrum_bytes, a multiple of the element size).
+ * One launch per pass for the whole group; workspace as for a batch of that
+ * size.  entry_done (nullable): entry b's int stop flag at entry_done +
+ * b * entry_done_stride bytes; the work of entries whose flag is non-zero is
+ * skipped and their out left as it was (a batched solve passes its per-entry
+ * status words).  No counterpart call in the reference, which solves such
+ * sets one problem at a time with src/em3d/operator.py:320-428 /
+ * src/em3d/acoustics/operator.py:25-73. */
+int em3d_em_matvec_grouped(const em3d_grid* g, int dtype, int batch, const void* spectra, size_t spectrum_stride,
+    const void* chis, const void* u, void* out, void* workspace, size_t workspace_bytes, const int* skip,
+    const void* entry_done, size_t entry_done_stride, void* stream);
+int em3d_em_rmatvec_grouped(const em3d_grid* g, int dtype, int batch, const void* spectra, size_t spectrum_stride,
+    const void* chis, const void* v, void* out, void* workspace, size_t workspace_bytes, const int* skip,
+    const void* entry_done, size_t entry_done_stride, void* stream);
+int em3d_acoustic_matvec_grouped(const em3d_grid* g, int dtype, int batch, const void* spectra, size_t spectrum_stride,
+    const void* chis, const void* u, void* out, void* workspace, size_t workspace_bytes, const int* skip,
+    const void* entry_done, size_t entry_done_stride, void* stream);
+int em3d_acoustic_rmatvec_grouped(const em3d_grid* g, int dtype, int batch, const void* spectra, size_t spectrum_stride,
+    const void* chis, const void* v, void* out, void* workspace, size_t workspace_bytes, const int* skip,
+    const void* entry_done, size_t entry_done_stride, void* stream);
+
 /* Scalar versions.  Replace AcousticOperator.matvec / rmatvec
  * (src/em3d/acoustics/operator.py:40-67). */
 int em3d_acoustic_matvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi,
