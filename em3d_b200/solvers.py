@@ -792,8 +792,8 @@ class MixedBiCGStab:
     updated residuals in hybrid Bi-CG methods", Computing 56 (1996).
 
     ``x0`` is judged like in :class:`DefectCorrection`: a guess whose true
-    residual is not below ``||f||`` is replaced by the zero guess.  One
-    right-hand side per solve (``DefectCorrection.solve_batch`` batches).
+    residual is not below ``||f||`` is replaced by the zero guess.
+    ``solve_batch`` runs many right-hand sides (or a group of problems) at once.
     """
 
     graph_chunk = 4
@@ -809,7 +809,7 @@ class MixedBiCGStab:
         self.guess_fallback = bool(guess_fallback)
         self.max_cycles = int(max_cycles)
 
-    def _buffers(self, operator, rhs, operator_low):
+    def _buffers(self, operator, rhs, batch, operator_low):
         from collections import OrderedDict
 
         import torch
@@ -818,16 +818,16 @@ class MixedBiCGStab:
 
         if not hasattr(self, "_cache"):
             self._cache = OrderedDict()
-        key = (id(operator), tuple(rhs.shape))
+        key = (id(operator), tuple(rhs.shape), batch)
         hit = self._cache.get(key)
         if hit is not None and hit["op"] is operator and (operator_low is None or hit["op_lo"] is operator_low):
             self._cache.move_to_end(key)
             hit["eng"].load_rhs(rhs)
             return hit
-        eng = _Engine(operator, rhs, hist_cap=4, batch=1)
+        eng = _Engine(operator, rhs, hist_cap=4, batch=batch)
         op_lo = operator_low if operator_low is not None else operator.with_precision(Precision.SINGLE)
         zero32 = torch.zeros(eng.rhs.shape, dtype=torch.complex64, device=eng.rhs.device)
-        e32 = _Engine(op_lo, zero32, hist_cap=int(self.cfg.max_iter) + 4, batch=1)
+        e32 = _Engine(op_lo, zero32, hist_cap=int(self.cfg.max_iter) + 4, batch=batch)
         vec32 = {k: e32.vec() for k in ("u", "r", "r_hat", "p", "v", "s", "t")}
         hit = {"op": operator, "op_lo": op_lo, "eng": eng, "u": eng.vec(), "r": eng.vec(), "e32": e32,
                "v32": vec32}
@@ -839,46 +839,81 @@ class MixedBiCGStab:
     def solve(self, operator, rhs, x0=None, *, operator_low=None) -> DefectCorrectionResult:
         import torch
 
-        cfg = self.cfg
         t = rhs if isinstance(rhs, torch.Tensor) else torch.as_tensor(np.asarray(rhs))
         if _batch_of(operator, t) != 1:
-            raise NotImplementedError("MixedBiCGStab solves one right-hand side; use DefectCorrection.solve_batch")
-        buf = self._buffers(operator, t, operator_low)
+            raise NotImplementedError("MixedBiCGStab.solve takes one right-hand side; use solve_batch")
+        return self._solve(operator, t, x0, 1, operator_low)[0]
+
+    def solve_batch(self, operator, rhs, x0=None, *, operator_low=None) -> list:
+        """``rhs`` stacked along a leading axis (or a group of problems and its
+        stacked right-hand sides).  Each right-hand side runs its own cycles
+        and stops on its own true residual, exactly as its single solve: a
+        cycle of the batch runs until every entry has met its cycle target,
+        entries that met theirs wait (their iteration work is skipped), then
+        one FP64 application forms every true residual."""
+        import torch
+
+        t = rhs if isinstance(rhs, torch.Tensor) else torch.as_tensor(np.asarray(rhs))
+        b = _batch_of(operator, t)
+        t = t.reshape((b,) + tuple(operator._field_shape()))
+        return self._solve(operator, t, x0, b, operator_low)
+
+    def _solve(self, operator, rhs, x0, batch, operator_low) -> list:
+        cfg = self.cfg
+        buf = self._buffers(operator, rhs, batch, operator_low)
         eng, e32, V = buf["eng"], buf["e32"], buf["v32"]
         f = eng.rhs
         x = _load_u(buf["u"], x0)
         r = buf["r"]
         stream = eng.stream()
-        fn = eng.norm(f)
-        if fn == 0.0:
-            x.zero_()
-            return DefectCorrectionResult(u=x.clone(), iterations=0, residual_history=[0.0], converged=True,
-                                          matvec_count=0, residual_action_counts=[0], status="converged",
-                                          true_final_residual=0.0)
-        tol = max(float(cfg.rtol), float(cfg.atol) / fn)
-        mv64 = 0
 
-        def true_residual():
-            nonlocal mv64
-            operator.apply_into(x, r)
-            mv64 += 1
-            _lib.call("em3d_vec_axpby", eng.dt, eng.n, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0, r.data_ptr(),
-                      stream)
-            return eng.norm(r) / fn
+        def row(t, b):
+            return t if batch == 1 else t[b]
 
-        rel = true_residual()
-        rejected = False
-        if x0 is not None and self.guess_fallback and not rel < 1.0:
-            x.zero_()
-            r.copy_(f)
-            rel = 1.0
-            rejected = True
-        hist, counts = [float(rel)], [mv64]
-        status = None
-        if not np.isfinite(rel):
-            status = "nonfinite"
-        elif rel < tol:
-            status = "converged"
+        fn = eng.norms(f)
+        fs = np.where(fn == 0.0, 1.0, fn)
+        tol = np.maximum(float(cfg.rtol), float(cfg.atol) / fs)
+        status = [None] * batch
+        for b in range(batch):
+            if fn[b] == 0.0:
+                row(x, b).zero_()
+                status[b] = "zero"
+        skip_entries = batch > 1 and getattr(operator, "accepts_entry_skip", False)
+        mv64 = np.zeros(batch, dtype=np.int64)
+
+        def true_residual(active):
+            if skip_entries:
+                # entries that have stopped skip the FP64 application
+                for b, h in enumerate(eng.state.hosts):
+                    h.status = 0 if b in active else 1
+                eng.state.upload()
+                operator.apply_into(x, r, entry_done=(eng.state.ptr + KrylovState.status.offset,
+                                                      eng.state.stride))
+            else:
+                operator.apply_into(x, r)
+            mv64[list(active)] += 1
+            _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0,
+                      r.data_ptr(), stream)
+            return eng.norms(r) / fs
+
+        hist = [[] for _ in range(batch)]
+        counts = [[] for _ in range(batch)]
+        rejected = [False] * batch
+        active = [b for b in range(batch) if status[b] is None]
+        if active:
+            rel = true_residual(active)
+            for b in active:
+                if x0 is not None and self.guess_fallback and not rel[b] < 1.0:
+                    row(x, b).zero_()
+                    row(r, b).copy_(row(f, b))
+                    rel[b] = 1.0
+                    rejected[b] = True
+                hist[b].append(float(rel[b]))
+                counts[b].append(int(mv64[b]))
+                if not np.isfinite(rel[b]):
+                    status[b] = "nonfinite"
+                elif rel[b] < tol[b]:
+                    status[b] = "converged"
 
         u32, r32, rh, p, v, s, tt = (V[k] for k in ("u", "r", "r_hat", "p", "v", "s", "t"))
 
@@ -893,73 +928,108 @@ class MixedBiCGStab:
                      rh.data_ptr())
             e32.step("em3d_bicgstab_finalize", u32.data_ptr(), p.data_ptr())
 
-        st = e32.state.host
-        restart = True
-        total_its = 0
-        mv32 = 0
-        cycles = []
-        stalled = 0
+        hosts = e32.state.hosts
+        restart = [True] * batch
+        total_its = np.zeros(batch, dtype=np.int64)
+        mv32 = np.zeros(batch, dtype=np.int64)
+        cycles = [[] for _ in range(batch)]
+        stalled = np.zeros(batch, dtype=np.int64)
         budget = int(cfg.max_iter)
-        while status is None:
-            if total_its >= budget or len(cycles) >= self.max_cycles:
-                status = "max_iter"
+        it0 = np.zeros(batch, dtype=np.int64)
+        mv_before = np.zeros(batch, dtype=np.int64)
+        while True:
+            for b in range(batch):
+                if status[b] is None and (total_its[b] >= budget or len(cycles[b]) >= self.max_cycles):
+                    status[b] = "max_iter"
+            running = [b for b in range(batch) if status[b] is None]
+            if not running:
                 break
-            _lib.call("em3d_vec_convert", eng.n, eng.dt, r.data_ptr(), _lib.EM3D_C64, r32.data_ptr(), 0, stream)
+            _lib.call("em3d_vec_convert", eng.n * batch, eng.dt, r.data_ptr(), _lib.EM3D_C64, r32.data_ptr(), 0,
+                      stream)
             u32.zero_()
-            n0 = e32.norm(r32)
-            if restart:
-                rh.copy_(r32)
-                st.iter = 0
-                st.rho_re, st.rho_im = n0 * n0, 0.0
-                st.rho_prev_re, st.rho_prev_im = 1.0, 0.0
-                st.alpha_re, st.alpha_im = 1.0, 0.0
-                st.omega_re, st.omega_im = 1.0, 0.0
-            else:
-                _lib.call("em3d_vec_dots", _lib.EM3D_C64, e32.n, 1, rh.data_ptr(), r32.data_ptr(), None, None,
+            n0 = e32.norms(r32)
+            dots = None
+            if any(not restart[b] for b in running):
+                _lib.call("em3d_vec_dots", _lib.EM3D_C64, e32.n, batch, rh.data_ptr(), r32.data_ptr(), None, None,
                           e32.state.ptr, e32.state.stride, stream)
-                rho_new = e32.state.dots()[0][0]
-                st.rho_prev_re, st.rho_prev_im = st.rho_re, st.rho_im
-                st.rho_re, st.rho_im = rho_new.real, rho_new.imag
-            it0 = int(st.iter)
-            st.rhs_norm = n0
-            st.tol = max(self.delta, self.safety * tol * fn / n0)
-            st.guard = -1.0
-            st.status = 0
-            st.pending = 0
-            st.first = 1  # cycles end on full iterations only
-            st.max_iter = it0 + (budget - total_its)
-            st.max_actions = -1
-            st.last_rel = 1.0
-            mv_before = int(st.matvecs)
-            e32.state.upload([[1.0]], [[mv_before]])
+                dots = e32.state.dots()
+            for b, st in enumerate(hosts):
+                if status[b] is not None:
+                    # stopped: every kernel of the cycle skips this entry
+                    st.status = 1
+                    st.pending = 0
+                    continue
+                if restart[b]:
+                    row(rh, b).copy_(row(r32, b))
+                    st.iter = 0
+                    st.rho_re, st.rho_im = n0[b] * n0[b], 0.0
+                    st.rho_prev_re, st.rho_prev_im = 1.0, 0.0
+                    st.alpha_re, st.alpha_im = 1.0, 0.0
+                    st.omega_re, st.omega_im = 1.0, 0.0
+                else:
+                    rho_new = dots[b][0]
+                    st.rho_prev_re, st.rho_prev_im = st.rho_re, st.rho_im
+                    st.rho_re, st.rho_im = rho_new.real, rho_new.imag
+                it0[b] = int(st.iter)
+                st.rhs_norm = n0[b]
+                st.tol = max(self.delta, self.safety * tol[b] * fs[b] / n0[b])
+                st.guard = -1.0
+                st.status = 0
+                st.pending = 0
+                st.first = 1  # cycles end on full iterations only
+                st.max_iter = int(it0[b] + (budget - total_its[b]))
+                st.max_actions = -1
+                st.last_rel = 1.0
+                mv_before[b] = int(st.matvecs)
+            e32.state.upload([[1.0]] * batch, [[int(m)] for m in mv_before])
             e32.run(iteration, self.graph_chunk, use_graph=True)
-            got = e32.state.download()[0][0]
-            for name in ("rho_re", "rho_im", "rho_prev_re", "rho_prev_im", "alpha_re", "alpha_im", "omega_re",
-                         "omega_im", "iter", "matvecs", "status", "pending"):
-                setattr(st, name, getattr(got, name))
-            its = int(got.iter) - it0
-            total_its += its
-            mv32 += int(got.matvecs) - mv_before
-            cycles.append(its)
-            _lib.call("em3d_vec_convert", eng.n, _lib.EM3D_C64, u32.data_ptr(), eng.dt, x.data_ptr(), 1, stream)
-            rel = true_residual()
-            hist.append(float(rel))
-            counts.append(mv64 + mv32)
-            inner = _status_name(got.status)
-            if cfg.log:
-                print(f"[MixedBiCGStab] update={len(cycles)}, fp32_iterations={its} ({inner}), rel_res={rel:.3e}")
-            if not np.isfinite(rel):
-                status = "nonfinite"
-            elif rel < tol:
-                status = "converged"
-            elif cfg.divergence_guard is not None and rel > float(cfg.divergence_guard):
-                status = "divergence_guard"
-            stalled = stalled + 1 if its == 0 else 0
-            if status is None and stalled >= 2:
-                status = inner if inner not in ("converged", "running") else "max_iter"
-            restart = int(got.pending) != 0 or inner not in ("converged", "max_iter")
-        return DefectCorrectionResult(
-            u=x.clone(), iterations=int(total_its), residual_history=hist, converged=status == "converged",
-            matvec_count=int(mv64 + mv32), rmatvec_count=0, residual_action_counts=counts, status=status,
-            true_final_residual=float(hist[-1]), outer_iterations=len(cycles), inner_iterations=cycles,
-            fp64_matvecs=int(mv64), fp32_matvecs=int(mv32), guess_rejected=rejected)
+            got_all = e32.state.download()
+            its_of = {}
+            for b in running:
+                got = got_all[b][0]
+                st = hosts[b]
+                for name in ("rho_re", "rho_im", "rho_prev_re", "rho_prev_im", "alpha_re", "alpha_im", "omega_re",
+                             "omega_im", "iter", "matvecs", "status", "pending"):
+                    setattr(st, name, getattr(got, name))
+                its = int(got.iter) - int(it0[b])
+                its_of[b] = its
+                total_its[b] += its
+                mv32[b] += int(got.matvecs) - int(mv_before[b])
+                cycles[b].append(its)
+            _lib.call("em3d_vec_convert", eng.n * batch, _lib.EM3D_C64, u32.data_ptr(), eng.dt, x.data_ptr(), 1,
+                      stream)
+            rel = true_residual(running)
+            for b in running:
+                st = hosts[b]
+                hist[b].append(float(rel[b]))
+                counts[b].append(int(mv64[b] + mv32[b]))
+                inner = _status_name(st.status)
+                if cfg.log:
+                    print(f"[MixedBiCGStab] rhs={b}, update={len(cycles[b])}, fp32_iterations={its_of[b]} "
+                          f"({inner}), rel_res={rel[b]:.3e}")
+                if not np.isfinite(rel[b]):
+                    status[b] = "nonfinite"
+                elif rel[b] < tol[b]:
+                    status[b] = "converged"
+                elif cfg.divergence_guard is not None and rel[b] > float(cfg.divergence_guard):
+                    status[b] = "divergence_guard"
+                stalled[b] = stalled[b] + 1 if its_of[b] == 0 else 0
+                if status[b] is None and stalled[b] >= 2:
+                    status[b] = inner if inner not in ("converged", "running") else "max_iter"
+                restart[b] = int(st.pending) != 0 or inner not in ("converged", "max_iter")
+        u = x.clone()  # the cached buffer is reused by the next solve
+        out = []
+        for b in range(batch):
+            ub = row(u, b)
+            if status[b] == "zero":
+                out.append(DefectCorrectionResult(u=ub, iterations=0, residual_history=[0.0], converged=True,
+                                                  matvec_count=0, residual_action_counts=[0], status="converged",
+                                                  true_final_residual=0.0))
+                continue
+            out.append(DefectCorrectionResult(
+                u=ub, iterations=int(total_its[b]), residual_history=hist[b], converged=status[b] == "converged",
+                matvec_count=int(mv64[b] + mv32[b]), rmatvec_count=0, residual_action_counts=counts[b],
+                status=status[b], true_final_residual=float(hist[b][-1]), outer_iterations=len(cycles[b]),
+                inner_iterations=cycles[b], fp64_matvecs=int(mv64[b]), fp32_matvecs=int(mv32[b]),
+                guess_rejected=rejected[b]))
+        return out
