@@ -422,22 +422,69 @@ def run_ours(args, world, rank, local):
         for j, pol in enumerate(workloads.orthogonal_polarisations(d3)):
             builders.plane_wave(g3, k=c3.k0, orient=tuple(d3), amplitude=tuple(pol), out=waves3[2 * i + j])
     chunk = 32
-    dcb = DefectCorrection(cfg)
-    dcb.solve_batch(o64, waves3[:chunk], operator_low=o32)
+    mxb = MixedBiCGStab(cfg)
+    mxb.solve_batch(o64, waves3[:chunk], operator_low=o32)
     batch_ms, resb = _events_ms(lambda: [r for c0 in range(0, 128, chunk)
-                                         for r in dcb.solve_batch(o64, waves3[c0:c0 + chunk], operator_low=o32)])
+                                         for r in mxb.solve_batch(o64, waves3[c0:c0 + chunk], operator_low=o32)])
     mx3 = MixedBiCGStab(cfg)
     mx3.solve(o64, waves3[0], operator_low=o32)
-    n_single = 8
+    n_single = 16
     single_ms, ress = _events_ms(lambda: [mx3.solve(o64, waves3[i], operator_low=o32) for i in range(n_single)])
+    dcb = DefectCorrection(cfg)
+    dcb.solve_batch(o64, waves3[:chunk], operator_low=o32)
+    dc_ms, resd = _events_ms(lambda: [r for c0 in range(0, 128, chunk)
+                                      for r in dcb.solve_batch(o64, waves3[c0:c0 + chunk], operator_low=o32)])
     multi_rhs = {"workload": "em_aniso_ellipsoid_96^3_k10_128_rhs", "rhs": 128, "batch": chunk,
+                 "solver": "MixedBiCGStab (FP32 BiCGStab, FP64 reliable updates) batched vs one right-hand side "
+                           "at a time",
                  "batched_solves_per_s": 128 * 1000.0 / batch_ms, "batched_ms_total": batch_ms,
-                 "single_solves_per_s": n_single * 1000.0 / single_ms,
+                 "single_solves_per_s": n_single * 1000.0 / single_ms, "single_sample": n_single,
                  "converged": int(sum(r.converged for r in resb)),
                  "true_residual_max": max(float(r.true_final_residual) for r in resb),
-                 "outer_iterations_max": max(r.outer_iterations for r in resb)}
+                 "iterations_max": max(r.iterations for r in resb),
+                 "iterations_equal_single": all(resb[i].iterations == ress[i].iterations for i in range(n_single)),
+                 "defect_correction_batched_solves_per_s": 128 * 1000.0 / dc_ms}
     multi_rhs["batching_gain"] = multi_rhs["batched_solves_per_s"] / multi_rhs["single_solves_per_s"]
-    del o64, o32, waves3, dcb, mx3, resb, ress
+    del o64, o32, waves3, dcb, mx3, mxb, resb, ress, resd
+    torch.cuda.empty_cache()
+
+    # -- 4d. 48 independent sphere problems of uneven sizes (N in {32, 48, 64, 80}, own spectrum each):
+    # one group per size, all problems of a group in every launch, vs one problem at a time
+    from em3d_b200.groups import group_by_grid
+
+    probs = workloads.uneven_sphere_problems("double", 48, seed=0)
+    groups = group_by_grid(probs)
+    lows = {key: grp.with_precision(e.Precision.SINGLE) for key, (_, grp) in groups.items()}
+    mxg = MixedBiCGStab(cfg)
+    mxg.max_cached = 2 * len(groups)
+
+    def grouped():
+        out = [None] * len(probs)
+        for key, (idx, grp) in groups.items():
+            for i, r in zip(idx, mxg.solve_batch(grp, grp.waves(), operator_low=lows[key])):
+                out[i] = r
+        return out
+
+    grouped()
+    grouped_ms, resg = _events_ms(grouped)
+    ops1 = [e.Operator(p) for p in probs]
+    ops1_lo = [o.with_precision(e.Precision.SINGLE) for o in ops1]
+    mx1 = MixedBiCGStab(cfg)
+    mx1.max_cached = 2 * len(probs)
+
+    def one_by_one():
+        return [mx1.solve(o, p.wave, operator_low=ol) for o, ol, p in zip(ops1, ops1_lo, probs)]
+
+    one_by_one()
+    single48_ms, res1 = _events_ms(one_by_one)
+    uneven = {"workload": "uneven_spheres_48_N32-80", "sizes": {str(k[0][0]): len(v[0]) for k, v in groups.items()},
+              "solver": "MixedBiCGStab grouped by grid size vs one problem at a time",
+              "grouped_ms": grouped_ms, "one_by_one_ms": single48_ms, "gain": single48_ms / grouped_ms,
+              "grouped_solves_per_s": len(probs) * 1000.0 / grouped_ms,
+              "converged": int(sum(r.converged for r in resg)),
+              "true_residual_max": max(float(r.true_final_residual) for r in resg),
+              "iterations_equal_one_by_one": all(a.iterations == b.iterations for a, b in zip(resg, res1))}
+    del probs, groups, lows, mxg, ops1, ops1_lo, mx1, resg, res1
     torch.cuda.empty_cache()
 
     # -- 4b. the acoustic scene: 200 spheres at 256^3, k0 = 20 (eta sampled on the device)
@@ -541,6 +588,7 @@ def run_ours(args, world, rank, local):
                             "fp64_true_residual": float(true_relative_residual(a64, b2.u, p2.wave))},
         "acoustic_spheres": acoustic,
         "multi_rhs": multi_rhs,
+        "uneven_problems": uneven,
         "readme_sphere_mie": readme,
         "matvec": {"fp32_ms": mv32_ms, "fp64_ms": mv64_ms, "fp32_gbs": ach32, "fp64_gbs": ach64,
                    "fp32_per_s": 1000.0 / mv32_ms, "fp64_per_s": 1000.0 / mv64_ms, "fp64_frac": ach64 / peak},

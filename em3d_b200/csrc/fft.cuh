@@ -185,13 +185,74 @@ template <bool INV, typename C> __device__ __forceinline__ void dft5(C* a) {
   else      { a[1] = cadd(b1, ie1); a[4] = csub(b1, ie1); a[2] = cadd(b2, ie2); a[3] = csub(b2, ie2); }
 }
 
+// cos and sin of 2 pi m / n for n in {6, 10, 12} (compile-time m): the
+// angles are multiples of 30 or 36 degrees, whose values are sqrt(3)/2, 1/2
+// and (sqrt(5) +- 1)/4 with their complements.
+__host__ __device__ constexpr double root_cos(int n, int m) {
+  constexpr double h3 = 0.86602540378443864676, c36 = 0.80901699437494742410, c72 = 0.30901699437494742410;
+  if (n == 6) return root_cos(12, 2 * m);
+  if (n == 12) {
+    constexpr double t[12] = {1.0, h3, 0.5, 0.0, -0.5, -h3, -1.0, -h3, -0.5, 0.0, 0.5, h3};
+    return t[m % 12];
+  }
+  constexpr double t[10] = {1.0, c36, c72, -c72, -c36, -1.0, -c36, -c72, c72, c36};
+  return t[m % 10];
+}
+__host__ __device__ constexpr double root_sin(int n, int m) {
+  constexpr double h3 = 0.86602540378443864676, s36 = 0.58778525229247312917, s72 = 0.95105651629515357212;
+  if (n == 6) return root_sin(12, 2 * m);
+  if (n == 12) {
+    constexpr double t[12] = {0.0, 0.5, h3, 1.0, h3, 0.5, 0.0, -0.5, -h3, -1.0, -h3, -0.5};
+    return t[m % 12];
+  }
+  constexpr double t[10] = {0.0, s36, s72, s72, s36, 0.0, -s36, -s72, -s72, -s36};
+  return t[m % 10];
+}
+
+template <int RX, bool INV, typename C> __device__ __forceinline__ void dft_fixed(C* a);
+
+// Radix A*B in registers (Cooley-Tukey, n = B n1 + n2, k = k1 + A k2):
+// B DFTs of length A on the inputs a[B n1 + n2], twiddles w_{AB}^{n2 k1},
+// then A DFTs of length B giving X[k1 + A k2].
+template <int A, int B, bool INV, typename C> __device__ __forceinline__ void dft_comp(C* a) {
+  using R = decltype(a[0].x);
+  constexpr int RX = A * B;
+  C y[B][A];
+#pragma unroll
+  for (int n2 = 0; n2 < B; ++n2) {
+#pragma unroll
+    for (int n1 = 0; n1 < A; ++n1) y[n2][n1] = a[B * n1 + n2];
+    dft_fixed<A, INV>(y[n2]);
+#pragma unroll
+    for (int k1 = 1; k1 < A; ++k1) {
+      if (n2 == 0) continue;
+      const int m = (n2 * k1) % RX;
+      const R c = (R)root_cos(RX, m), s = (R)root_sin(RX, m);
+      y[n2][k1] = cmul(y[n2][k1], mk<R>(c, INV ? s : -s));
+    }
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < A; ++k1) {
+    C z[B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) z[n2] = y[n2][k1];
+    dft_fixed<B, INV>(z);
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) a[k1 + A * k2] = z[k2];
+  }
+}
+
 template <int RX, bool INV, typename C> __device__ __forceinline__ void dft_fixed(C* a) {
   if constexpr (RX == 2) dft2<INV>(a[0], a[1]);
   else if constexpr (RX == 3) dft3<INV>(a[0], a[1], a[2]);
   else if constexpr (RX == 4) dft4<INV>(a[0], a[1], a[2], a[3]);
   else if constexpr (RX == 5) dft5<INV>(a);
+  else if constexpr (RX == 6) dft_comp<2, 3, INV>(a);
   else if constexpr (RX == 8) dft8<INV>(a);
+  else if constexpr (RX == 10) dft_comp<2, 5, INV>(a);
+  else if constexpr (RX == 12) dft_comp<4, 3, INV>(a);
   else if constexpr (RX == 16) dft16<INV>(a);
+  else static_assert(RX == 2, "no fixed DFT for this radix");
 }
 
 // One Stockham stage with a compile-time radix.

@@ -1,4 +1,5 @@
-// Register-resident Stockham FFT for power-of-two lengths 32..1024.
+// Register-resident Stockham FFT for power-of-two lengths 32..1024 and the
+// mixed lengths 96, 160 and 192.
 //
 // T = L / E threads cooperate on one pencil; each holds E elements in
 // registers.  A stage of radix R (a power of two dividing E) runs E / R
@@ -24,14 +25,28 @@ namespace em3d {
 
 __host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x / 2); }
 
+// Mixed-radix plans (L = 3 or 5 times a power of two).  The first and last
+// radices are even, so the zero-padded half of a forward input and the
+// cropped half of an inverse output are whole register groups, exactly as in
+// the power-of-two plans; every radix divides E.
+__host__ __device__ constexpr int mixed_stages(int L, int E) {
+  return (L == 96 && E == 12) || (L == 192 && E == 12) || (L == 160 && E == 20) ? 3 : 0;
+}
+__host__ __device__ constexpr int mixed_radix(int L, int E, int s) {
+  return s != 1 ? 4 : (L == 96 ? 6 : L == 192 ? 12 : 10);
+}
+
 template <int L, int E> struct RegPlan {
-  static_assert((L & (L - 1)) == 0 && (E & (E - 1)) == 0 && L >= E && E >= 2, "power-of-two plan");
+  static constexpr bool POW2 = (L & (L - 1)) == 0 && (E & (E - 1)) == 0;
+  static_assert(L >= E && E >= 2 && (POW2 || mixed_stages(L, E) > 0), "no register plan for this length");
   static constexpr int A = ilog2c(L), EB = ilog2c(E);
-  static constexpr int NS = (A + EB - 1) / EB;
+  static constexpr int NS = POW2 ? (A + EB - 1) / EB : mixed_stages(L, E);
   static constexpr int T = L / E;
   __host__ __device__ static constexpr int bits(int s) { return A / NS + (s < A % NS ? 1 : 0); }
   // radix of stage s in forward (REV = false) or reversed order
-  __host__ __device__ static constexpr int rad(bool rev, int s) { return 1 << bits(rev ? NS - 1 - s : s); }
+  __host__ __device__ static constexpr int rad(bool rev, int s) {
+    return POW2 ? 1 << bits(rev ? NS - 1 - s : s) : mixed_radix(L, E, rev ? NS - 1 - s : s);
+  }
   __host__ __device__ static constexpr int nsb(bool rev, int s) {
     int n = 1;
     for (int i = 0; i < s; ++i) n *= rad(rev, i);
@@ -39,6 +54,12 @@ template <int L, int E> struct RegPlan {
   }
   __host__ __device__ static constexpr int first(bool rev) { return rad(rev, 0); }
   __host__ __device__ static constexpr int last(bool rev) { return rad(rev, NS - 1); }
+  __host__ __device__ static constexpr bool valid() {
+    for (int s = 0; s < NS; ++s)
+      if (E % rad(false, s) != 0) return false;
+    return nsb(false, NS) == L && first(false) % 2 == 0 && last(false) % 2 == 0;
+  }
+  static_assert(valid(), "register plan: radices must divide E, multiply to L, and start and end even");
 };
 
 // Twiddle-multiply and DFT of this thread's butterflies in one stage, for C

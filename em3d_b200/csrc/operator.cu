@@ -652,7 +652,7 @@ static int ac_kernel_hat_full(const em3d_grid* g, const Dims& d, double k0, int 
   return EM3D_OK;
 }
 
-// ---- register-FFT dispatch (power-of-two doubled axes 32..512) -----------
+// ---- register-FFT dispatch (doubled axes 32..512 and 96, 160, 192) -------
 
 // Tuning knobs (em3d_set_tuning / em3d_get_tuning).  They select among
 // equivalent implementations; results do not depend on them beyond rounding.
@@ -663,14 +663,17 @@ static bool generic_forced() {
   return g_tuning[EM3D_TUNE_FFT_GENERIC] != 0 || (v && v[0] == '1');
 }
 
-static bool fast_len(int L) {
-  return !generic_forced() && (L == 32 || L == 64 || L == 128 || L == 256 || L == 512);
+// 160 has a register plan in complex64 only: its 20 elements per thread
+// would spill in complex128.
+static bool fast_len(int L, bool fp64) {
+  return !generic_forced() &&
+         (L == 32 || L == 64 || L == 128 || L == 256 || L == 512 || L == 96 || L == 192 || (L == 160 && !fp64));
 }
 
 template <typename R, int L, int C, int LD, int ST, bool INV>
 static int go_rows(const cx<R>* in, const cx<R>* chi, const cx<R>* base, cx<R>* out, const cx<R>* tw, int rows_pb,
                    int nrows, const int* skip, cudaStream_t st, BatchStrides bs) {
-  using G = RowsGeom<L, FastE<R>::E, C>;
+  using G = RowsGeom<L, FastE<R, L>::E, C>;
   auto kern = kf_rows<R, L, C, LD, ST, INV>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const size_t smem = (size_t)(L + C * G::RPB * G::PSTRIDE) * sizeof(cx<R>);
@@ -690,6 +693,11 @@ static int launch_rows_fast(int L, const cx<R>* in, const cx<R>* chi, const cx<R
     case 128: return go_rows<R, 128, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
     case 256: return go_rows<R, 256, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
     case 512: return go_rows<R, 512, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
+    case 96: return go_rows<R, 96, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
+    case 160:
+      if constexpr (sizeof(R) == 4) return go_rows<R, 160, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
+      break;
+    case 192: return go_rows<R, 192, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
   }
   em3d_set_last_error("no register FFT for this length");
   return EM3D_ERR_UNSUPPORTED;
@@ -698,7 +706,7 @@ static int launch_rows_fast(int L, const cx<R>* in, const cx<R>* chi, const cx<R
 template <typename R, int L, bool INV>
 static int go_strided(const cx<R>* in, cx<R>* out, const cx<R>* tw, int outer, int inner, const int* skip,
                       cudaStream_t st, BatchStrides bs) {
-  using G = StridedGeom<L, FastE<R>::E>;
+  using G = StridedGeom<L, FastE<R, L>::E>;
   auto kern = kf_strided<R, L, INV>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const int ntiles = (inner + G::P - 1) / G::P;
@@ -718,6 +726,11 @@ static int launch_strided_fast(int L, const cx<R>* in, cx<R>* out, const cx<R>* 
     case 128: return go_strided<R, 128, INV>(in, out, tw, outer, inner, skip, st, bs);
     case 256: return go_strided<R, 256, INV>(in, out, tw, outer, inner, skip, st, bs);
     case 512: return go_strided<R, 512, INV>(in, out, tw, outer, inner, skip, st, bs);
+    case 96: return go_strided<R, 96, INV>(in, out, tw, outer, inner, skip, st, bs);
+    case 160:
+      if constexpr (sizeof(R) == 4) return go_strided<R, 160, INV>(in, out, tw, outer, inner, skip, st, bs);
+      break;
+    case 192: return go_strided<R, 192, INV>(in, out, tw, outer, inner, skip, st, bs);
   }
   em3d_set_last_error("no register FFT for this length");
   return EM3D_ERR_UNSUPPORTED;
@@ -780,20 +793,45 @@ static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& 
 // in registers, 256-thread CTAs; 1 = the same with 128-thread CTAs (two per
 // SM); 2 = component-split threads (EM only); 3 = persistent CTAs with the
 // next tile's field and spectrum prefetched by cp.async, 256 threads; 4 = the
-// same with 128 threads.  -1 (the default) picks, per operator kind and
-// precision, the fastest measured on B200 at 128^3 (EM) / 256^3 (acoustic):
-// EM complex64 4, EM complex128 3, acoustic 0.
-static int xmul_variant(int C, bool fp64) {
+// same with 128 threads.  -1 (the default) picks, per operator kind,
+// precision and axis, the fastest measured on B200: EM complex64 4 on
+// power-of-two axes (128^3) and 3 on mixed ones (80^3, 96^3), EM complex128 3,
+// acoustic 0 (256^3).
+static int xmul_variant(int C, bool fp64, int L) {
   const int v = g_tuning[EM3D_TUNE_XPASS_VARIANT];
   if (v >= 0) return v;
-  return C == 3 ? (fp64 ? 3 : 4) : 0;
+  if (C != 3) return 0;
+  return fp64 || (L & (L - 1)) != 0 ? 3 : 4;
+}
+
+// Shared memory of each x-pass variant; a variant that does not fit in the
+// 227 KB a CTA may use (large mixed-radix plans in complex128) is replaced by
+// the first that fits in the order 4, 1, 2, 0, 3.
+constexpr size_t kSmemPerCta = 227 * 1024;
+
+template <typename R, int L, int C, int E>
+static size_t xvariant_smem(int v) {
+  switch (v) {
+    case 0: return (size_t)(L + XmulGeom<L, E, C, 256>::REGIONS * L * XmulGeom<L, E, C, 256>::S) * sizeof(cx<R>);
+    case 1: return (size_t)(L + XmulGeom<L, E, C, 128>::REGIONS * L * XmulGeom<L, E, C, 128>::S) * sizeof(cx<R>);
+    case 2: return C == 3 ? (size_t)(L + 3 * XsplitGeom<L, E>::REGION) * sizeof(cx<R>) : ~(size_t)0;
+    case 3: return (size_t)XpipeGeom<L, E, C, 256>::TOTAL * sizeof(cx<R>);
+    case 4: return (size_t)XpipeGeom<L, E, C, 128>::TOTAL * sizeof(cx<R>);
+  }
+  return ~(size_t)0;
 }
 
 template <typename R, int C, bool ADJ, int L>
 static int launch_xmul_len(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
                            const int* skip, cudaStream_t st, BatchStrides bs) {
-  constexpr int EB = FastE<R>::E;
-  const int v = xmul_variant(C, sizeof(R) == 8);
+  constexpr int EB = FastE<R, L>::E;
+  int v = xmul_variant(C, sizeof(R) == 8, L);
+  if (C == 1 && v == 2) v = 0;  // the component split is EM only
+  if (xvariant_smem<R, L, C, EB>(v) > kSmemPerCta) {
+    for (int alt : {4, 1, 2, 0, 3}) {
+      if (xvariant_smem<R, L, C, EB>(alt) <= kSmemPerCta) { v = alt; break; }
+    }
+  }
   if constexpr (C == 3) {
     if (v == 2) return go_xsplit<R, L, ADJ, EB>(T2, spec, tw, d, batch, skip, st, bs);
   }
@@ -812,6 +850,11 @@ static int launch_xmul_fast(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const
     case 128: return launch_xmul_len<R, C, ADJ, 128>(T2, spec, tw, d, batch, skip, st, bs);
     case 256: return launch_xmul_len<R, C, ADJ, 256>(T2, spec, tw, d, batch, skip, st, bs);
     case 512: return launch_xmul_len<R, C, ADJ, 512>(T2, spec, tw, d, batch, skip, st, bs);
+    case 96: return launch_xmul_len<R, C, ADJ, 96>(T2, spec, tw, d, batch, skip, st, bs);
+    case 160:
+      if constexpr (sizeof(R) == 4) return launch_xmul_len<R, C, ADJ, 160>(T2, spec, tw, d, batch, skip, st, bs);
+      break;
+    case 192: return launch_xmul_len<R, C, ADJ, 192>(T2, spec, tw, d, batch, skip, st, bs);
   }
   em3d_set_last_error("no register FFT for this length");
   return EM3D_ERR_UNSUPPORTED;
@@ -843,7 +886,8 @@ static int apply(const Dims& d, int batch, const void* spectrum, const void* chi
   const int nrows = batch * rows;
   int rc;
   const int Lz = 2 * d.nz, Ly = 2 * d.ny;
-  const bool fz = fast_len(Lz), fy = fast_len(Ly), fx = fast_len(2 * d.nx);
+  constexpr bool F64 = sizeof(R) == 8;
+  const bool fz = fast_len(Lz, F64), fy = fast_len(Ly, F64), fx = fast_len(2 * d.nx, F64);
   constexpr int LDF = C == 3 ? LD_EM_CHI : LD_AC_CHI;
   constexpr int FLDF = C == 3 ? FLD_EM_CHI : FLD_AC_CHI;
   constexpr int STA = C == 3 ? ST_EM_ADJ : ST_AC_ADJ;

@@ -1,4 +1,5 @@
-// Operator passes on the register-resident FFT (power-of-two axes 32..512).
+// Operator passes on the register-resident FFT (power-of-two axes 32..512,
+// and 96, 160, 192).
 // Same data layouts and fused work as the generic passes in operator.cu:
 //   kf_rows    pass 1 (z forward, chi applied on load) and pass 5 (z inverse,
 //              crop, u - y or v - chi^H y on store)
@@ -13,7 +14,11 @@ namespace em3d {
 enum { FLD_PLAIN = 0, FLD_EM_CHI = 1, FLD_AC_CHI = 2 };
 enum { FST_PLAIN = 0, FST_SUB = 1, FST_EM_ADJ = 2, FST_AC_ADJ = 3 };
 
-template <typename R> struct FastE { static constexpr int E = sizeof(R) == 4 ? 16 : 8; };
+// Elements per thread: power-of-two axes 16 (complex64) or 8 (complex128);
+// mixed axes 12 (3 x 2^k) or 20 (5 x 2^k).
+template <typename R, int L> struct FastE {
+  static constexpr int E = (L & (L - 1)) == 0 ? (sizeof(R) == 4 ? 16 : 8) : (L % 5 == 0 ? 20 : 12);
+};
 
 template <int L, int E, int C> struct RowsGeom {
   static constexpr int TT = L / E;
@@ -26,11 +31,11 @@ template <int L, int E, int C> struct RowsGeom {
 // output rows of length L.  Inverse: input rows of length L, output the
 // first L/2 (crop).  One thread handles one (component, row) pencil slice.
 template <typename R, int L, int C, int LD, int ST, bool INV>
-__global__ void __launch_bounds__(RowsGeom<L, FastE<R>::E, C>::NT)
+__global__ void __launch_bounds__(RowsGeom<L, FastE<R, L>::E, C>::NT)
 kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>* out,
         const cx<R>* __restrict__ twg, int rows_pb, int nrows, BatchStrides bs, const int* skip) {
   using T = cx<R>;
-  constexpr int E = FastE<R>::E;
+  constexpr int E = FastE<R, L>::E;
   using G = RowsGeom<L, E, C>;
   using P = RegPlan<L, E>;
   constexpr int TT = G::TT, RPB = G::RPB;
@@ -143,11 +148,11 @@ template <int L, int E> struct StridedGeom {
 
 // Pencils along y: in (outer, L/2 or L, inner) -> out (outer, L or L/2, inner).
 template <typename R, int L, bool INV>
-__global__ void __launch_bounds__(StridedGeom<L, FastE<R>::E>::NT)
+__global__ void __launch_bounds__(StridedGeom<L, FastE<R, L>::E>::NT)
 kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner, int ntiles, BatchStrides bs,
            const int* skip) {
   using T = cx<R>;
-  constexpr int E = FastE<R>::E;
+  constexpr int E = FastE<R, L>::E;
   using G = StridedGeom<L, E>;
   using PL = RegPlan<L, E>;
   constexpr int TT = G::TT, PP = G::P, S = G::S;

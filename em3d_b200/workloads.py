@@ -165,23 +165,19 @@ def multi_rhs_ellipsoid(N: int = 96, k0: float = 10.0, n_directions: int = 64, p
 
 def uneven_sphere_params(count: int = 48, seed: int = 0, sizes=(32, 48, 64, 80)) -> list:
     """A set of ``count`` independent single-sphere EM problems of uneven grid
-    sizes: N from ``sizes`` in turn, radius U[0.15, 0.3], eps_r U[1.5, 3.0] +
-    i U[0, 0.1], k0 U[4, 10], a unit propagation direction drawn uniformly and
-    a polarisation orthogonal to it.  Returns dicts (N, center, radius, eps,
-    k0, orient, amplitude)."""
+    sizes (L = 1, centred sphere): N drawn uniformly from ``sizes``, radius
+    U[0.15, 0.35], eps_r U[1.5, 4] + i U[0, 0.2], k0 U[2, 8], incident along
+    +z, x-polarised.  Returns dicts (N, center, radius, eps, k0, orient,
+    amplitude)."""
     rng = np.random.default_rng(seed)
     out = []
-    for i in range(count):
-        N = int(sizes[i % len(sizes)])
-        radius = float(rng.uniform(0.15, 0.3))
-        center = tuple(float(v) for v in rng.uniform(-0.1, 0.1, 3))
-        eps = complex(rng.uniform(1.5, 3.0), rng.uniform(0.0, 0.1))
-        k0 = float(rng.uniform(4.0, 10.0))
-        d = rng.normal(size=3)
-        d /= np.linalg.norm(d)
-        amp = orthogonal_polarisations(d)[0]
-        out.append(dict(N=N, center=center, radius=radius, eps=eps, k0=k0, orient=tuple(float(v) for v in d),
-                        amplitude=tuple(float(v) for v in amp)))
+    for _ in range(count):
+        N = int(rng.choice(np.asarray(sizes)))
+        radius = float(rng.uniform(0.15, 0.35))
+        eps = complex(rng.uniform(1.5, 4.0), rng.uniform(0.0, 0.2))
+        k0 = float(rng.uniform(2.0, 8.0))
+        out.append(dict(N=N, center=(0.0, 0.0, 0.0), radius=radius, eps=eps, k0=k0, orient=(0.0, 0.0, 1.0),
+                        amplitude=(1.0, 0.0, 0.0)))
     return out
 
 

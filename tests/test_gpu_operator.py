@@ -225,6 +225,64 @@ def test_register_fft_path_matches_generic_path(prec, kind, monkeypatch):
     del rng
 
 
+@pytest.mark.parametrize("prec", ["double", "single"])
+@pytest.mark.parametrize("kind", ["em", "acoustic"])
+def test_mixed_radix_register_path_matches_generic_path(prec, kind):
+    """Doubled axes 96 = 3 x 32, 160 = 5 x 32 and 192 = 3 x 64 on the register
+    FFT (radix 4, 6 / 10 / 12, 4), every x-pass variant, against the generic
+    passes (complex128 keeps 160 on the generic passes)."""
+    import torch
+    import em3d_b200 as e
+    from em3d_b200 import _lib, acoustics as ea
+    from em3d_b200.tune import set_xpass_variant
+
+    be = _be(prec)
+    tol = 1e-13 if prec == "double" else 3e-6
+    for N in ((48, 80, 96), (96, 48, 16), (80, 96, 48)):
+        grid = e.Grid(N=N, L=(1.0, 0.9, 1.1), center=(0.0, 0.0, 0.0), backend=be)
+        tc = be.precision.torch_complex
+        if kind == "em":
+            chi = (torch.randn((3, 3) + N, dtype=tc, device="cuda") * 0.3).contiguous()
+            u = torch.randn((3,) + N, dtype=tc, device="cuda")
+            op = e.Operator(e.Problem(grid=grid, eps_tensor=chi, wave=u, k0=7.0, volume=1.0))
+        else:
+            eta = (1.0 + torch.rand(N, dtype=tc, device="cuda")).contiguous()
+            op = ea.AcousticOperator(ea.make_acoustic_problem(grid, eta, k0=9.0))
+            u = torch.randn(N, dtype=tc, device="cuda")
+        _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 1)
+        gen_mv, gen_rmv = op.matvec(u), op.rmatvec(u)
+        _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 0)
+        try:
+            for v in (-1, 0, 1, 2, 3, 4):
+                set_xpass_variant(v)
+                fast_mv, fast_rmv = op.matvec(u), op.rmatvec(u)
+                assert rel_err(be.to_host(fast_mv), be.to_host(gen_mv)) < tol, (N, v)
+                assert rel_err(be.to_host(fast_rmv), be.to_host(gen_rmv)) < tol, (N, v)
+        finally:
+            set_xpass_variant(-1)
+
+
+def test_em_matvec_oracle_on_mixed_radix_axes():
+    """Doubled axes 96, 32 and 160 against the oracle: complex128 to 1e-12,
+    complex64 to 1e-5."""
+    import em3d_b200 as e
+    from oracle import em as oem
+
+    N, L, k = (48, 16, 80), (1.0, 0.5, 1.2), 9.0
+    rng = np.random.default_rng(11)
+    chi = (rng.standard_normal((3, 3) + N) + 1j * rng.standard_normal((3, 3) + N)) * 0.2
+    u = rng.standard_normal((3,) + N) + 1j * rng.standard_normal((3,) + N)
+    kh = oem.kernel_hat(N, L, k)
+    ref, ref_a = oem.matvec(chi, u, kh, N), oem.rmatvec(chi, u, N, khat=kh)
+    for prec, tol in (("double", 1e-12), ("single", 1e-5)):
+        be = _be(prec)
+        cdt = be.complex_dtype
+        grid = e.Grid(N=N, L=L, center=(0.0, 0.0, 0.0), backend=be)
+        op = e.Operator(e.Problem(grid=grid, eps_tensor=chi.astype(cdt), wave=u.astype(cdt), k0=k, volume=1.0))
+        assert rel_err(be.to_host(op.matvec(u.astype(cdt))), ref) < tol, prec
+        assert rel_err(be.to_host(op.rmatvec(u.astype(cdt))), ref_a) < tol, prec
+
+
 def test_em_matvec_oracle_at_32_cubed_both_paths(monkeypatch):
     """Register path and generic path both against the oracle (FP64, 1e-12)."""
     import em3d_b200 as e
