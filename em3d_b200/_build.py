@@ -14,7 +14,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr",
 ]
 
@@ -31,22 +31,41 @@ def needs_build() -> bool:
     return any(os.path.getmtime(p) > t for p in deps)
 
 
+def _run(cmd):
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"nvcc failed ({proc.returncode}): {' '.join(cmd)}\n{proc.stdout}\n{proc.stderr}")
+    return proc.stderr
+
+
 def build(verbose: bool = False, force: bool = False) -> str:
-    """Compile every ``csrc/*.cu`` into one shared library; returns its path."""
+    """Compile every ``csrc/*.cu`` (one object each, in parallel) and link them
+    into one shared library; returns its path."""
+    from concurrent.futures import ThreadPoolExecutor
+
     if not force and not needs_build():
         return LIB
     os.makedirs(NATIVE, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    tmp = LIB + ".tmp"
-    cmd = [nvcc, *NVCC_FLAGS, "-I", INCLUDE, *sources(), "-o", tmp]
+    objdir = os.path.join(NATIVE, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    jobs = []
+    for src in sources():
+        obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
+        cmd = [nvcc, *NVCC_FLAGS, "-I", INCLUDE, "-c", src, "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        jobs.append((cmd, obj))
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(workers) as pool:
+        logs = list(pool.map(lambda j: _run(j[0]), jobs))
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    proc = subprocess.run(cmd, capture_output=True, text=True)
-    if proc.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({proc.returncode}):\n{proc.stdout}\n{proc.stderr}")
-    if verbose and proc.stderr:
-        print(proc.stderr)
+        for (cmd, _), log in zip(jobs, logs):
+            print(" ".join(cmd))
+            if log:
+                print(log)
+    tmp = LIB + ".tmp"
+    _run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *[o for _, o in jobs]])
     os.replace(tmp, LIB)
     return LIB
 
