@@ -789,15 +789,13 @@ static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& 
 // in registers, 256-thread CTAs; 1 = the same with 128-thread CTAs (two per
 // SM); 2 = component-split threads (EM only); 3 = persistent CTAs with the
 // next tile's field and spectrum prefetched by cp.async, 256 threads; 4 = the
-// same with 128 threads.  -1 (the default) picks, per operator kind,
-// precision and axis, the fastest measured on B200: EM complex64 4 on
-// power-of-two axes (128^3) and 3 on mixed ones (80^3, 96^3), EM complex128 3,
+// same with 128 threads.  -1 (the default) picks, per operator kind, the
+// fastest measured on B200: EM 4 (both precisions; 128^3, 96^3, 80^3),
 // acoustic 0 (256^3).
-static int xmul_variant(int C, bool fp64, int L) {
+static int xmul_variant(int C) {
   const int v = g_tuning[EM3D_TUNE_XPASS_VARIANT];
   if (v >= 0) return v;
-  if (C != 3) return 0;
-  return fp64 || (L & (L - 1)) != 0 ? 3 : 4;
+  return C == 3 ? 4 : 0;
 }
 
 // Shared memory of each x-pass variant; a variant that does not fit in the
@@ -821,7 +819,7 @@ template <typename R, int C, bool ADJ, int L>
 static int launch_xmul_len(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
                            const int* skip, cudaStream_t st, BatchStrides bs) {
   constexpr int EB = FastE<R, L>::E;
-  int v = xmul_variant(C, sizeof(R) == 8, L);
+  int v = xmul_variant(C);
   if (C == 1 && v == 2) v = 0;  // the component split is EM only
   if (xvariant_smem<R, L, C, EB>(v) > kSmemPerCta) {
     for (int alt : {4, 1, 2, 0, 3}) {

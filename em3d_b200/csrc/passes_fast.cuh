@@ -207,8 +207,8 @@ template <int L, int E, int C, int NTT = 256> struct XmulGeom {
   static constexpr int REGIONS = SEQ ? 1 : C;
 };
 
-template <int L, int E, int R, int NSV, int RN, int C, typename T>
-__device__ __forceinline__ void reg_exchange_seq(T (&a)[C][E], int t, T* sm, const LayInter& lay) {
+template <int L, int E, int R, int NSV, int RN, int C, typename T, class Lay>
+__device__ __forceinline__ void reg_exchange_seq(T (&a)[C][E], int t, T* sm, const Lay& lay) {
   constexpr int TT = L / E;
 #pragma unroll
   for (int c = 0; c < C; ++c) {
@@ -231,8 +231,8 @@ __device__ __forceinline__ void reg_exchange_seq(T (&a)[C][E], int t, T* sm, con
 }
 
 template <int L, int E, bool INV, bool REV, int S, bool HALF_IN> struct RegFFTSeq {
-  template <int C, typename T>
-  __device__ __forceinline__ static void run(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const LayInter& lay) {
+  template <int C, typename T, class Lay>
+  __device__ __forceinline__ static void run(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const Lay& lay) {
     using P = RegPlan<L, E>;
     constexpr int R = P::rad(REV, S);
     constexpr int NSV = P::nsb(REV, S);
@@ -245,8 +245,8 @@ template <int L, int E, bool INV, bool REV, int S, bool HALF_IN> struct RegFFTSe
   }
 };
 
-template <int L, int E, bool INV, bool REV, bool SEQ, int C, typename T>
-__device__ __forceinline__ void reg_fft_x(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const LayInter& lay) {
+template <int L, int E, bool INV, bool REV, bool SEQ, int C, typename T, class Lay>
+__device__ __forceinline__ void reg_fft_x(T (&a)[C][E], int t, T* sm, const T* __restrict__ tw, const Lay& lay) {
   if constexpr (SEQ) RegFFTSeq<L, E, INV, REV, 0, !INV>::template run<C>(a, t, sm, tw, lay);
   else reg_fft<L, E, INV, REV, C, !INV>(a, t, sm, tw, lay);
 }
@@ -375,6 +375,16 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
+// Exchange layout of the pipelined x pass: element pos of pencil p at
+// pos * P + p + 2 (pos / 4).  The shift by two words every four positions
+// spreads both the stage-output stores (stride R positions per thread) and
+// the next stage's loads over distinct banks for the 8-pencil tiles (a plain
+// odd stride P + 1 gives them two-way conflicts there).
+template <int P> struct LayPipe {
+  int p;
+  __device__ __forceinline__ int operator()(int c, int pos) const { return pos * P + p + 2 * (pos >> 2); }
+};
+
 template <int L, int E, int C, int NTT> struct XpipeGeom {
   static constexpr int TT = L / E;
   static constexpr int P = (NTT / TT) > 32 ? 32 : ((NTT / TT) >= 2 ? (NTT / TT) : 2);
@@ -383,7 +393,7 @@ template <int L, int E, int C, int NTT> struct XpipeGeom {
   static constexpr int NX = L / 2;
   static constexpr int NSPEC = C == 3 ? 6 : 1;
   static constexpr int TW = L;
-  static constexpr int EXCH = L * S;
+  static constexpr int EXCH = L * P + L / 2;   // LayPipe
   static constexpr int FIELD = C * NX * P;
   static constexpr int SPEC = NSPEC * (NX + 1) * P;
   static constexpr int TOTAL = TW + EXCH + FIELD + SPEC;   // complex elements of shared memory
@@ -396,7 +406,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   using T = cx<R>;
   using G = XpipeGeom<L, E, C, NTT>;
   using PL = RegPlan<L, E>;
-  constexpr int TT = G::TT, PP = G::P, S = G::S, NX = G::NX, NSP = G::NSPEC;
+  constexpr int TT = G::TT, PP = G::P, NX = G::NX, NSP = G::NSPEC;
   constexpr int R1 = PL::first(false), RL = PL::last(false);
   constexpr int M1 = L / R1, ML = L / RL;
   constexpr int EB = (int)sizeof(T);
@@ -460,7 +470,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   cp_async_commit();
   if (tile0 < ntiles) issue_spec(tile0);
   cp_async_commit();
-  const LayInter lay{p, S, 0};
+  const LayPipe<PP> lay{p};
 
   for (int tile = tile0; tile < ntiles; tile += gridDim.x) {
     int b, ky, kz0;

@@ -56,8 +56,7 @@ const char* em3d_last_error(void);
  * in the reference, which has no native code to tune.
  * ------------------------------------------------------------------------ */
 enum em3d_tune_key {
-  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: EM complex64 4 on power-of-two axes and 3 on
-                                   96/160/192, complex128 3, acoustic 0), 0 register 256-thread, 1 register
+  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: EM 4, acoustic 0), 0 register 256-thread, 1 register
                                    128-thread, 2 component-split, 3 persistent cp.async-pipelined 256-thread,
                                    4 the same 128-thread; a variant whose shared memory does not fit is
                                    replaced by the first that fits in the order 4, 1, 2, 0, 3 */
