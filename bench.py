@@ -330,6 +330,11 @@ def run_ours(args, world, rank, local):
         fp64(i)
     for w in range(max(args.warmup, 1)):
         mixed_nn(w % K)
+    # the timed legs keep their results until the end of the run; one untimed
+    # pass of each leg with its results held leaves those blocks in the
+    # allocator's cache, so no timed step waits on cudaMalloc
+    held = [[fn(s % K) for s in range(args.steps)] for fn in (mixed_nn, fp64, mixed_zero)]
+    del held
 
     def timed(fn):
         barrier(world)
@@ -422,18 +427,23 @@ def run_ours(args, world, rank, local):
         for j, pol in enumerate(workloads.orthogonal_polarisations(d3)):
             builders.plane_wave(g3, k=c3.k0, orient=tuple(d3), amplitude=tuple(pol), out=waves3[2 * i + j])
     chunk = 32
-    mxb = MixedBiCGStab(cfg)
-    mxb.solve_batch(o64, waves3[:chunk], operator_low=o32)
-    batch_ms, resb = _events_ms(lambda: [r for c0 in range(0, 128, chunk)
-                                         for r in mxb.solve_batch(o64, waves3[c0:c0 + chunk], operator_low=o32)])
-    mx3 = MixedBiCGStab(cfg)
-    mx3.solve(o64, waves3[0], operator_low=o32)
     n_single = 16
-    single_ms, ress = _events_ms(lambda: [mx3.solve(o64, waves3[i], operator_low=o32) for i in range(n_single)])
-    dcb = DefectCorrection(cfg)
-    dcb.solve_batch(o64, waves3[:chunk], operator_low=o32)
-    dc_ms, resd = _events_ms(lambda: [r for c0 in range(0, 128, chunk)
-                                      for r in dcb.solve_batch(o64, waves3[c0:c0 + chunk], operator_low=o32)])
+    mxb, mx3, dcb = MixedBiCGStab(cfg), MixedBiCGStab(cfg), DefectCorrection(cfg)
+
+    def batched(solver):
+        return [r for c0 in range(0, 128, chunk)
+                for r in solver.solve_batch(o64, waves3[c0:c0 + chunk], operator_low=o32)]
+
+    def singles():
+        return [mx3.solve(o64, waves3[i], operator_low=o32) for i in range(n_single)]
+
+    # each leg runs once untimed first: engines, graphs and the result buffers
+    # (held until the leg ends) come from the allocator's cache when timed
+    for leg in (lambda: batched(mxb), singles, lambda: batched(dcb)):
+        leg()
+    batch_ms, resb = _events_ms(lambda: batched(mxb))
+    single_ms, ress = _events_ms(singles)
+    dc_ms, resd = _events_ms(lambda: batched(dcb))
     multi_rhs = {"workload": "em_aniso_ellipsoid_96^3_k10_128_rhs", "rhs": 128, "batch": chunk,
                  "solver": "MixedBiCGStab (FP32 BiCGStab, FP64 reliable updates) batched vs one right-hand side "
                            "at a time",
