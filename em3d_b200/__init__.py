@@ -13,7 +13,7 @@ from .backend import Backend, Precision
 from .problem import (AxisAlignedBox, Ellipsoid, FullDomain, Grid, Problem, cylinder_refraction,
                       ellipsis_refraction, flat_wave_vec, sample_contrast_tensor)
 from .operator import Operator, PreparedEMKernel, prep_coeffs_em3d, prep_conj_coeffs_em3d
-from . import acoustics
+from . import acoustics, gamma0
 
 __version__ = "0.1.0"
 REFERENCE_VERSION = "0.8.0"
@@ -21,5 +21,5 @@ REFERENCE_VERSION = "0.8.0"
 __all__ = [
     "Backend", "Precision", "Grid", "Problem", "Operator", "PreparedEMKernel", "prep_coeffs_em3d",
     "prep_conj_coeffs_em3d", "flat_wave_vec", "sample_contrast_tensor", "cylinder_refraction",
-    "ellipsis_refraction", "Ellipsoid", "AxisAlignedBox", "FullDomain", "acoustics",
+    "ellipsis_refraction", "Ellipsoid", "AxisAlignedBox", "FullDomain", "acoustics", "gamma0",
 ]
