@@ -37,7 +37,7 @@ from .fno import FNO
 from .operator import Operator
 from .problem import Grid, Problem
 from .scenes import EllipsoidShape, plane_wave, sample_scene
-from .solvers import BiCGStab, DefectCorrection, SolverConfig, true_relative_residual
+from .solvers import BiCGStab, MixedBiCGStab, SolverConfig, true_relative_residual
 from .workloads import orthogonal_polarisations
 
 TRAIN_SEEDS = range(0, 4000)
@@ -230,9 +230,10 @@ def _timed(fn, reps: int):
 
 def evaluate(net: FNO, seeds: Sequence[int], N: int, *, rtol: float = 1e-6, max_iter: int = 4000,
              reps: int = 2, device_index: int = 0, log_every: int = 0) -> List[EvalRecord]:
-    """Per held-out scene: FP64 BiCGStab and mixed defect correction, each from
-    the zero guess and from the network's guess, to a TRUE relative residual of
-    ``rtol``; ``reps`` runs per solve, the last one timed (graphs captured)."""
+    """Per held-out scene: FP64 BiCGStab and the mixed solve (FP32 BiCGStab with
+    FP64 reliable updates, ``MixedBiCGStab``), each from the zero guess and from
+    the network's guess, to a TRUE relative residual of ``rtol``; ``reps`` runs
+    per solve, the last one timed (graphs captured)."""
     import torch
 
     grid = unit_grid(N, Precision.DOUBLE, device_index)
@@ -248,7 +249,7 @@ def evaluate(net: FNO, seeds: Sequence[int], N: int, *, rtol: float = 1e-6, max_
         cfg = SolverConfig(max_iter=max_iter, rtol=rtol)
         runs = {}
         bic = BiCGStab(cfg)
-        dc = DefectCorrection(SolverConfig(max_iter=max_iter, rtol=rtol))
+        dc = MixedBiCGStab(SolverConfig(max_iter=max_iter, rtol=rtol))
         plans = {
             "fp64_zero": lambda: bic.solve(op64, f),
             "fp64_nn": lambda: bic.solve(op64, f, x0=u_nn),
