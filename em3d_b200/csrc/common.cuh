@@ -45,13 +45,14 @@ template <> __host__ __device__ __forceinline__ double2 from_c64<double>(double2
 // one operator; non-zero for a group of operators of one grid).  done
 // (nullable): entry b's stop flag at done + b * done_stride bytes (non-zero =
 // that entry's solve has stopped, its work is skipped); outer: pencil groups
-// per entry in the strided passes (C * Nx).
+// per entry in the strided passes (C * Nx); status: see the field.
 struct BatchStrides {
   size_t chi;
   size_t spec;
   const char* done;
   size_t done_stride;
   int outer;
+  int* status;  // this application's status words (bounded waits that gave up), or null
 };
 
 __device__ __forceinline__ bool entry_done(const BatchStrides& bs, int b) {

@@ -66,10 +66,16 @@ static size_t build_ws_bytes(const Dims& d) {
   return align_up(d.doubled() * sizeof(double2)) + align_up((size_t)2 * (d.nx + d.ny + d.nz) * sizeof(double2));
 }
 
-template <typename R> static size_t apply_ws_bytes(const Dims& d, int C, int batch) {
+// Apply workspace: T1, T2, then 256 bytes of status words (word 0 counts the
+// bounded waits that gave up; zero the workspace once after allocating it).
+constexpr size_t kStatusBytes = 256;
+template <typename R> static size_t apply_status_offset(const Dims& d, int C, int batch) {
   size_t t1 = (size_t)batch * C * d.nx * d.ny * 2 * d.nz;
   size_t t2 = (size_t)batch * C * d.nx * 2 * d.ny * 2 * d.nz;
   return align_up(t1 * sizeof(cx<R>)) + align_up(t2 * sizeof(cx<R>));
+}
+template <typename R> static size_t apply_ws_bytes(const Dims& d, int C, int batch) {
+  return apply_status_offset<R>(d, C, batch) + kStatusBytes;
 }
 
 // ---------------------------------------------------------------------------
@@ -746,13 +752,13 @@ static int go_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d,
   return EM3D_OK;
 }
 
-template <typename R, int L, int C, bool ADJ, int E, int NTT>
+template <typename R, int L, int C, bool ADJ, int E, int NTT, bool TMAF>
 static int go_xpipe(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
                     cudaStream_t st, BatchStrides bs) {
   using G = XpipeGeom<L, E, C, NTT>;
-  auto kern = kf_xmul_pipe<R, L, C, ADJ, E, NTT>;
+  auto kern = kf_xmul_pipe<R, L, C, ADJ, E, NTT, TMAF>;
   EM3D_CUDA_TRY(allow_smem(kern));
-  const size_t smem = (size_t)G::TOTAL * sizeof(cx<R>);
+  const size_t smem = (size_t)G::TOTAL * sizeof(cx<R>) + G::BYTES_EXTRA;
   const int ntz = (2 * d.nz + G::P - 1) / G::P;
   const long long ntiles = (long long)batch * 2 * d.ny * ntz;
   static int sms = 0;
@@ -766,7 +772,28 @@ static int go_xpipe(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d
   if (per_sm < 1) per_sm = 1;
   const long long grid = std::min<long long>(ntiles, (long long)sms * per_sm);
   if (grid <= 0) return EM3D_OK;
-  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, bs, skip);
+  CUtensorMap fmap;
+  memset(&fmap, 0, sizeof fmap);
+  if constexpr (TMAF) {
+    // T2 as 8-byte words: (2 Nz * W, 2 Ny, batch * C * Nx), one box of
+    // P * W words x 1 x Nx per component and tile.  The row strides are
+    // multiples of 16 bytes, the box's inner extent is P * 8 or P * 16 bytes
+    // and every tile starts at kz0 = a multiple of P (even), so each load
+    // starts on a 16-byte boundary.
+    static_assert(G::P % 2 == 0 && L / 2 <= 256, "TMA field slab: even tile width, at most 256 rows per box");
+    auto enc = tensor_map_encoder();
+    if (enc == nullptr) { em3d_set_last_error("cuTensorMapEncodeTiled is unavailable"); return EM3D_ERR_CUDA; }
+    constexpr cuuint64_t W = sizeof(cx<R>) / 8;
+    const cuuint64_t dims[3] = {(cuuint64_t)2 * d.nz * W, (cuuint64_t)2 * d.ny, (cuuint64_t)batch * C * d.nx};
+    const cuuint64_t strides[2] = {(cuuint64_t)2 * d.nz * sizeof(cx<R>), (cuuint64_t)4 * d.ny * d.nz * sizeof(cx<R>)};
+    const cuuint32_t box[3] = {(cuuint32_t)(G::P * W), 1u, (cuuint32_t)d.nx};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    const CUresult r = enc(&fmap, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, (void*)T2, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) { em3d_set_last_error("cuTensorMapEncodeTiled rejected the field slab map"); return EM3D_ERR_CUDA; }
+  }
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, bs, skip, fmap, bs.status);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
@@ -789,18 +816,19 @@ static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& 
 // in registers, 256-thread CTAs; 1 = the same with 128-thread CTAs (two per
 // SM); 2 = component-split threads (EM only); 3 = persistent CTAs with the
 // next tile's field and spectrum prefetched by cp.async, 256 threads; 4 = the
-// same with 128 threads.  -1 (the default) picks, per operator kind, the
-// fastest measured on B200: EM 4 (both precisions; 128^3, 96^3, 80^3),
+// same with 128 threads; 5 and 6 = 3 and 4 with the field slab loaded by TMA.
+// -1 (the default) picks, per operator kind, the
+// fastest measured on B200: EM 6 (both precisions; 128^3, 96^3, 80^3),
 // acoustic 0 (256^3).
 static int xmul_variant(int C) {
   const int v = g_tuning[EM3D_TUNE_XPASS_VARIANT];
   if (v >= 0) return v;
-  return C == 3 ? 4 : 0;
+  return C == 3 ? 6 : 0;
 }
 
 // Shared memory of each x-pass variant; a variant that does not fit in the
 // 227 KB a CTA may use (large mixed-radix plans in complex128) is replaced by
-// the first that fits in the order 4, 1, 2, 0, 3.
+// the first that fits in the order 6, 4, 1, 2, 0, 5, 3.
 constexpr size_t kSmemPerCta = 227 * 1024;
 
 template <typename R, int L, int C, int E>
@@ -809,8 +837,8 @@ static size_t xvariant_smem(int v) {
     case 0: return (size_t)(L + XmulGeom<L, E, C, 256>::REGIONS * L * XmulGeom<L, E, C, 256>::S) * sizeof(cx<R>);
     case 1: return (size_t)(L + XmulGeom<L, E, C, 128>::REGIONS * L * XmulGeom<L, E, C, 128>::S) * sizeof(cx<R>);
     case 2: return C == 3 ? (size_t)(L + 3 * XsplitGeom<L, E>::REGION) * sizeof(cx<R>) : ~(size_t)0;
-    case 3: return (size_t)XpipeGeom<L, E, C, 256>::TOTAL * sizeof(cx<R>);
-    case 4: return (size_t)XpipeGeom<L, E, C, 128>::TOTAL * sizeof(cx<R>);
+    case 3: case 5: return (size_t)XpipeGeom<L, E, C, 256>::TOTAL * sizeof(cx<R>) + 16;
+    case 4: case 6: return (size_t)XpipeGeom<L, E, C, 128>::TOTAL * sizeof(cx<R>) + 16;
   }
   return ~(size_t)0;
 }
@@ -822,15 +850,17 @@ static int launch_xmul_len(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const 
   int v = xmul_variant(C);
   if (C == 1 && v == 2) v = 0;  // the component split is EM only
   if (xvariant_smem<R, L, C, EB>(v) > kSmemPerCta) {
-    for (int alt : {4, 1, 2, 0, 3}) {
+    for (int alt : {6, 4, 1, 2, 0, 5, 3}) {
       if (xvariant_smem<R, L, C, EB>(alt) <= kSmemPerCta) { v = alt; break; }
     }
   }
   if constexpr (C == 3) {
     if (v == 2) return go_xsplit<R, L, ADJ, EB>(T2, spec, tw, d, batch, skip, st, bs);
   }
-  if (v == 3) return go_xpipe<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st, bs);
-  if (v == 4) return go_xpipe<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st, bs);
+  if (v == 3) return go_xpipe<R, L, C, ADJ, EB, 256, false>(T2, spec, tw, d, batch, skip, st, bs);
+  if (v == 4) return go_xpipe<R, L, C, ADJ, EB, 128, false>(T2, spec, tw, d, batch, skip, st, bs);
+  if (v == 5) return go_xpipe<R, L, C, ADJ, EB, 256, true>(T2, spec, tw, d, batch, skip, st, bs);
+  if (v == 6) return go_xpipe<R, L, C, ADJ, EB, 128, true>(T2, spec, tw, d, batch, skip, st, bs);
   if (v == 1) return go_xmul<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st, bs);
   return go_xmul<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st, bs);
 }
@@ -865,6 +895,7 @@ int apply(const Dims& d, int batch, const void* spectrum, const void* chi, const
   if (out == u) { em3d_set_last_error("out must not alias the input field"); return EM3D_ERR_INVALID; }
   using T = cx<R>;
   bs.outer = C * d.nx;
+  bs.status = (int*)((char*)ws + apply_status_offset<R>(d, C, batch));
   SpecLayout<R> lay(d, C == 3 ? EM3D_EM : EM3D_ACOUSTIC);
   void* sp = const_cast<void*>(spectrum);
   const T* twx = lay.twx(sp, d);

@@ -8,6 +8,7 @@
 #pragma once
 
 #include "fft_reg.cuh"
+#include "tma.cuh"
 
 namespace em3d {
 
@@ -397,12 +398,16 @@ template <int L, int E, int C, int NTT> struct XpipeGeom {
   static constexpr int FIELD = C * NX * P;
   static constexpr int SPEC = NSPEC * (NX + 1) * P;
   static constexpr int TOTAL = TW + EXCH + FIELD + SPEC;   // complex elements of shared memory
+  static constexpr size_t BYTES_EXTRA = 16;                  // the TMA mbarrier after the slabs
 };
 
-template <typename R, int L, int C, bool ADJ, int E, int NTT>
+// TMAF: the field slab arrives by TMA (one tile load per component, issued by
+// thread 0 and completed on an mbarrier; `fmap` describes T2 as (kz words,
+// ky, batch * C * Nx rows)) instead of per-thread cp.async copies.
+template <typename R, int L, int C, bool ADJ, int E, int NTT, bool TMAF>
 __global__ void __launch_bounds__(XpipeGeom<L, E, C, NTT>::NT)
 kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
-             int nb, BatchStrides bs, const int* skip) {
+             int nb, BatchStrides bs, const int* skip, const __grid_constant__ CUtensorMap fmap, int* status) {
   using T = cx<R>;
   using G = XpipeGeom<L, E, C, NTT>;
   using PL = RegPlan<L, E>;
@@ -411,12 +416,22 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   constexpr int M1 = L / R1, ML = L / RL;
   constexpr int EB = (int)sizeof(T);
   if (skip_launch(skip)) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* tw = reinterpret_cast<T*>(smem_raw);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // the field slab first: TMA writes it at a 128-byte aligned address
+  T* sfield = reinterpret_cast<T*>(smem_raw);
+  T* tw = sfield + G::FIELD;
   T* sm = tw + G::TW;
-  T* sfield = sm + G::EXCH;
-  T* sspec = sfield + G::FIELD;
+  T* sspec = sm + G::EXCH;
+  uint64_t* fbar = reinterpret_cast<uint64_t*>(sspec + G::SPEC);
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
+  if constexpr (TMAF) {
+    if (threadIdx.x == 0) {
+      mbar_init(fbar, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
+  uint32_t fphase = 0;
   const int p = threadIdx.x % PP, t = threadIdx.x / PP;
   const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
   const size_t xstride = (size_t)Ny2 * Nz2;
@@ -437,6 +452,17 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     int b, ky, kz0;
     decode(tile, b, ky, kz0);
     if (entry_done(bs, b)) return;
+    if constexpr (TMAF) {
+      // kz words of 8 bytes: one per complex64, two per complex128; rows
+      // past Nz2 (the last tile) are filled with zeros by the TMA unit
+      constexpr int W = EB / 8;
+      if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(fbar, (uint32_t)(C * NX * PP * EB));
+#pragma unroll
+        for (int c = 0; c < C; ++c) tma_load_3d(sfield + c * NX * PP, &fmap, fbar, kz0 * W, ky, (b * C + c) * NX);
+      }
+      return;
+    }
     const bool ok = kz0 + p < Nz2;
     int row = threadIdx.x / PP;                       // c * NX + x
     const T* src = T2 + (size_t)b * C * NX * xstride + (size_t)ky * Nz2 + kz0 + p + (size_t)row * xstride;
@@ -483,6 +509,12 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
 
     cp_async_wait_one();  // this tile's field slab
     __syncthreads();
+    if constexpr (TMAF) {
+      if (live) {
+        mbar_wait_bounded(fbar, fphase, status);
+        fphase ^= 1u;
+      }
+    }
     T a[C][E];
 #pragma unroll
     for (int q = 0; q < E / R1; ++q) {
@@ -494,6 +526,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
         for (int c = 0; c < C; ++c) a[c][q * R1 + r] = r < R1 / 2 ? sfield[(c * NX + x) * PP + p] : mk<R>(0, 0);
       }
     }
+    if constexpr (TMAF) fence_proxy_async_smem();  // these reads before the next tile's TMA overwrite
     __syncthreads();
     if (next < ntiles) issue_field(next);
     cp_async_commit();

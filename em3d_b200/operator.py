@@ -172,7 +172,7 @@ class _Applier:
             nb = _lib.load().em3d_apply_workspace_bytes(ctypes_ref(self._grid_c), self._kind, self._dt, int(batch))
             if nb == 0:
                 _lib.check(_lib.EM3D_ERR_INVALID, "em3d_apply_workspace_bytes")
-            ws = _uint8(nb, self._be.torch_device)
+            ws = _uint8(nb, self._be.torch_device).zero_()  # the status words at its end start at zero
             self._workspaces[batch] = ws
         return ws
 

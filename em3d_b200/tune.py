@@ -20,7 +20,7 @@ def get_xpass_variant() -> int:
     return int(_lib.load().em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT))
 
 
-def autotune(op, *, reps: int = 10, variants=(0, 1, 2, 3, 4)) -> dict:
+def autotune(op, *, reps: int = 10, variants=(0, 1, 2, 3, 4, 5, 6)) -> dict:
     """Time every x-pass variant on ``op`` (an ``Operator`` or
     ``AcousticOperator``) and select the fastest.  Returns {variant: ms}."""
     import torch

@@ -56,10 +56,11 @@ const char* em3d_last_error(void);
  * in the reference, which has no native code to tune.
  * ------------------------------------------------------------------------ */
 enum em3d_tune_key {
-  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: EM 4, acoustic 0), 0 register 256-thread, 1 register
+  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: EM 6, acoustic 0), 0 register 256-thread, 1 register
                                    128-thread, 2 component-split, 3 persistent cp.async-pipelined 256-thread,
-                                   4 the same 128-thread; a variant whose shared memory does not fit is
-                                   replaced by the first that fits in the order 4, 1, 2, 0, 3 */
+                                   4 the same 128-thread, 5 and 6 = 3 and 4 with the field slab loaded by
+                                   TMA; a variant whose shared memory does not fit is
+                                   replaced by the first that fits in the order 6, 4, 1, 2, 0, 5, 3 */
   EM3D_TUNE_FFT_GENERIC = 1,   /* 1 = use the generic shared-memory FFT passes for every axis length */
   EM3D_TUNE_FNO_SIMT = 2,      /* 1 = FNO row pass on CUDA cores even where the tensor-core one applies */
   EM3D_TUNE_COUNT = 3,
@@ -82,7 +83,11 @@ size_t em3d_spectrum_bytes(const em3d_grid* g, int kind, int dtype);
 /* FP64 scratch needed by the spectrum builders (two doubled-grid blocks). */
 size_t em3d_build_workspace_bytes(const em3d_grid* g);
 
-/* Scratch needed by one matvec / rmatvec over `batch` right-hand sides. */
+/* Scratch needed by one matvec / rmatvec over `batch` right-hand sides.  Its
+ * last 256 bytes are status words: the int at the start of them counts the
+ * bounded waits inside the passes that gave up (a transfer that never
+ * completed; the result is then wrong).  Zero the workspace once after
+ * allocating it; the library only ever adds to that count. */
 size_t em3d_apply_workspace_bytes(const em3d_grid* g, int kind, int dtype, int batch);
 
 /* ------------------------------------------------------------------------

@@ -101,8 +101,8 @@ def test_tuning_keys_validate_without_gpu():
 
     lib = _lib.load()
     assert lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT) == -1   # automatic by default
-    assert lib.em3d_set_tuning(_lib.EM3D_TUNE_XPASS_VARIANT, 5) == _lib.EM3D_ERR_INVALID
+    assert lib.em3d_set_tuning(_lib.EM3D_TUNE_XPASS_VARIANT, 7) == _lib.EM3D_ERR_INVALID
     assert "variant" in _lib.last_error()
-    for v in (3, 4, 0, -1):
+    for v in (5, 6, 3, 4, 0, -1):
         assert lib.em3d_set_tuning(_lib.EM3D_TUNE_XPASS_VARIANT, v) == 0
         assert lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT) == v

@@ -121,7 +121,7 @@ def test_grouped_defect_correction_reaches_fp64_residuals():
     assert group.true_relative_residuals(u, group.waves()).max() < 1e-10
 
 
-@pytest.mark.parametrize("variant", [-1, 0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [-1, 0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("prec", ["double", "single"])
 def test_stopped_entries_are_left_untouched(variant, prec):
     import torch

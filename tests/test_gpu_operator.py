@@ -216,7 +216,7 @@ def test_register_fft_path_matches_generic_path(prec, kind, monkeypatch):
         _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 1)
         gen_mv, gen_rmv = op.matvec(u), op.rmatvec(u)
         _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 0)
-        for v in (0, 1, 2, 3, 4):
+        for v in (0, 1, 2, 3, 4, 5, 6):
             set_xpass_variant(v)
             fast_mv, fast_rmv = op.matvec(u), op.rmatvec(u)
             assert rel_err(be.to_host(fast_mv), be.to_host(gen_mv)) < tol, (N, v)
@@ -253,7 +253,7 @@ def test_mixed_radix_register_path_matches_generic_path(prec, kind):
         gen_mv, gen_rmv = op.matvec(u), op.rmatvec(u)
         _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 0)
         try:
-            for v in (-1, 0, 1, 2, 3, 4):
+            for v in (-1, 0, 1, 2, 3, 4, 5, 6):
                 set_xpass_variant(v)
                 fast_mv, fast_rmv = op.matvec(u), op.rmatvec(u)
                 assert rel_err(be.to_host(fast_mv), be.to_host(gen_mv)) < tol, (N, v)
@@ -339,3 +339,33 @@ def test_batched_matvec_equals_single_register_path(N, prec):
     Z = aop.matvec(V)
     for b in range(5):
         assert rel_err(be.to_host(Z[b]), be.to_host(aop.matvec(V[b]))) < tol, b
+
+
+@pytest.mark.parametrize("prec", ["double", "single"])
+def test_tma_field_slab_completes(prec):
+    """The TMA-fed x-pass variants (5, 6) give the cp.async variants' result
+    and no bounded wait gives up (the status word at the end of the apply
+    workspace stays zero)."""
+    import torch
+    import em3d_b200 as e
+    from em3d_b200.tune import set_xpass_variant
+
+    be = _be(prec)
+    tol = 1e-13 if prec == "double" else 3e-6
+    for N in ((32, 16, 64), (64, 64, 64), (48, 96, 32)):
+        grid = e.Grid(N=N, L=(1.0, 0.9, 1.1), center=(0.0, 0.0, 0.0), backend=be)
+        tc = be.precision.torch_complex
+        chi = (torch.randn((3, 3) + N, dtype=tc, device="cuda") * 0.3).contiguous()
+        u = torch.randn((2, 3) + N, dtype=tc, device="cuda")
+        op = e.Operator(e.Problem(grid=grid, eps_tensor=chi, wave=u[0], k0=7.0, volume=1.0))
+        try:
+            set_xpass_variant(3)
+            ref, ref_a = op.matvec(u), op.rmatvec(u)
+            for v in (5, 6):
+                set_xpass_variant(v)
+                assert rel_err(be.to_host(op.matvec(u)), be.to_host(ref)) < tol, (N, v)
+                assert rel_err(be.to_host(op.rmatvec(u)), be.to_host(ref_a)) < tol, (N, v)
+        finally:
+            set_xpass_variant(-1)
+        torch.cuda.synchronize()
+        assert int(op.workspace(2)[-256:].view(torch.int32)[0]) == 0
