@@ -54,9 +54,10 @@ SCENE_SEEDS = list(range(10000, 10008))
 # fp64 leg); used only by the reference arm to convert a CPU matvec timing
 # into solves/s.
 FP64_MATVECS_PER_SOLVE = 29.6
-# dram__bytes_read.sum + dram__bytes_write.sum per complex64 EM matvec (all
-# five passes) from the ncu launch list summarised in profiles/em_matvec_128.md.
-NCU_TRAFFIC_BYTES = 1489.6e6
+# dram__bytes_read.sum + dram__bytes_write.sum per complex64 EM matvec at
+# 128^3 (all five passes, default x-pass variant) from an ncu launch list of
+# the same operator (-k regex:kf_, second matvec of the run).
+NCU_TRAFFIC_BYTES = 1493.7e6
 
 
 def byte_model(n: int, c: int) -> int:
