@@ -1,0 +1,85 @@
+"""Fixed workloads for profiling the device path (ncu launch lists and
+captures): ``matvec`` applies the EM operator of the anisotropic ellipsoid
+(``workloads.aniso_ellipsoid_em``, k0 = 12) ``--reps`` times; ``step`` runs
+the benchmark step (network guess + ``MixedBiCGStab`` to true rtol 1e-6 on a
+held-out warm-start scene, untrained network of the benchmark's shape) twice
+and brackets a third run with ``cudaProfilerStart/Stop`` for
+``ncu --profile-from-start off``.
+
+    python -m em3d_b200.profiling matvec --precision single --n 128
+    python -m em3d_b200.profiling step --n 128 --seed 10001
+"""
+from __future__ import annotations
+
+import argparse
+
+
+def matvec(precision: str, n: int, reps: int) -> float:
+    import torch
+
+    from . import workloads
+    from .backend import Backend, Precision
+    from .operator import Operator
+    from .problem import Grid, Problem
+
+    case = workloads.aniso_ellipsoid_em(n, precision, k0=12.0)
+    be = Backend.b200(Precision.SINGLE if precision == "single" else Precision.DOUBLE)
+    grid = Grid(N=case.N, L=case.L, center=case.center, backend=be)
+    prob = Problem(grid=grid, eps_tensor=case.chi, wave=case.wave, k0=case.k0, volume=1.0)
+    op = Operator(prob)
+    out = torch.empty_like(prob.wave)
+    for _ in range(reps):
+        op.apply_into(prob.wave, out)
+    torch.cuda.synchronize()
+    return float(out.abs().sum())
+
+
+def step(n: int, seed: int):
+    import torch
+
+    from . import warmstart as ws
+    from .backend import Precision
+    from .fno import FNO
+    from .operator import Operator
+    from .solvers import MixedBiCGStab, SolverConfig
+
+    net = FNO(width=32, modes=12, layers=4, act="bf16", seed=0)
+    prob = ws.scene_problem(ws.random_scene(seed), ws.unit_grid(n, Precision.DOUBLE, 0))
+    op64 = Operator(prob)
+    op32 = op64.with_precision(Precision.SINGLE)
+    solver = MixedBiCGStab(SolverConfig(max_iter=2000, rtol=1e-6))
+
+    def run():
+        return solver.solve(op64, prob.wave, x0=ws.guess(net, prob), operator_low=op32)
+
+    for _ in range(2):
+        run()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    res = run()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    return res
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    sub = ap.add_subparsers(dest="what", required=True)
+    m = sub.add_parser("matvec")
+    m.add_argument("--precision", choices=("single", "double"), default="single")
+    m.add_argument("--n", type=int, default=128)
+    m.add_argument("--reps", type=int, default=4)
+    s = sub.add_parser("step")
+    s.add_argument("--n", type=int, default=128)
+    s.add_argument("--seed", type=int, default=10001)
+    args = ap.parse_args(argv)
+    if args.what == "matvec":
+        print("ok", matvec(args.precision, args.n, args.reps))
+    else:
+        res = step(args.n, args.seed)
+        print("ok", res.iterations, res.inner_iterations, res.status)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
