@@ -436,21 +436,24 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
   const size_t xstride = (size_t)Ny2 * Nz2;
   const size_t ostride = (size_t)(NX + 1) * (Ny + 1) * (Nz + 1);
-  const int ntiles = nb * Ny2 * ntz;
-
-  auto decode = [&](int tile, int& b, int& ky, int& kz0) {
-    b = tile % nb;
-    const int idx = tile / nb;
+  // Work units (b, jy, kz tile) with jy = 0..Ny: the tiles ky = jy and
+  // ky = 2Ny - jy (one tile when jy is 0 or Ny) fold to the same spectrum
+  // rows, so a CTA transforms both in a row and loads the spectrum slab once.
+  const int nunits = nb * (Ny + 1) * ntz;
+  auto decode = [&](int u, int& b, int& jy, int& kz0) {
+    b = u % nb;
+    const int idx = u / nb;
     kz0 = (idx % ntz) * PP;
-    ky = idx / ntz;
+    jy = idx / ntz;
   };
   // Prefetch loops: a thread always copies the kz lane p of its pencil and
   // steps through the rows (component x position, or spectrum component x
   // folded kx) with a constant stride, so the addresses are incremental.
   constexpr int RSTEP = G::NT / PP;
-  auto issue_field = [&](int tile) {
-    int b, ky, kz0;
-    decode(tile, b, ky, kz0);
+  auto issue_field = [&](int u, int sub) {
+    int b, jy, kz0;
+    decode(u, b, jy, kz0);
+    const int ky = sub ? Ny2 - jy : jy;
     if (entry_done(bs, b)) return;
     if constexpr (TMAF) {
       // kz words of 8 bytes: one per complex64, two per complex128; rows
@@ -472,13 +475,13 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
       else *dst = mk<R>(0, 0);
     }
   };
-  auto issue_spec = [&](int tile) {
-    int b, ky, kz0;
-    decode(tile, b, ky, kz0);
+  auto issue_spec = [&](int u) {
+    int b, jy, kz0;
+    decode(u, b, jy, kz0);
     if (entry_done(bs, b)) return;
     const int kz = kz0 + p;
     const bool ok = kz < Nz2;
-    const T* base = spec + (size_t)b * bs.spec + (size_t)kfold(ky, Ny) * (Nz + 1) + (ok ? kfold(kz, Nz) : 0);
+    const T* base = spec + (size_t)b * bs.spec + (size_t)jy * (Nz + 1) + (ok ? kfold(kz, Nz) : 0);
     const size_t xs = (size_t)(Ny + 1) * (Nz + 1);
     int row = threadIdx.x / PP;                       // component * (NX + 1) + ix
     int sc = row / (NX + 1), ix = row - sc * (NX + 1);
@@ -491,19 +494,25 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     }
   };
 
-  const int tile0 = blockIdx.x;
-  if (tile0 < ntiles) issue_field(tile0);
+  int u = blockIdx.x, sub = 0;
+  if (u < nunits) issue_field(u, 0);
   cp_async_commit();
-  if (tile0 < ntiles) issue_spec(tile0);
+  if (u < nunits) issue_spec(u);
   cp_async_commit();
   const LayPipe<PP> lay{p};
 
-  for (int tile = tile0; tile < ntiles; tile += gridDim.x) {
-    int b, ky, kz0;
-    decode(tile, b, ky, kz0);
+  while (u < nunits) {
+    int b, jy, kz0;
+    decode(u, b, jy, kz0);
+    const int ky = sub ? Ny2 - jy : jy;
     const int kz = kz0 + p;
     const bool valid = kz < Nz2;
-    const int next = tile + gridDim.x;
+    // the next tile: the mirrored ky of this unit, else the CTA's next unit
+    int nu = u, ns = sub + 1;
+    if (ns >= ((jy == 0 || jy == Ny) ? 1 : 2)) {
+      nu = u + gridDim.x;
+      ns = 0;
+    }
     // the same for every thread of the CTA, so the barriers below stay uniform
     const bool live = !entry_done(bs, b);
 
@@ -528,7 +537,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     }
     if constexpr (TMAF) fence_proxy_async_smem();  // these reads before the next tile's TMA overwrite
     __syncthreads();
-    if (next < ntiles) issue_field(next);
+    if (nu < nunits) issue_field(nu, ns);
     cp_async_commit();
 
     if (live) reg_fft_x<L, E, false, false, true, C>(a, t, sm, tw, lay);
@@ -564,7 +573,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
       }
     }
     __syncthreads();
-    if (next < ntiles) issue_spec(next);
+    if (nu < nunits && nu != u) issue_spec(nu);  // the mirrored tile keeps this slab
     cp_async_commit();
 
     if (live) reg_fft_x<L, E, true, true, true, C>(a, t, sm, tw, lay);
@@ -581,6 +590,8 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
         }
       }
     }
+    u = nu;
+    sub = ns;
   }
   cp_async_wait_all();
 }
