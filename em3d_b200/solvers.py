@@ -706,11 +706,16 @@ class DefectCorrection:
         budget_inner = int(self.inner_max_iter or cfg.max_iter)
         rejected = [False] * batch
         for outer in range(self.max_outer + 1):
-            operator.apply_into(u, r)
-            mv64 += 1
-            _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0,
-                      r.data_ptr(), eng.stream())
-            rel = eng.norms(r) / fs
+            if outer == 0 and x0 is None:
+                # zero guess: the residual is f itself (A 0 = 0), no FP64 application
+                r.copy_(f)
+                rel = np.where(fn == 0.0, 0.0, 1.0)
+            else:
+                operator.apply_into(u, r)
+                mv64 += 1
+                _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0,
+                          r.data_ptr(), eng.stream())
+                rel = eng.norms(r) / fs
             if outer == 0 and x0 is not None and self.guess_fallback:
                 for b in range(batch):
                     if status[b] is None and not rel[b] < 1.0:
@@ -901,7 +906,12 @@ class MixedBiCGStab:
         rejected = [False] * batch
         active = [b for b in range(batch) if status[b] is None]
         if active:
-            rel = true_residual(active)
+            if x0 is None:
+                # zero guess: the residual is f itself (A 0 = 0), no FP64 application
+                r.copy_(f)
+                rel = np.ones(batch)
+            else:
+                rel = true_residual(active)
             for b in active:
                 if x0 is not None and self.guess_fallback and not rel[b] < 1.0:
                     row(x, b).zero_()
