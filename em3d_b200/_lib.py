@@ -24,6 +24,7 @@ EM3D_EM = 3
 EM3D_TUNE_XPASS_VARIANT = 0
 EM3D_TUNE_FFT_GENERIC = 1
 EM3D_TUNE_FNO_SIMT = 2
+EM3D_TUNE_FNO_CONTRACT = 3
 
 
 class EmGrid(ctypes.Structure):

@@ -1183,6 +1183,26 @@ int em3d_fno_lift_bwd(int B, size_t ncell, int W, const void* chi, const void* w
   return EM3D_OK;
 }
 
+// Outputs per thread of the blocked contraction: every thread reads its input
+// column once per JB outputs, so a large JB saves loads, while a small JB
+// gives more threads to small problems (the x contractions have outer = B W).
+static int contract_jb(size_t outer, int J, size_t inner) {
+  const size_t cols = outer * inner;
+  if (cols * (size_t)((J + 7) / 8) < (size_t)148 * 256 * 2) return 2;
+  return 8;
+}
+
+#define CONTRACT_JB_DISPATCH(jb, CALL)                                    \
+  do {                                                                    \
+    switch (jb) {                                                         \
+      case 2: { constexpr int JB = 2; CALL; break; }                      \
+      case 4: { constexpr int JB = 4; CALL; break; }                      \
+      case 12: { constexpr int JB = 12; CALL; break; }                    \
+      case 24: { constexpr int JB = 24; CALL; break; }                    \
+      default: { constexpr int JB = 8; CALL; break; }                     \
+    }                                                                     \
+  } while (0)
+
 int em3d_fno_contract(int kind, int act, size_t outer, int L, int J, int inner, const void* X, const void* M, void* Y,
                       void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
@@ -1193,14 +1213,17 @@ int em3d_fno_contract(int kind, int act, size_t outer, int L, int J, int inner, 
   } else if (kind == 1 || kind == 2) {
     const size_t smem = sizeof(float2) * (size_t)L * J;
     if (smem <= 48 * 1024) {
-      constexpr int JB = 8;
-      const size_t nthr = outer * (size_t)((J + JB - 1) / JB) * inner;
-      if (kind == 1)
-        k_contract_blk<JB, false><<<blocks_for(nthr), 256, smem, st>>>(outer, L, J, inner, (const float2*)X,
-                                                                       (const float2*)M, Y);
-      else
-        k_contract_blk<JB, true><<<blocks_for(nthr), 256, smem, st>>>(outer, L, J, inner, (const float2*)X,
-                                                                      (const float2*)M, Y);
+      int jb = em3d_get_tuning(EM3D_TUNE_FNO_CONTRACT);
+      if (jb == 0) jb = contract_jb(outer, J, inner);
+      if (kind == 1) {
+        CONTRACT_JB_DISPATCH(jb, (k_contract_blk<JB, false><<<blocks_for(outer * (size_t)((J + JB - 1) / JB) * inner),
+                                                                256, smem, st>>>(outer, L, J, inner, (const float2*)X,
+                                                                                 (const float2*)M, Y)));
+      } else {
+        CONTRACT_JB_DISPATCH(jb, (k_contract_blk<JB, true><<<blocks_for(outer * (size_t)((J + JB - 1) / JB) * inner),
+                                                               256, smem, st>>>(outer, L, J, inner, (const float2*)X,
+                                                                                (const float2*)M, Y)));
+      }
     } else if (kind == 1) {
       k_contract_c2c<<<blocks_for(n), 256, 0, st>>>(outer, L, J, inner, (const float2*)X, (const float2*)M,
                                                     (float2*)Y);

@@ -34,7 +34,7 @@ extern "C" int em3d_abi_version(void) { return EM3D_ABI_VERSION; }
 namespace em3d {
 
 // Tuning knobs (em3d_set_tuning / em3d_get_tuning).
-int g_tuning[EM3D_TUNE_COUNT] = {-1, 0, 0};
+int g_tuning[EM3D_TUNE_COUNT] = {-1, 0, 0, 0};
 
 // The passes are instantiated in apply_*.cu.
 extern template int apply<float, 3, false>(const Dims&, int, const void*, const void*, const void*, void*, void*, size_t, const int*, cudaStream_t, BatchStrides);
@@ -103,6 +103,11 @@ int em3d_set_tuning(int key, int value) {
   }
   if (key == EM3D_TUNE_FNO_SIMT && value != 0 && value != 1) {
     em3d_set_last_error("FNO row-pass switch must be 0 or 1");
+    return EM3D_ERR_INVALID;
+  }
+  if (key == EM3D_TUNE_FNO_CONTRACT && value != 0 && value != 2 && value != 4 && value != 8 && value != 12 &&
+      value != 24) {
+    em3d_set_last_error("FNO contraction blocking must be 0 (automatic), 2, 4, 8, 12 or 24");
     return EM3D_ERR_INVALID;
   }
   g_tuning[key] = value;

@@ -63,7 +63,8 @@ enum em3d_tune_key {
                                    replaced by the first that fits in the order 6, 4, 1, 2, 0, 5, 3 */
   EM3D_TUNE_FFT_GENERIC = 1,   /* 1 = use the generic shared-memory FFT passes for every axis length */
   EM3D_TUNE_FNO_SIMT = 2,      /* 1 = FNO row pass on CUDA cores even where the tensor-core one applies */
-  EM3D_TUNE_COUNT = 3,
+  EM3D_TUNE_FNO_CONTRACT = 3,  /* FNO truncated-DFT contractions: 0 automatic, else outputs per thread (2, 4, 8, 12, 24) */
+  EM3D_TUNE_COUNT = 4,
 };
 int em3d_set_tuning(int key, int value);
 int em3d_get_tuning(int key);
