@@ -103,6 +103,8 @@ SIGNATURES = {
     "em3d_fno_loss": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "em3d_fno_adam": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_float,
                               ctypes.c_float, ctypes.c_float, ctypes.c_float, c_int, c_void_p, c_void_p]),
+    "em3d_fno_downsample2": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "em3d_fno_upsample2": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "em3d_fno_cast": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p]),
     "em3d_fno_uncast": (c_int, [c_int, c_size_t, c_void_p, c_void_p, c_void_p]),
     "em3d_krylov_state_size": (c_size_t, []),

@@ -1108,6 +1108,88 @@ __global__ void k_contract_blk(size_t outer, int L, int J, int inner, const floa
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Grid resampling for evaluating the network on the half-resolution grid:
+// 2x2x2 cell means down (complex64 or complex128 in, complex64 out) and
+// trilinear interpolation up between cell centres (clamped at the faces, the
+// align_corners = false convention), complex64 in, complex64 or complex128
+// out.  Fields are (C, nx, ny, nz) on the coarse side, C stacked components.
+// ---------------------------------------------------------------------------
+
+template <typename S>
+__global__ void k_down2(int C, int nx, int ny, int nz, const S* __restrict__ in, float2* __restrict__ out) {
+  const size_t n = (size_t)C * nx * ny * nz;
+  const size_t fy = 2 * (size_t)ny, fz = 2 * (size_t)nz;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(o % nz);
+    const int y = (int)((o / nz) % ny);
+    const int x = (int)((o / ((size_t)nz * ny)) % nx);
+    const size_t c = o / ((size_t)nz * ny * nx);
+    const S* b = in + ((c * 2 * nx + 2 * x) * fy + 2 * y) * fz + 2 * z;
+    double re = 0.0, im = 0.0;
+#pragma unroll
+    for (int dx = 0; dx < 2; ++dx)
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+        for (int dz = 0; dz < 2; ++dz) {
+          const S v = b[(dx * fy + dy) * fz + dz];
+          re += (double)v.x;
+          im += (double)v.y;
+        }
+    out[o] = make_float2((float)(0.125 * re), (float)(0.125 * im));
+  }
+}
+
+// fine index j of a doubled axis -> coarse neighbours (i0, i1) and weight of i1
+__device__ __forceinline__ void up_axis(int j, int n, int& i0, int& i1, float& w1) {
+  const int i = j >> 1;
+  if (j & 1) {  // source coordinate i + 1/4
+    i0 = i;
+    i1 = min(i + 1, n - 1);
+    w1 = 0.25f;
+  } else {      // source coordinate i - 1/4, clamped to 0 at the face
+    i0 = i > 0 ? i - 1 : 0;
+    i1 = i;
+    w1 = i > 0 ? 0.75f : 0.0f;
+  }
+}
+
+template <typename D>
+__global__ void k_up2(int C, int nx, int ny, int nz, const float2* __restrict__ in, D* __restrict__ out) {
+  const int Fx = 2 * nx, Fy = 2 * ny, Fz = 2 * nz;
+  const size_t n = (size_t)C * Fx * Fy * Fz;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const int jz = (int)(o % Fz);
+    const int jy = (int)((o / Fz) % Fy);
+    const int jx = (int)((o / ((size_t)Fz * Fy)) % Fx);
+    const size_t c = o / ((size_t)Fz * Fy * Fx);
+    int x0, x1, y0, y1, z0, z1;
+    float wx, wy, wz;
+    up_axis(jx, nx, x0, x1, wx);
+    up_axis(jy, ny, y0, y1, wy);
+    up_axis(jz, nz, z0, z1, wz);
+    const float2* b = in + c * (size_t)nx * ny * nz;
+    float re = 0.0f, im = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+        for (int d = 0; d < 2; ++d) {
+          const float w = (a ? wx : 1.0f - wx) * (bb ? wy : 1.0f - wy) * (d ? wz : 1.0f - wz);
+          const float2 v = b[((size_t)(a ? x1 : x0) * ny + (bb ? y1 : y0)) * nz + (d ? z1 : z0)];
+          re += w * v.x;
+          im += w * v.y;
+        }
+    D r;
+    r.x = re;
+    r.y = im;
+    out[o] = r;
+  }
+}
+
 inline int blocks_for(size_t n, int threads = 256) {
   size_t b = (n + threads - 1) / threads;
   if (b > (size_t)148 * 32) b = (size_t)148 * 32;
@@ -1423,4 +1505,27 @@ int em3d_fno_uncast(int act, size_t n, const void* src, float* dst, void* stream
   return EM3D_OK;
 }
 
+int em3d_fno_downsample2(int in_dtype, int C, int nx, int ny, int nz, const void* in, void* out, void* stream) {
+  if (C < 1 || nx < 1 || ny < 1 || nz < 1 || !in || !out) { em3d_set_last_error("downsample2: bad arguments"); return EM3D_ERR_INVALID; }
+  const size_t n = (size_t)C * nx * ny * nz;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (in_dtype == EM3D_C64) k_down2<float2><<<blocks_for(n), 256, 0, st>>>(C, nx, ny, nz, (const float2*)in, (float2*)out);
+  else if (in_dtype == EM3D_C128) k_down2<double2><<<blocks_for(n), 256, 0, st>>>(C, nx, ny, nz, (const double2*)in, (float2*)out);
+  else { em3d_set_last_error("dtype must be EM3D_C64 or EM3D_C128"); return EM3D_ERR_INVALID; }
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_upsample2(int out_dtype, int C, int nx, int ny, int nz, const void* in, void* out, void* stream) {
+  if (C < 1 || nx < 1 || ny < 1 || nz < 1 || !in || !out) { em3d_set_last_error("upsample2: bad arguments"); return EM3D_ERR_INVALID; }
+  const size_t n = (size_t)C * 8 * nx * ny * nz;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (out_dtype == EM3D_C64) k_up2<float2><<<blocks_for(n), 256, 0, st>>>(C, nx, ny, nz, (const float2*)in, (float2*)out);
+  else if (out_dtype == EM3D_C128) k_up2<double2><<<blocks_for(n), 256, 0, st>>>(C, nx, ny, nz, (const float2*)in, (double2*)out);
+  else { em3d_set_last_error("dtype must be EM3D_C64 or EM3D_C128"); return EM3D_ERR_INVALID; }
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
 }  // extern "C"
+

@@ -32,6 +32,7 @@ from typing import List, Sequence
 
 import numpy as np
 
+from . import _lib
 from .backend import Backend, Precision
 from .fno import FNO
 from .operator import Operator
@@ -187,14 +188,47 @@ def load(path: str, act: str = "bf16") -> FNO:
 
 
 # ----------------------------------------------------------- warm start
-def guess(net: FNO, problem: Problem, wave=None):
+def guess(net: FNO, problem: Problem, wave=None, *, half_grid: bool = False):
     """The network's u for ``problem`` (incident field ``wave``, default the
-    problem's own), in the problem's dtype (3, N, N, N)."""
+    problem's own), in the problem's dtype (3, N, N, N).
+
+    ``half_grid``: evaluate the network on the grid of half the resolution
+    (2x2x2 cell means of the contrast and the incident field, on the device)
+    and interpolate its output back to the problem's grid (trilinear between
+    cell centres).  A network trained at 64^3 then runs at the resolution it
+    was trained on for a 128^3 problem, at an eighth of the cells."""
     import torch
 
-    chi = problem.eps_tensor.to(torch.complex64).unsqueeze(0)
-    wave = (problem.wave if wave is None else wave).to(torch.complex64).unsqueeze(0)
-    return net.forward(chi, wave, train=False)[0].to(problem.wave.dtype)
+    w = problem.wave if wave is None else wave
+    if not half_grid:
+        chi = problem.eps_tensor.to(torch.complex64).unsqueeze(0)
+        return net.forward(chi, w.to(torch.complex64).unsqueeze(0), train=False)[0].to(problem.wave.dtype)
+    N = tuple(int(v) for v in problem.grid.N)
+    if any(v % 2 for v in N):
+        raise ValueError(f"half_grid needs even grid sizes, got {N}")
+    n = tuple(v // 2 for v in N)
+    dev = problem.eps_tensor.device
+    st = _lib.stream_handle()
+    chi = torch.empty((1, 3, 3) + n, dtype=torch.complex64, device=dev)
+    _lib.call("em3d_fno_downsample2", _native(problem.eps_tensor), 9, *n, problem.eps_tensor.contiguous().data_ptr(),
+              chi.data_ptr(), st)
+    wc = w.contiguous()
+    wv = torch.empty((1, 3) + n, dtype=torch.complex64, device=dev)
+    _lib.call("em3d_fno_downsample2", _native(wc), 3, *n, wc.data_ptr(), wv.data_ptr(), st)
+    u = net.forward(chi, wv, train=False)[0].contiguous()
+    out = torch.empty((3,) + N, dtype=problem.wave.dtype, device=dev)
+    _lib.call("em3d_fno_upsample2", _native(out), 3, *n, u.data_ptr(), out.data_ptr(), st)
+    return out
+
+
+def _native(t) -> int:
+    import torch
+
+    if t.dtype == torch.complex64:
+        return _lib.EM3D_C64
+    if t.dtype == torch.complex128:
+        return _lib.EM3D_C128
+    raise TypeError(f"expected complex64 or complex128, got {t.dtype}")
 
 
 # ----------------------------------------------------------- evaluation
@@ -229,7 +263,7 @@ def _timed(fn, reps: int):
 
 
 def evaluate(net: FNO, seeds: Sequence[int], N: int, *, rtol: float = 1e-6, max_iter: int = 4000,
-             reps: int = 2, device_index: int = 0, log_every: int = 0) -> List[EvalRecord]:
+             reps: int = 2, device_index: int = 0, log_every: int = 0, half_grid: bool = False) -> List[EvalRecord]:
     """Per held-out scene: FP64 BiCGStab and the mixed solve (FP32 BiCGStab with
     FP64 reliable updates, ``MixedBiCGStab``), each from the zero guess and from
     the network's guess, to a TRUE relative residual of ``rtol``; ``reps`` runs
@@ -244,7 +278,7 @@ def evaluate(net: FNO, seeds: Sequence[int], N: int, *, rtol: float = 1e-6, max_
         op64 = Operator(prob)
         op32 = op64.with_precision(Precision.SINGLE)
         f = prob.wave
-        u_nn, nn_ms = _timed(lambda: guess(net, prob), reps)
+        u_nn, nn_ms = _timed(lambda: guess(net, prob, half_grid=half_grid), reps)
         u_nn = u_nn.clone()
         cfg = SolverConfig(max_iter=max_iter, rtol=rtol)
         runs = {}
@@ -318,6 +352,8 @@ def main(argv=None) -> int:
     ap.add_argument("--eval", type=int, default=len(EVAL_SEEDS), help="held-out scenes (seeds 10000..)")
     ap.add_argument("--eval-n", default="64,128")
     ap.add_argument("--data-rtol", type=float, default=1e-4)
+    ap.add_argument("--half-grid", action="store_true",
+                    help="evaluate the network on the half-resolution grid and interpolate its output")
     ap.add_argument("--out", default=None, help="JSON summary path")
     ap.add_argument("--save", default=None, help="weights .npz path")
     a = ap.parse_args(argv)
@@ -338,7 +374,7 @@ def main(argv=None) -> int:
     print(json.dumps(summary["train"]), flush=True)
     del data
     for n in (int(v) for v in a.eval_n.split(",") if v):
-        recs = evaluate(net, list(EVAL_SEEDS)[:a.eval], n, log_every=max(a.eval // 4, 1))
+        recs = evaluate(net, list(EVAL_SEEDS)[:a.eval], n, log_every=max(a.eval // 4, 1), half_grid=a.half_grid)
         summary[f"eval_{n}"] = summarize(recs)
         print(json.dumps({f"eval_{n}": summary[f"eval_{n}"]}), flush=True)
     summary["total_s"] = time.perf_counter() - t0

@@ -321,6 +321,13 @@ int em3d_fno_row_forward(int act, int lift, int B, int W, int X, int Y, int Z, i
                          const void* wave, const void* vin, const void* Uxy, const void* Wt, const float* bias,
                          int apply_gelu, void* pre_out, void* vout, void* Vz, const void* Q, const float* qb,
                          void* u_out, void* stream);
+/* Half-resolution evaluation of the network on an even grid: 2x2x2 cell
+ * means of (C, 2nx, 2ny, 2nz) fields (complex64 or complex128) into complex64
+ * (C, nx, ny, nz), and trilinear interpolation back between cell centres
+ * (clamped at the faces) into complex64 or complex128 (C, 2nx, 2ny, 2nz).
+ * No reference counterpart (the network is not part of the reference). */
+int em3d_fno_downsample2(int in_dtype, int C, int nx, int ny, int nz, const void* in, void* out, void* stream);
+int em3d_fno_upsample2(int out_dtype, int C, int nx, int ny, int nz, const void* in, void* out, void* stream);
 int em3d_fno_cast(int act, size_t n, const float* src, void* dst, void* stream);
 int em3d_fno_uncast(int act, size_t n, const void* src, float* dst, void* stream);
 

@@ -150,3 +150,62 @@ def test_tensor_core_row_pass_matches_cuda_core_pass(N, m):
         assert float(torch.linalg.vector_norm(corr_a - corr_b) / torch.linalg.vector_norm(corr_b)) < 3e-2
         for x, y in zip(out[(0, train)][1], out[(1, train)][1]):
             assert float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)) < 3e-2
+
+
+@pytest.mark.parametrize("src", ["complex64", "complex128"])
+def test_half_grid_resampling_matches_torch(src):
+    """2x2x2 means and trilinear interpolation between cell centres against
+    torch's avg_pool3d / interpolate(align_corners=False) in FP32."""
+    import torch
+    import torch.nn.functional as F
+
+    from em3d_b200 import _lib
+
+    dt = getattr(torch, src)
+    n = (5, 6, 7)
+    C = 4
+    x = torch.randn((C,) + tuple(2 * v for v in n), dtype=dt, device="cuda")
+    down = torch.empty((C,) + n, dtype=torch.complex64, device="cuda")
+    _lib.call("em3d_fno_downsample2", _lib.EM3D_C64 if src == "complex64" else _lib.EM3D_C128, C, *n, x.data_ptr(),
+              down.data_ptr(), _lib.stream_handle())
+    xr = torch.view_as_real(x.to(torch.complex64)).permute(0, 4, 1, 2, 3).reshape(1, 2 * C, *(2 * v for v in n))
+    ref = F.avg_pool3d(xr, 2).reshape(C, 2, *n).permute(0, 2, 3, 4, 1)
+    assert torch.allclose(torch.view_as_real(down), ref, atol=1e-6, rtol=1e-5)
+
+    up = torch.empty((C,) + tuple(2 * v for v in n), dtype=dt, device="cuda")
+    _lib.call("em3d_fno_upsample2", _lib.EM3D_C64 if src == "complex64" else _lib.EM3D_C128, C, *n, down.data_ptr(),
+              up.data_ptr(), _lib.stream_handle())
+    dr = torch.view_as_real(down).permute(0, 4, 1, 2, 3).reshape(1, 2 * C, *n)
+    ref_up = F.interpolate(dr, scale_factor=2, mode="trilinear", align_corners=False)
+    ref_up = ref_up.reshape(C, 2, *(2 * v for v in n)).permute(0, 2, 3, 4, 1)
+    assert torch.allclose(torch.view_as_real(up).float(), ref_up, atol=1e-6, rtol=1e-5)
+
+
+def test_half_grid_guess_composes_the_resampling():
+    """guess(..., half_grid=True) is the network on the 2x2x2-averaged inputs,
+    interpolated back."""
+    import torch
+
+    import em3d_b200 as e
+    from em3d_b200 import warmstart as ws
+    from em3d_b200.fno import FNO
+
+    net = FNO(width=32, modes=4, layers=2, act="bf16", seed=1)
+    prob = ws.scene_problem(ws.random_scene(3), ws.unit_grid(32, e.Precision.DOUBLE, 0))
+    got = ws.guess(net, prob, half_grid=True)
+    assert got.shape == prob.wave.shape and got.dtype == prob.wave.dtype
+    # inputs of the half grid: the means of the fine grid's inputs (in FP64,
+    # then rounded to complex64 as the kernel does)
+    import torch.nn.functional as F
+
+    def avg(t):
+        r = torch.view_as_real(t.to(torch.complex128)).movedim(-1, 0)
+        lead = r.shape[:-3]
+        y = F.avg_pool3d(r.reshape(-1, 1, 32, 32, 32), 2).reshape(lead + (16, 16, 16))
+        return torch.view_as_complex(y.movedim(0, -1).contiguous()).to(torch.complex64)
+
+    u = net.forward(avg(prob.eps_tensor).unsqueeze(0), avg(prob.wave).unsqueeze(0), train=False)[0]
+    ur = torch.view_as_real(u).permute(0, 4, 1, 2, 3).reshape(1, 6, 16, 16, 16)
+    ref = F.interpolate(ur, scale_factor=2, mode="trilinear", align_corners=False)
+    ref = torch.view_as_complex(ref.reshape(3, 2, 32, 32, 32).permute(0, 2, 3, 4, 1).contiguous())
+    assert float((got.to(torch.complex64) - ref).abs().max()) < 1e-4 * float(ref.abs().max())
