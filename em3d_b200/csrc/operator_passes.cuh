@@ -665,11 +665,13 @@ static bool generic_forced() {
   return g_tuning[EM3D_TUNE_FFT_GENERIC] != 0 || (v && v[0] == '1');
 }
 
-// 160 has a register plan in complex64 only: its 20 elements per thread
-// would spill in complex128.
-static bool fast_len(int L, bool fp64) {
-  return !generic_forced() &&
-         (L == 32 || L == 64 || L == 128 || L == 256 || L == 512 || L == 96 || L == 192 || (L == 160 && !fp64));
+// 160 (20 elements per thread) runs on the register plan in complex64 for
+// every pass and in complex128 for the row and pencil passes (one pencil per
+// thread); the complex128 x pass, which holds three pencils per thread, would
+// spill and uses the generic passes.
+static bool fast_len(int L, bool fp64, bool x_pass) {
+  return !generic_forced() && (L == 32 || L == 64 || L == 128 || L == 256 || L == 512 || L == 96 || L == 192 ||
+                               (L == 160 && !(fp64 && x_pass)));
 }
 
 template <typename R, int L, int C, int LD, int ST, bool INV>
@@ -697,8 +699,7 @@ static int launch_rows_fast(int L, const cx<R>* in, const cx<R>* chi, const cx<R
     case 512: return go_rows<R, 512, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
     case 96: return go_rows<R, 96, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
     case 160:
-      if constexpr (sizeof(R) == 4) return go_rows<R, 160, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
-      break;
+      return go_rows<R, 160, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
     case 192: return go_rows<R, 192, C, LD, ST, INV>(in, chi, base, out, tw, rows_pb, nrows, skip, st, bs);
   }
   em3d_set_last_error("no register FFT for this length");
@@ -730,8 +731,7 @@ static int launch_strided_fast(int L, const cx<R>* in, cx<R>* out, const cx<R>* 
     case 512: return go_strided<R, 512, INV>(in, out, tw, outer, inner, skip, st, bs);
     case 96: return go_strided<R, 96, INV>(in, out, tw, outer, inner, skip, st, bs);
     case 160:
-      if constexpr (sizeof(R) == 4) return go_strided<R, 160, INV>(in, out, tw, outer, inner, skip, st, bs);
-      break;
+      return go_strided<R, 160, INV>(in, out, tw, outer, inner, skip, st, bs);
     case 192: return go_strided<R, 192, INV>(in, out, tw, outer, inner, skip, st, bs);
   }
   em3d_set_last_error("no register FFT for this length");
@@ -913,7 +913,7 @@ int apply(const Dims& d, int batch, const void* spectrum, const void* chi, const
   int rc;
   const int Lz = 2 * d.nz, Ly = 2 * d.ny;
   constexpr bool F64 = sizeof(R) == 8;
-  const bool fz = fast_len(Lz, F64), fy = fast_len(Ly, F64), fx = fast_len(2 * d.nx, F64);
+  const bool fz = fast_len(Lz, F64, false), fy = fast_len(Ly, F64, false), fx = fast_len(2 * d.nx, F64, true);
   constexpr int LDF = C == 3 ? LD_EM_CHI : LD_AC_CHI;
   constexpr int FLDF = C == 3 ? FLD_EM_CHI : FLD_AC_CHI;
   constexpr int STA = C == 3 ? ST_EM_ADJ : ST_AC_ADJ;

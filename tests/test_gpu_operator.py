@@ -230,7 +230,7 @@ def test_register_fft_path_matches_generic_path(prec, kind, monkeypatch):
 def test_mixed_radix_register_path_matches_generic_path(prec, kind):
     """Doubled axes 96 = 3 x 32, 160 = 5 x 32 and 192 = 3 x 64 on the register
     FFT (radix 4, 6 / 10 / 12, 4), every x-pass variant, against the generic
-    passes (complex128 keeps 160 on the generic passes)."""
+    passes (complex128 runs the x pass of 160 on the generic passes)."""
     import torch
     import em3d_b200 as e
     from em3d_b200 import _lib, acoustics as ea
