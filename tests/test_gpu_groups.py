@@ -144,3 +144,19 @@ def test_stopped_entries_are_left_untouched(variant, prec):
         tune.set_xpass_variant(old)
     assert torch.equal(out[1], torch.full_like(x[1], 7.0 + 3.0j))
     assert torch.equal(out[0], full[0]) and torch.equal(out[2], full[2])
+
+
+def test_acoustic_group_mixed_solve_matches_problem_by_problem():
+    from em3d_b200.acoustics import AcousticOperator
+    from em3d_b200.groups import AcousticOperatorGroup
+    from em3d_b200.solvers import MixedBiCGStab, SolverConfig
+
+    probs = _problems((16, 12, 10), acoustic=True)
+    group = AcousticOperatorGroup(probs)
+    cfg = SolverConfig(max_iter=300, rtol=1e-8)
+    batch = MixedBiCGStab(cfg).solve_batch(group, group.waves())
+    for b, p in enumerate(probs):
+        one = MixedBiCGStab(cfg).solve(AcousticOperator(p), p.wave)
+        assert batch[b].status == one.status == "converged", b
+        assert batch[b].iterations == one.iterations and batch[b].inner_iterations == one.inner_iterations, b
+        assert rel_err(batch[b].u.cpu().numpy(), one.u.cpu().numpy()) < 1e-6, b
