@@ -760,8 +760,8 @@ static int go_xpipe(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d
   EM3D_CUDA_TRY(allow_smem(kern));
   const size_t smem = (size_t)G::TOTAL * sizeof(cx<R>) + G::BYTES_EXTRA;
   const int ntz = (2 * d.nz + G::P - 1) / G::P;
-  // work units: (entry, jy = 0..Ny, kz tile), each one or two tiles
-  const long long ntiles = (long long)batch * (d.ny + 1) * ntz;
+  // work units: (entries, jy = 0..Ny, kz tile), see kf_xmul_pipe
+  const long long ntiles = (long long)(batch / xpipe_entries_per_unit(batch, bs.spec == 0)) * (d.ny + 1) * ntz;
   static int sms = 0;
   if (sms == 0) {
     int dev = 0;

@@ -386,6 +386,13 @@ template <int P> struct LayPipe {
   __device__ __forceinline__ int operator()(int c, int pos) const { return pos * P + p + 2 * (pos >> 2); }
 };
 
+// Batch entries per work unit of the pipelined x pass: up to 4 when the batch
+// shares one spectrum (the slab is then loaded once for up to 8 tiles), 1 for
+// a group of operators.  Small units keep the CTAs' loads balanced.
+__host__ __device__ inline int xpipe_entries_per_unit(int nb, bool shared) {
+  return !shared ? 1 : (nb % 4 == 0 ? 4 : (nb % 2 == 0 ? 2 : 1));
+}
+
 template <int L, int E, int C, int NTT> struct XpipeGeom {
   static constexpr int TT = L / E;
   static constexpr int P = (NTT / TT) > 32 ? 32 : ((NTT / TT) >= 2 ? (NTT / TT) : 2);
@@ -436,24 +443,30 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   const int Ny2 = 2 * Ny, Nz2 = 2 * Nz;
   const size_t xstride = (size_t)Ny2 * Nz2;
   const size_t ostride = (size_t)(NX + 1) * (Ny + 1) * (Nz + 1);
-  // Work units (b, jy, kz tile) with jy = 0..Ny: the tiles ky = jy and
+  // Work units (jy, kz tile) with jy = 0..Ny: the tiles ky = jy and
   // ky = 2Ny - jy (one tile when jy is 0 or Ny) fold to the same spectrum
-  // rows, so a CTA transforms both in a row and loads the spectrum slab once.
-  const int nunits = nb * (Ny + 1) * ntz;
-  auto decode = [&](int u, int& b, int& jy, int& kz0) {
-    b = u % nb;
-    const int idx = u / nb;
+  // rows, and when the batch shares one spectrum (bs.spec == 0) so do its
+  // entries; a unit covers nbu entries, whose tiles a CTA transforms in a row
+  // (entry-major, then the two ky), loading the spectrum slab once.
+  const int nbu = xpipe_entries_per_unit(nb, bs.spec == 0);
+  const int ngroups = nb / nbu;                 // units per (jy, kz tile)
+  const int nunits = ngroups * (Ny + 1) * ntz;
+  auto decode = [&](int u, int& bg, int& jy, int& kz0) {
+    bg = u % ngroups;
+    const int idx = u / ngroups;
     kz0 = (idx % ntz) * PP;
     jy = idx / ntz;
   };
+  auto nmirror = [&](int jy) { return (jy == 0 || jy == Ny) ? 1 : 2; };
   // Prefetch loops: a thread always copies the kz lane p of its pencil and
   // steps through the rows (component x position, or spectrum component x
   // folded kx) with a constant stride, so the addresses are incremental.
   constexpr int RSTEP = G::NT / PP;
   auto issue_field = [&](int u, int sub) {
-    int b, jy, kz0;
-    decode(u, b, jy, kz0);
-    const int ky = sub ? Ny2 - jy : jy;
+    int bg, jy, kz0;
+    decode(u, bg, jy, kz0);
+    const int b = bg * nbu + sub / nmirror(jy);
+    const int ky = (sub % nmirror(jy)) ? Ny2 - jy : jy;
     if (entry_done(bs, b)) return;
     if constexpr (TMAF) {
       // kz words of 8 bytes: one per complex64, two per complex128; rows
@@ -477,8 +490,8 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   };
   auto issue_spec = [&](int u) {
     int b, jy, kz0;
-    decode(u, b, jy, kz0);
-    if (entry_done(bs, b)) return;
+    decode(u, b, jy, kz0);  // with one entry per unit, b is that entry
+    if (nbu == 1 && entry_done(bs, b)) return;
     const int kz = kz0 + p;
     const bool ok = kz < Nz2;
     const T* base = spec + (size_t)b * bs.spec + (size_t)jy * (Nz + 1) + (ok ? kfold(kz, Nz) : 0);
@@ -502,14 +515,15 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   const LayPipe<PP> lay{p};
 
   while (u < nunits) {
-    int b, jy, kz0;
-    decode(u, b, jy, kz0);
-    const int ky = sub ? Ny2 - jy : jy;
+    int bg, jy, kz0;
+    decode(u, bg, jy, kz0);
+    const int b = bg * nbu + sub / nmirror(jy);
+    const int ky = (sub % nmirror(jy)) ? Ny2 - jy : jy;
     const int kz = kz0 + p;
     const bool valid = kz < Nz2;
-    // the next tile: the mirrored ky of this unit, else the CTA's next unit
+    // the next tile: the unit's next (entry, ky), else the CTA's next unit
     int nu = u, ns = sub + 1;
-    if (ns >= ((jy == 0 || jy == Ny) ? 1 : 2)) {
+    if (ns >= nbu * nmirror(jy)) {
       nu = u + gridDim.x;
       ns = 0;
     }
