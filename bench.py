@@ -50,10 +50,10 @@ METRIC = "time_to_true_rtol1e-6_128^3_mixed+nn_solves_per_s"
 UNIT = "solves/s"
 SCENE_SEEDS = list(range(10000, 10008))
 # Mean FP64 BiCGStab matvecs per solve to true rtol 1e-6 of the scenes a
-# default run times (seeds 10000..10004; measured on B200 by this script's
-# fp64 leg); used only by the reference arm to convert a CPU matvec timing
-# into solves/s.
-FP64_MATVECS_PER_SOLVE = 29.6
+# default run times (seeds 10000..10007, each twice; measured on B200 by this
+# script's fp64 leg); used only by the reference arm to convert a CPU matvec
+# timing into solves/s.
+FP64_MATVECS_PER_SOLVE = 23.375
 # dram__bytes_read.sum + dram__bytes_write.sum per complex64 EM matvec at
 # 128^3 (all five passes, default x-pass variant) from an ncu launch list of
 # the same operator (-k regex:kf_, second matvec of the run).
