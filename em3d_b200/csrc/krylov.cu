@@ -160,7 +160,18 @@ __global__ void __launch_bounds__(kThreads) k_dots(size_t n, const cx<R>* x0, co
   x0 += vo; y0 += vo;
   if (x1) { x1 += vo; y1 += vo; }
   double v[4] = {0, 0, 0, 0};
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+  const size_t gs = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (!x1) {
+    for (; i + 3 * gs < n; i += 4 * gs) {
+      cx<R> x[4], y[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { x[k] = x0[i + k * gs]; y[k] = y0[i + k * gs]; }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc_dot(v[0], v[1], x[k], y[k]);
+    }
+  }
+  for (; i < n; i += gs) {
     acc_dot(v[0], v[1], x0[i], y0[i]);
     if (x1) acc_dot(v[2], v[3], x1[i], y1[i]);
   }
@@ -234,8 +245,17 @@ __global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, 
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; rh += vo; v += vo; }
   double a[2] = {0, 0};
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    acc_dot(a[0], a[1], rh[i], v[i]);
+  // four strides of loads in flight per thread (this kernel only reads)
+  const size_t gs = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  for (; i + 3 * gs < n; i += 4 * gs) {
+    cx<R> x[4], y[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { x[k] = rh[i + k * gs]; y[k] = v[i + k * gs]; }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc_dot(a[0], a[1], x[k], y[k]);
+  }
+  for (; i < n; i += gs) acc_dot(a[0], a[1], rh[i], v[i]);
   double tot[2];
   if (reduce_last<2>(sv, a, tot) && threadIdx.x == 0) {
     em3d_krylov_state* st = sv.st;
