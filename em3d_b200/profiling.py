@@ -1,8 +1,9 @@
 """Fixed workloads for profiling the device path (ncu launch lists and
 captures): ``matvec`` applies the EM operator of the anisotropic ellipsoid
 (``workloads.aniso_ellipsoid_em``, k0 = 12) ``--reps`` times; ``step`` runs
-the benchmark step (network guess + ``MixedBiCGStab`` to true rtol 1e-6 on a
-held-out warm-start scene, untrained network of the benchmark's shape) twice
+the benchmark step (network guess on the half-resolution grid +
+``MixedBiCGStab`` to true rtol 1e-6 on a held-out warm-start scene, untrained
+network of the benchmark's shape) twice
 and brackets a third run with ``cudaProfilerStart/Stop`` for
 ``ncu --profile-from-start off``.
 
@@ -50,7 +51,7 @@ def step(n: int, seed: int):
     solver = MixedBiCGStab(SolverConfig(max_iter=2000, rtol=1e-6))
 
     def run():
-        return solver.solve(op64, prob.wave, x0=ws.guess(net, prob), operator_low=op32)
+        return solver.solve(op64, prob.wave, x0=ws.guess(net, prob, half_grid=True), operator_low=op32)
 
     for _ in range(2):
         run()
