@@ -57,7 +57,7 @@ FP64_MATVECS_PER_SOLVE = 23.375
 # dram__bytes_read.sum + dram__bytes_write.sum per complex64 EM matvec at
 # 128^3 (all five passes, default x-pass variant) from an ncu launch list of
 # the same operator (-k regex:kf_, second matvec of the run).
-NCU_TRAFFIC_BYTES = 1491.7e6
+NCU_TRAFFIC_BYTES = 1405.8e6
 
 
 def byte_model(n: int, c: int) -> int:
