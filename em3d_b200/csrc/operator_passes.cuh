@@ -440,7 +440,7 @@ template <typename K> static cudaError_t allow_smem(K kernel) {
   return e;
 }
 
-static int check_grid(const em3d_grid* g, Dims* d) {
+static inline int check_grid(const em3d_grid* g, Dims* d) {
   if (!g) { em3d_set_last_error("grid is NULL"); return EM3D_ERR_INVALID; }
   if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0) { em3d_set_last_error("grid sizes must be positive"); return EM3D_ERR_INVALID; }
   if (!(g->lx > 0 && g->ly > 0 && g->lz > 0)) { em3d_set_last_error("grid lengths must be positive"); return EM3D_ERR_INVALID; }

@@ -418,14 +418,14 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
   using T = cx<R>;
   using G = XpipeGeom<L, E, C, NTT>;
   using PL = RegPlan<L, E>;
-  constexpr int TT = G::TT, PP = G::P, NX = G::NX, NSP = G::NSPEC;
+  constexpr int TT = G::TT, PP = G::P, NX = G::NX;
   constexpr int R1 = PL::first(false), RL = PL::last(false);
   constexpr int M1 = L / R1, ML = L / RL;
   constexpr int EB = (int)sizeof(T);
   if (skip_launch(skip)) return;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_pipe[];
   // the field slab first: TMA writes it at a 128-byte aligned address
-  T* sfield = reinterpret_cast<T*>(smem_raw);
+  T* sfield = reinterpret_cast<T*>(smem_pipe);
   T* tw = sfield + G::FIELD;
   T* sm = tw + G::TW;
   T* sspec = sm + G::EXCH;
