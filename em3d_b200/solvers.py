@@ -904,6 +904,9 @@ class MixedBiCGStab:
         hist = [[] for _ in range(batch)]
         counts = [[] for _ in range(batch)]
         rejected = [False] * batch
+        u32, r32, rh, p, v, s, tt = (V[k] for k in ("u", "r", "r_hat", "p", "v", "s", "t"))
+        mv32 = np.zeros(batch, dtype=np.int64)
+        r32_ready = False  # the first cycle starts from r32 as it stands
         active = [b for b in range(batch) if status[b] is None]
         if active:
             if x0 is None:
@@ -911,21 +914,36 @@ class MixedBiCGStab:
                 r.copy_(f)
                 rel = np.ones(batch)
             else:
-                rel = true_residual(active)
+                # a guess only starts the iteration: its residual is formed with
+                # the FP32 operator (the first update takes the FP64 one); a
+                # guess that may already meet the tolerance is judged in FP64
+                n_all = eng.n * batch
+                _lib.call("em3d_vec_convert", n_all, eng.dt, x.data_ptr(), _lib.EM3D_C64, u32.data_ptr(), 0, stream)
+                buf["op_lo"].apply_into(u32, v)
+                _lib.call("em3d_vec_convert", n_all, eng.dt, f.data_ptr(), _lib.EM3D_C64, r32.data_ptr(), 0, stream)
+                _lib.call("em3d_vec_axpby", _lib.EM3D_C64, n_all, r32.data_ptr(), 1.0, 0.0, r32.data_ptr(), -1.0, 0.0,
+                          v.data_ptr(), stream)
+                mv32[active] += 1
+                rel = e32.norms(r32) / fs
+                if any(rel[b] < 10.0 * tol[b] or not np.isfinite(rel[b]) for b in active):
+                    rel = true_residual(active)
+                else:
+                    r32_ready = True
             for b in active:
                 if x0 is not None and self.guess_fallback and not rel[b] < 1.0:
                     row(x, b).zero_()
                     row(r, b).copy_(row(f, b))
+                    if r32_ready:
+                        _lib.call("em3d_vec_convert", eng.n, eng.dt, row(f, b).data_ptr(), _lib.EM3D_C64,
+                                  row(r32, b).data_ptr(), 0, stream)
                     rel[b] = 1.0
                     rejected[b] = True
                 hist[b].append(float(rel[b]))
-                counts[b].append(int(mv64[b]))
+                counts[b].append(int(mv64[b] + mv32[b]))
                 if not np.isfinite(rel[b]):
                     status[b] = "nonfinite"
                 elif rel[b] < tol[b]:
                     status[b] = "converged"
-
-        u32, r32, rh, p, v, s, tt = (V[k] for k in ("u", "r", "r_hat", "p", "v", "s", "t"))
 
         def iteration():
             e32.step("em3d_bicgstab_p", r32.data_ptr(), p.data_ptr(), v.data_ptr())
@@ -941,7 +959,6 @@ class MixedBiCGStab:
         hosts = e32.state.hosts
         restart = [True] * batch
         total_its = np.zeros(batch, dtype=np.int64)
-        mv32 = np.zeros(batch, dtype=np.int64)
         cycles = [[] for _ in range(batch)]
         stalled = np.zeros(batch, dtype=np.int64)
         budget = int(cfg.max_iter)
@@ -954,8 +971,10 @@ class MixedBiCGStab:
             running = [b for b in range(batch) if status[b] is None]
             if not running:
                 break
-            _lib.call("em3d_vec_convert", eng.n * batch, eng.dt, r.data_ptr(), _lib.EM3D_C64, r32.data_ptr(), 0,
-                      stream)
+            if not r32_ready:
+                _lib.call("em3d_vec_convert", eng.n * batch, eng.dt, r.data_ptr(), _lib.EM3D_C64, r32.data_ptr(), 0,
+                          stream)
+            r32_ready = False
             u32.zero_()
             n0 = e32.norms(r32)
             dots = None
