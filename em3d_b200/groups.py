@@ -189,3 +189,75 @@ def group_by_grid(problems: Sequence, acoustic: bool = False) -> "OrderedDict":
         buckets.setdefault((tuple(p.grid.N), tuple(p.grid.L)), []).append(i)
     cls = AcousticOperatorGroup if acoustic else OperatorGroup
     return OrderedDict((k, (idx, cls([problems[i] for i in idx]))) for k, idx in buckets.items())
+
+
+class GroupedSolver:
+    """Solves a list of problems of mixed grid sizes: one group per size, each
+    group solved as one batch by its own solver, the groups' solves on their
+    own CUDA streams at the same time (one host thread each), so small grids
+    run alongside large ones.  Results come back in the input order.
+
+        gs = GroupedSolver(problems, lambda: MixedBiCGStab(cfg), low_precision=Precision.SINGLE)
+        results = gs.solve()
+
+    ``make_solver`` builds one solver per group (solvers keep per-operator
+    caches and are not shared between threads); ``low_precision`` builds each
+    group's twin for the mixed solvers' ``operator_low``.
+    """
+
+    def __init__(self, problems, make_solver, *, acoustic: bool = False, low_precision=None):
+        import torch
+
+        self.problems = list(problems)
+        self.groups = group_by_grid(self.problems, acoustic=acoustic)
+        self.solvers = {k: make_solver() for k in self.groups}
+        self.lows = ({k: g.with_precision(low_precision) for k, (_, g) in self.groups.items()}
+                     if low_precision is not None else {})
+        self.streams = {k: torch.cuda.Stream(device=g.backend.torch_device) for k, (_, g) in self.groups.items()}
+
+    def _solve_group(self, key):
+        idx, group = self.groups[key]
+        kw = {"operator_low": self.lows[key]} if key in self.lows else {}
+        return idx, self.solvers[key].solve_batch(group, group.waves(), **kw)
+
+    def solve(self, concurrent: bool = True) -> list:
+        import threading
+
+        import torch
+
+        out = [None] * len(self.problems)
+        if not concurrent or len(self.groups) == 1:
+            for key in self.groups:
+                idx, res = self._solve_group(key)
+                for i, r in zip(idx, res):
+                    out[i] = r
+            return out
+        caller = torch.cuda.current_stream()
+        errors = []
+
+        def work(key):
+            try:
+                stream = self.streams[key]
+                stream.wait_stream(caller)
+                with torch.cuda.stream(stream):
+                    idx, res = self._solve_group(key)
+                for r in res:
+                    # the results are used on the caller's stream from here on
+                    if isinstance(getattr(r, "u", None), torch.Tensor):
+                        r.u.record_stream(caller)
+                stream.synchronize()
+                for i, r in zip(idx, res):
+                    out[i] = r
+            except BaseException as exc:  # re-raised in the calling thread
+                errors.append(exc)
+
+        threads = [threading.Thread(target=work, args=(key,)) for key in self.groups]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
+        for stream in self.streams.values():
+            caller.wait_stream(stream)
+        return out

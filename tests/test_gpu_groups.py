@@ -160,3 +160,23 @@ def test_acoustic_group_mixed_solve_matches_problem_by_problem():
         assert batch[b].status == one.status == "converged", b
         assert batch[b].iterations == one.iterations and batch[b].inner_iterations == one.inner_iterations, b
         assert rel_err(batch[b].u.cpu().numpy(), one.u.cpu().numpy()) < 1e-6, b
+
+
+def test_grouped_solver_concurrent_equals_sequential():
+    """Problems of two grid sizes: the groups' solves on their own streams at
+    the same time give the sequential results, in the input order."""
+    import em3d_b200 as e
+    from em3d_b200.groups import GroupedSolver
+    from em3d_b200.solvers import MixedBiCGStab, SolverConfig
+
+    a, b = _problems((16, 16, 16)), _problems((12, 10, 14))
+    probs = [a[0], b[0], a[1], b[1], a[2], b[2]]
+    cfg = SolverConfig(max_iter=300, rtol=1e-8)
+    gs = GroupedSolver(probs, lambda: MixedBiCGStab(cfg), low_precision=e.Precision.SINGLE)
+    seq = gs.solve(concurrent=False)
+    con = gs.solve(concurrent=True)
+    for i, p in enumerate(probs):
+        one = MixedBiCGStab(cfg).solve(e.Operator(p), p.wave)
+        assert seq[i].iterations == con[i].iterations == one.iterations, i
+        assert rel_err(con[i].u.cpu().numpy(), seq[i].u.cpu().numpy()) == 0.0, i
+        assert con[i].u.shape == p.wave.shape
