@@ -818,13 +818,14 @@ static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& 
 // SM); 2 = component-split threads (EM only); 3 = persistent CTAs with the
 // next tile's field and spectrum prefetched by cp.async, 256 threads; 4 = the
 // same with 128 threads; 5 and 6 = 3 and 4 with the field slab loaded by TMA.
-// -1 (the default) picks, per operator kind, the
-// fastest measured on B200: EM 6 (both precisions; 128^3, 96^3, 80^3),
-// acoustic 0 (256^3).
-static int xmul_variant(int C) {
+// -1 (the default) picks, per operator kind and x length, the fastest
+// measured on B200: EM 6 (both precisions; 128^3, 96^3, 80^3); acoustic 5 on
+// 512-point axes (256^3) and 0 on shorter ones (128^3).
+static int xmul_variant(int C, int L) {
   const int v = g_tuning[EM3D_TUNE_XPASS_VARIANT];
   if (v >= 0) return v;
-  return C == 3 ? 6 : 0;
+  if (C == 3) return 6;
+  return L >= 512 ? 5 : 0;
 }
 
 // Shared memory of each x-pass variant; a variant that does not fit in the
@@ -848,7 +849,7 @@ template <typename R, int C, bool ADJ, int L>
 static int launch_xmul_len(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch,
                            const int* skip, cudaStream_t st, BatchStrides bs) {
   constexpr int EB = FastE<R, L>::E;
-  int v = xmul_variant(C);
+  int v = xmul_variant(C, L);
   if (C == 1 && v == 2) v = 0;  // the component split is EM only
   if (xvariant_smem<R, L, C, EB>(v) > kSmemPerCta) {
     for (int alt : {6, 4, 1, 2, 0, 5, 3}) {

@@ -56,7 +56,7 @@ const char* em3d_last_error(void);
  * in the reference, which has no native code to tune.
  * ------------------------------------------------------------------------ */
 enum em3d_tune_key {
-  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: EM 6, acoustic 0), 0 register 256-thread, 1 register
+  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: EM 6, acoustic 5 at 512 points, else 0), 0 register 256-thread, 1 register
                                    128-thread, 2 component-split, 3 persistent cp.async-pipelined 256-thread,
                                    4 the same 128-thread, 5 and 6 = 3 and 4 with the field slab loaded by
                                    TMA; a variant whose shared memory does not fit is
