@@ -6,8 +6,10 @@ raised.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import os
+import threading
 from ctypes import POINTER, c_double, c_int, c_int32, c_size_t, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -46,6 +48,7 @@ SIGNATURES = {
     "em3d_apply_workspace_bytes": (c_size_t, [_GRID, c_int, c_int, c_int]),
     "em3d_em_spectrum_build": (c_int, [_GRID, c_double, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
     "em3d_acoustic_spectrum_build": (c_int, [_GRID, c_double, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "em3d_spectrum_convert": (c_int, [_GRID, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p]),
     "em3d_em_kernel_hat_full": (c_int, [_GRID, c_double, c_int, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
     "em3d_acoustic_kernel_hat_full": (c_int, [_GRID, c_double, c_int, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
     "em3d_em_matvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
@@ -167,14 +170,41 @@ def check(status: int, what: str) -> None:
 LAUNCHES = {
     "em3d_em_matvec": 5, "em3d_em_rmatvec": 5, "em3d_acoustic_matvec": 5, "em3d_acoustic_rmatvec": 5,
 }
+# Kernels launched by this process (graph replays add their captured counts).
+# Host threads update it under a lock; a thread that is capturing a graph
+# counts into its own capture counter instead (captured, not launched).
 launch_count = 0
+_count_lock = threading.Lock()
+_tls = threading.local()
+
+
+def add_launches(n: int) -> None:
+    global launch_count
+    with _count_lock:
+        launch_count += int(n)
+
+
+@contextlib.contextmanager
+def capturing():
+    """Count this thread's launches into a list ``[n]`` instead of
+    ``launch_count`` while a CUDA graph is being captured."""
+    prev = getattr(_tls, "capture", None)
+    _tls.capture = [0]
+    try:
+        yield _tls.capture
+    finally:
+        _tls.capture = prev
 
 
 def count_launches(name: str) -> None:
-    global launch_count
     if name.startswith("em3d_") and not name.endswith(("_bytes", "_offset", "_size", "_error", "_version",
                                                        "_tuning")):
-        launch_count += LAUNCHES.get(name, 1)
+        n = LAUNCHES.get(name, 1)
+        cap = getattr(_tls, "capture", None)
+        if cap is not None:
+            cap[0] += n
+        else:
+            add_launches(n)
 
 
 def call(name: str, *args) -> int:

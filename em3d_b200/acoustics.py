@@ -113,18 +113,20 @@ class AcousticOperator(_Applier):
     _kind = _lib.EM3D_ACOUSTIC
     _native_names = ("em3d_acoustic_matvec", "em3d_acoustic_rmatvec")
 
-    def __init__(self, problem: AcousticProblem):
+    def __init__(self, problem: AcousticProblem, *, _spectrum=None):
         self.problem = problem
         grid = problem.grid
         self._be = grid.backend
         self._N = tuple(grid.N)
-        g, ws = _build_workspace(grid)
-        dt = self._be.precision.native_dtype
-        nbytes = _lib.load().em3d_spectrum_bytes(ctypes_ref(g), _lib.EM3D_ACOUSTIC, dt)
-        spec = _uint8(nbytes, self._be.torch_device)
-        _lib.call("em3d_acoustic_spectrum_build", ctypes_ref(g), float(problem.k0), dt, spec.data_ptr(),
-                  ws.data_ptr(), ws.numel(), _lib.stream_handle())
-        del ws
+        spec = _spectrum
+        if spec is None:
+            g, ws = _build_workspace(grid)
+            dt = self._be.precision.native_dtype
+            nbytes = _lib.load().em3d_spectrum_bytes(ctypes_ref(g), _lib.EM3D_ACOUSTIC, dt)
+            spec = _uint8(nbytes, self._be.torch_device)
+            _lib.call("em3d_acoustic_spectrum_build", ctypes_ref(g), float(problem.k0), dt, spec.data_ptr(),
+                      ws.data_ptr(), ws.numel(), _lib.stream_handle())
+            del ws
         self._setup_native(grid, spec, problem.chi)
 
     @property
@@ -142,17 +144,19 @@ class AcousticOperator(_Applier):
         import torch
 
         x = self._as_field(u, "u")
-        return self.apply_into(x, torch.empty_like(x))
+        return self._apply_checked(x, torch.empty_like(x))
 
     def rmatvec(self, v):
         import torch
 
         x = self._as_field(v, "v")
-        return self.apply_into(x, torch.empty_like(x), adjoint=True)
+        return self._apply_checked(x, torch.empty_like(x), adjoint=True)
 
     def with_precision(self, precision) -> "AcousticOperator":
-        """The same operator at another precision (FP32 twin for inner solves)."""
+        """The same operator at another precision (FP32 twin for inner solves);
+        its spectrum is this operator's, converted on the device."""
         from .backend import Backend
+        from .operator import convert_spectrum
 
         if precision == self._be.precision:
             return self
@@ -162,7 +166,8 @@ class AcousticOperator(_Applier):
         tc = precision.torch_complex
         prob = AcousticProblem(grid=grid, eta=self.problem.eta.to(tc), wave=self.problem.wave.to(tc),
                                k0=self.problem.k0, volume=self.problem.volume)
-        return AcousticOperator(prob)
+        spec = convert_spectrum(self._spectrum, grid, _lib.EM3D_ACOUSTIC, self._be.precision, precision)
+        return AcousticOperator(prob, _spectrum=spec)
 
     def kernel_hat(self, adjoint: bool = False):
         """Reference-layout spectrum ``fftn(K)`` (or ``fftn(conj K)``), (2Nx,2Ny,2Nz)."""

@@ -49,6 +49,52 @@ class Precision(Enum):
         return EM3D_C64 if self is Precision.SINGLE else EM3D_C128
 
 
+_DEVICE_ARRAY = None
+
+
+def device_array_type():
+    """``torch.Tensor`` subclass carrying NumPy's ``copy()`` method.
+
+    The reference solvers copy vectors with ``x.copy()``
+    (``src/em3d/solvers/bicgstab.py:76, 91``), which plain torch tensors lack.
+    Arrays made by :class:`TorchNamespace` are of this type, and torch
+    propagates it through arithmetic (and ``Operator.matvec`` keeps the type
+    of its argument), so every vector the reference solvers derive from them
+    has ``copy()`` as well.  Created on first use so that importing this
+    module does not import torch.
+
+    The type also passes NumPy complex scalars to torch as Python ``complex``:
+    the reference scales vectors by ``be.complex_dtype(alpha)``
+    (``bicgstab.py:95-114``), and torch drops the imaginary part of a
+    ``numpy.complex64`` scalar operand (only ``numpy.complex128``, a subclass
+    of ``complex``, is read correctly).  ``complex(np.complex64(a))`` holds the
+    same FP32-rounded value, and a Python scalar does not promote a complex64
+    tensor, so the product is the reference's complex64 product."""
+    global _DEVICE_ARRAY
+    if _DEVICE_ARRAY is None:
+        import torch
+
+        def _scalar(a):
+            return complex(a) if isinstance(a, np.complexfloating) else a
+
+        class DeviceArray(torch.Tensor):
+            def copy(self):
+                return self.clone()
+
+            @classmethod
+            def __torch_function__(cls, func, types, args=(), kwargs=None):
+                args = tuple(_scalar(a) for a in args)
+                return super().__torch_function__(func, types, args, kwargs or {})
+
+        _DEVICE_ARRAY = DeviceArray
+    return _DEVICE_ARRAY
+
+
+def as_device_array(t):
+    """View a torch tensor as :func:`device_array_type` (no copy)."""
+    return t.as_subclass(device_array_type())
+
+
 def _torch_dtype(dtype):
     import torch
 
@@ -78,24 +124,26 @@ class TorchNamespace:
 
     # construction
     def zeros(self, shape, dtype=None):
-        return self._torch.zeros(shape, dtype=_torch_dtype(dtype), device=self.device)
+        return as_device_array(self._torch.zeros(shape, dtype=_torch_dtype(dtype), device=self.device))
 
     def empty(self, shape, dtype=None):
-        return self._torch.empty(shape, dtype=_torch_dtype(dtype), device=self.device)
+        return as_device_array(self._torch.empty(shape, dtype=_torch_dtype(dtype), device=self.device))
 
     def zeros_like(self, x):
-        return self._torch.zeros_like(x)
+        return as_device_array(self._torch.zeros_like(x))
 
     def ones_like(self, x):
-        return self._torch.ones_like(x)
+        return as_device_array(self._torch.ones_like(x))
 
     def asarray(self, obj, dtype=None):
         t = self._torch
         if isinstance(obj, t.Tensor):
             out = obj.to(device=self.device)
-            return out if dtype is None else out.to(_torch_dtype(dtype))
-        arr = np.asarray(obj) if dtype is None else np.asarray(obj, dtype=dtype)
-        return t.as_tensor(arr, device=self.device)
+            out = out if dtype is None else out.to(_torch_dtype(dtype))
+        else:
+            arr = np.asarray(obj) if dtype is None else np.asarray(obj, dtype=dtype)
+            out = t.as_tensor(arr, device=self.device)
+        return as_device_array(out)
 
     array = asarray
 

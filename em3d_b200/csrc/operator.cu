@@ -89,6 +89,32 @@ static int apply_grouped(const em3d_grid* g, int dtype, int batch, const void* s
   return apply<double, C, ADJ>(d, batch, spectra, chis, u, out, ws, wsb, skip, st, bs);
 }
 
+template <typename S, typename D> __global__ void k_round_copy(const S* __restrict__ src, D* __restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = from_c64<decltype(dst[0].x)>(to_c64(src[i]));
+}
+
+// Copy a prepared spectrum into another precision: the octant blocks and the
+// twiddle tables are converted element by element.  A build in either
+// precision computes the same FP64 values (octant samples scaled by 1/(8N);
+// twiddles from sincospi) and rounds them once to the stored type, so a
+// complex128 spectrum rounded to complex64 is bit-identical to a complex64
+// build (the widening direction only changes the type).
+template <typename RS, typename RD>
+static int spectrum_convert(const Dims& d, int kind, const void* src, void* dst, cudaStream_t st) {
+  SpecLayout<RS> ls(d, kind);
+  SpecLayout<RD> ld(d, kind);
+  const size_t noct = ls.blocks * ls.oct_elems;
+  const size_t ntw = (size_t)2 * (d.nx + d.ny + d.nz);
+  void* s = const_cast<void*>(src);
+  const int g1 = (int)std::min<size_t>((noct + 255) / 256, (size_t)148 * 16);
+  k_round_copy<<<g1, 256, 0, st>>>(ls.oct(s), ld.oct(dst), noct);
+  EM3D_LAUNCH_CHECK();
+  k_round_copy<<<(int)((ntw + 255) / 256), 256, 0, st>>>(ls.twx(s, d), ld.twx(dst, d), ntw);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
 }  // namespace em3d
 
 using namespace em3d;
@@ -156,6 +182,23 @@ int em3d_acoustic_spectrum_build(const em3d_grid* g, double k0, int dtype, void*
   cudaStream_t st = (cudaStream_t)stream;
   if (dtype == EM3D_C64) return ac_spectrum_build<float>(g, d, k0, spectrum, ws, wsb, st);
   if (dtype == EM3D_C128) return ac_spectrum_build<double>(g, d, k0, spectrum, ws, wsb, st);
+  em3d_set_last_error("dtype must be EM3D_C64 or EM3D_C128");
+  return EM3D_ERR_INVALID;
+}
+
+int em3d_spectrum_convert(const em3d_grid* g, int kind, int src_dtype, const void* src, int dst_dtype, void* dst,
+                          void* stream) {
+  Dims d;
+  int rc = check_grid(g, &d);
+  if (rc) return rc;
+  if (kind != EM3D_EM && kind != EM3D_ACOUSTIC) { em3d_set_last_error("kind must be EM3D_EM or EM3D_ACOUSTIC"); return EM3D_ERR_INVALID; }
+  if (!src || !dst) { em3d_set_last_error("NULL spectrum"); return EM3D_ERR_INVALID; }
+  if (src == dst) { em3d_set_last_error("src and dst must be different buffers"); return EM3D_ERR_INVALID; }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (src_dtype == EM3D_C128 && dst_dtype == EM3D_C64) return spectrum_convert<double, float>(d, kind, src, dst, st);
+  if (src_dtype == EM3D_C64 && dst_dtype == EM3D_C128) return spectrum_convert<float, double>(d, kind, src, dst, st);
+  if (src_dtype == EM3D_C64 && dst_dtype == EM3D_C64) return spectrum_convert<float, float>(d, kind, src, dst, st);
+  if (src_dtype == EM3D_C128 && dst_dtype == EM3D_C128) return spectrum_convert<double, double>(d, kind, src, dst, st);
   em3d_set_last_error("dtype must be EM3D_C64 or EM3D_C128");
   return EM3D_ERR_INVALID;
 }

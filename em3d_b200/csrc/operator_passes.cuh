@@ -440,6 +440,25 @@ template <typename K> static cudaError_t allow_smem(K kernel) {
   return e;
 }
 
+// Multiprocessor count of the current device, looked up once per device
+// ordinal (host threads driving different GPUs each get their own entry).
+static cudaError_t sm_count(int* out) {
+  constexpr int kMaxDev = 64;
+  static std::mutex mu;
+  static int cache[kMaxDev] = {0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < kMaxDev && cache[dev] > 0) { *out = cache[dev]; return cudaSuccess; }
+  int n = 0;
+  e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < kMaxDev) cache[dev] = n;
+  *out = n;
+  return cudaSuccess;
+}
+
 static inline int check_grid(const em3d_grid* g, Dims* d) {
   if (!g) { em3d_set_last_error("grid is NULL"); return EM3D_ERR_INVALID; }
   if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0) { em3d_set_last_error("grid sizes must be positive"); return EM3D_ERR_INVALID; }
@@ -762,12 +781,8 @@ static int go_xpipe(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d
   const int ntz = (2 * d.nz + G::P - 1) / G::P;
   // work units: (entries, jy = 0..Ny, kz tile), see kf_xmul_pipe
   const long long ntiles = (long long)(batch / xpipe_entries_per_unit(batch, bs.spec == 0)) * (d.ny + 1) * ntz;
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    EM3D_CUDA_TRY(cudaGetDevice(&dev));
-    EM3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  }
+  int sms = 0;
+  EM3D_CUDA_TRY(sm_count(&sms));
   int per_sm = 0;
   EM3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, G::NT, smem));
   if (per_sm < 1) per_sm = 1;

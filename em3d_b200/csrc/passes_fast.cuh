@@ -533,8 +533,17 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     cp_async_wait_one();  // this tile's field slab
     __syncthreads();
     if constexpr (TMAF) {
-      if (live) {
-        mbar_wait_bounded(fbar, fphase, status);
+      if (live) {  // uniform over the CTA
+        const bool arrived = mbar_wait_bounded(fbar, fphase);
+        if (!__syncthreads_and(arrived)) {
+          // the field slab never arrived: count it once, give the copy still in
+          // flight one more bounded wait, issue nothing further and leave (the
+          // host reads the count and reports the application as failed)
+          if (threadIdx.x == 0 && status != nullptr) atomicAdd(status, 1);
+          mbar_wait_bounded(fbar, fphase);
+          cp_async_wait_all();
+          return;
+        }
         fphase ^= 1u;
       }
     }

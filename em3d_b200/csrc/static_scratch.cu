@@ -16,10 +16,13 @@
 // variable directly: the host-side symbol is only a stand-in).  That look-up
 // happens during the first call on each device, so make that first call
 // before capturing a stream into a CUDA graph.  The passes write every
-// workspace element before reading it, so nothing has to be cleared between
-// calls.  All calls share the one array: calls that overlap on the GPU (on
-// different streams, or from several host threads) race and must be
-// serialised by the caller.
+// transform element before reading it; the one part that must start at zero,
+// the status words at the end of this call's workspace (the count of bounded
+// waits that gave up), is cleared by each call on its stream before the
+// passes.  This entry point does not report that count to its caller (the
+// regular entry points leave it in the caller's workspace).  All calls share the
+// one array: calls that overlap on the GPU (on different streams, or from
+// several host threads) race and must be serialised by the caller.
 #include <mutex>
 
 #include "common.cuh"
@@ -74,7 +77,11 @@ int em3d_em_matvec_static_scratch(const em3d_grid* g, int dtype, const void* spe
   void* ws = nullptr;
   const int rc = scratch_address(&ws);
   if (rc != EM3D_OK) return rc;
-  return em3d_em_matvec(g, dtype, 1, spectrum, chi, u, out, ws, kStaticScratchBytes, skip, stream);
+  // The status words are the workspace's last 256 bytes (need - 256 into the
+  // array), a place that a call on a larger grid used for transform data:
+  // clear them on the caller's stream so this call starts from a zero count.
+  EM3D_CUDA_TRY(cudaMemsetAsync((char*)ws + (need - 256), 0, 256, (cudaStream_t)stream));
+  return em3d_em_matvec(g, dtype, 1, spectrum, chi, u, out, ws, need, skip, stream);
 }
 
 }  // extern "C"

@@ -22,7 +22,7 @@ from typing import Sequence
 import numpy as np
 
 from . import _lib
-from .operator import _build_workspace, _uint8, ctypes_ref
+from .operator import _build_workspace, _uint8, ctypes_ref, raise_on_failed_waits, status_word
 
 
 def _align(n: int, a: int = 256) -> int:
@@ -105,17 +105,30 @@ class _Group:
                   int(entry_done[1]) if entry_done else 0, _lib.stream_handle(stream))
         return out
 
+    def status_word(self, batch: int = 0):
+        """Device int32 counting the failed bounded waits of this group's
+        applications (every application covers the whole group)."""
+        return status_word(self.workspace(len(self)))
+
+    def check_status(self) -> None:
+        """Raise ``NativeError`` if an application since the last check lost a transfer."""
+        raise_on_failed_waits(list(self._workspaces.values()), type(self).__name__)
+
     def matvec(self, fields):
         import torch
 
         x = fields.to(device=self._be.torch_device, dtype=self._tc).contiguous()
-        return self.apply_into(x, torch.empty_like(x))
+        out = self.apply_into(x, torch.empty_like(x))
+        self.check_status()
+        return out
 
     def rmatvec(self, fields):
         import torch
 
         x = fields.to(device=self._be.torch_device, dtype=self._tc).contiguous()
-        return self.apply_into(x, torch.empty_like(x), adjoint=True)
+        out = self.apply_into(x, torch.empty_like(x), adjoint=True)
+        self.check_status()
+        return out
 
     def true_relative_residuals(self, u, rhs) -> np.ndarray:
         """``||f_b - A_b u_b|| / ||f_b||`` per problem (FP64 norms)."""

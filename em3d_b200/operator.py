@@ -37,6 +37,18 @@ def _uint8(nbytes, device):
     return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=device)
 
 
+def convert_spectrum(spectrum, grid: Grid, kind: int, src_precision, dst_precision):
+    """A prepared spectrum buffer converted to ``dst_precision`` on the device."""
+    g = _lib.make_grid(grid.N, grid.L)
+    nbytes = _lib.load().em3d_spectrum_bytes(ctypes_ref(g), kind, dst_precision.native_dtype)
+    if nbytes == 0:
+        _lib.check(_lib.EM3D_ERR_INVALID, "em3d_spectrum_bytes")
+    out = _uint8(nbytes, spectrum.device)
+    _lib.call("em3d_spectrum_convert", ctypes_ref(g), kind, src_precision.native_dtype, spectrum.data_ptr(),
+              dst_precision.native_dtype, out.data_ptr(), _lib.stream_handle())
+    return out
+
+
 def _build_workspace(grid: Grid):
     g = _lib.make_grid(grid.N, grid.L)
     nb = _lib.load().em3d_build_workspace_bytes(ctypes_ref(g))
@@ -49,6 +61,36 @@ def ctypes_ref(obj):
     import ctypes
 
     return ctypes.byref(obj)
+
+
+# The last bytes of an apply workspace hold status words; the int32 at their
+# start counts the bounded waits inside the passes that gave up (a transfer
+# into shared memory that never completed; the application is then invalid).
+STATUS_BYTES = 256
+
+
+def status_word(ws):
+    """int32 view (one element) of the give-up count of apply workspace ``ws``."""
+    import torch
+
+    n = ws.numel()
+    return ws[n - STATUS_BYTES:n - STATUS_BYTES + 4].view(torch.int32)
+
+
+def raise_on_failed_waits(workspaces, what: str, counts=None) -> None:
+    """Raise ``NativeError`` when a workspace's give-up count is non-zero.
+
+    ``counts`` (optional) are values already read on the host, one per
+    workspace, so callers that synchronise anyway need no further read.  The
+    count is reset to zero before raising, so the operator stays usable."""
+    for i, ws in enumerate(workspaces):
+        v = status_word(ws)
+        n = int(v.item()) if counts is None else int(counts[i])
+        if n:
+            v.zero_()
+            raise _lib.NativeError(
+                f"{what}: {n} bounded wait(s) inside the operator passes gave up (a transfer into shared memory "
+                f"did not complete); the result of this application is invalid")
 
 
 @dataclass(frozen=True)
@@ -93,7 +135,14 @@ class PreparedEMKernel:
 
     @property
     def persistent_nbytes(self) -> int:
-        return int(self.spectrum.numel())
+        """Device bytes this kernel holds: the octant spectrum, plus the full
+        reference-layout spectra once ``kernel_hat`` / ``kernel_hat_adjoint``
+        have materialised them (see :meth:`release_full_spectra`)."""
+        return int(self.spectrum.numel()) + sum(int(t.numel() * t.element_size()) for t in self._cache.values())
+
+    def release_full_spectra(self) -> None:
+        """Drop the cached full spectra (the operator never reads them)."""
+        self._cache.clear()
 
     def _full(self, adjoint: bool):
         import torch
@@ -166,6 +215,16 @@ class _Applier:
     def _field_shape(self):
         raise NotImplementedError
 
+    def status_word(self, batch: int = 1):
+        """Device int32 counting the failed bounded waits of applications over
+        ``batch`` right-hand sides (see :func:`raise_on_failed_waits`)."""
+        return status_word(self.workspace(batch))
+
+    def check_status(self) -> None:
+        """Raise ``NativeError`` if an application since the last check lost a
+        transfer (reads the status words on the host: one synchronisation)."""
+        raise_on_failed_waits(list(self._workspaces.values()), type(self).__name__)
+
     def workspace(self, batch: int):
         ws = self._workspaces.get(batch)
         if ws is None:
@@ -201,6 +260,15 @@ class _Applier:
         name = self._native_names[1 if adjoint else 0]
         _lib.call(name, ctypes_ref(self._grid_c), self._dt, b, self._spectrum.data_ptr(), self._chi.data_ptr(),
                   x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(), skip_ptr, _lib.stream_handle(stream))
+        return out
+
+    def _apply_checked(self, x, out, adjoint: bool = False):
+        """``apply_into`` followed by :meth:`check_status`: the public
+        ``matvec`` / ``rmatvec`` return only results whose transfers all
+        completed.  (``apply_into`` itself does not synchronise; the solvers
+        read the status words together with their own flags.)"""
+        self.apply_into(x, out, adjoint=adjoint)
+        self.check_status()
         return out
 
 
@@ -243,12 +311,14 @@ class Operator(_Applier):
         import torch
 
         out = torch.empty_like(x)
-        return self.apply_into(x, out)
+        return self._apply_checked(x, out)
 
     def with_precision(self, precision) -> "Operator":
         """The same operator (grid, k0, contrast) at another precision: the
         FP32 twin used for inner solves of a defect-correction loop.  Its
-        spectrum is rebuilt from the FP64 sampling and stored in ``precision``."""
+        spectrum is this operator's, converted (``em3d_spectrum_convert``:
+        complex128 -> complex64 gives the bytes of a complex64 build) rather
+        than sampled and transformed again."""
         from .backend import Backend
         from .problem import Grid, Problem
 
@@ -260,7 +330,11 @@ class Operator(_Applier):
         tc = precision.torch_complex
         prob = Problem(grid=grid, eps_tensor=self.problem.eps_tensor.to(tc), wave=self.problem.wave.to(tc),
                        k0=self.problem.k0, volume=self.problem.volume)
-        pk = PreparedEMKernel.build(grid, k=self.problem.k0, include_adjoint=self._prepared_kernel.supports_adjoint)
+        src = self._prepared_kernel
+        spec = convert_spectrum(src.spectrum, grid, _lib.EM3D_EM, self._be.precision, precision)
+        pk = PreparedEMKernel(grid_shape=src.grid_shape, grid_lengths=src.grid_lengths, wave_number=src.wave_number,
+                              device=str(be.device), precision=str(precision.value), spectrum=spec,
+                              adjoint_storage=src.adjoint_storage, build_strategy=src.build_strategy, _backend=be)
         return Operator(prob, prepared_kernel=pk)
 
     def rmatvec(self, field):
@@ -270,7 +344,7 @@ class Operator(_Applier):
         import torch
 
         out = torch.empty_like(x)
-        return self.apply_into(x, out, adjoint=True)
+        return self._apply_checked(x, out, adjoint=True)
 
     def matvec_flat(self, vector):
         from .layout import flatten_field, unflatten_field

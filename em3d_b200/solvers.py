@@ -183,6 +183,13 @@ class DeviceState:
         return res
 
 
+def _check_status(operator) -> None:
+    """Raise if one of ``operator``'s applications lost a transfer (operators
+    of this package; other operators have no status words)."""
+    if hasattr(operator, "check_status"):
+        operator.check_status()
+
+
 def _native_dtype(t) -> int:
     import torch
 
@@ -270,33 +277,50 @@ class _Engine:
         CUDA graph."""
         import torch
 
-        if self.state.done():
+        if self.poll():
             return
         if self.graph is None and use_graph and self.native_op:
             iteration()  # the first iteration runs eagerly (and loads the kernels)
-            if self.state.done():
+            if self.poll():
                 return
-            before = _lib.launch_count
-            try:
-                graph = torch.cuda.CUDAGraph()
-                side = torch.cuda.Stream(device=self.rhs.device)
-                side.wait_stream(torch.cuda.current_stream())
-                with torch.cuda.graph(graph, stream=side, capture_error_mode="thread_local"):
-                    for _ in range(chunk):
-                        iteration()
-                torch.cuda.current_stream().wait_stream(side)
-                self.graph = graph
-            except RuntimeError:
-                self.graph = None
-            self.per_replay = _lib.launch_count - before
-            _lib.launch_count = before  # captured, not launched
-        while not self.state.done():
+            with _lib.capturing() as captured:
+                try:
+                    graph = torch.cuda.CUDAGraph()
+                    side = torch.cuda.Stream(device=self.rhs.device)
+                    side.wait_stream(torch.cuda.current_stream())
+                    with torch.cuda.graph(graph, stream=side, capture_error_mode="thread_local"):
+                        for _ in range(chunk):
+                            iteration()
+                    torch.cuda.current_stream().wait_stream(side)
+                    self.graph = graph
+                except RuntimeError:
+                    self.graph = None
+            self.per_replay = captured[0]
+        while not self.poll():
             if self.graph is not None:
                 self.graph.replay()
-                _lib.launch_count += self.per_replay
+                _lib.add_launches(self.per_replay)
             else:
                 for _ in range(chunk if self.native_op else 1):
                     iteration()
+
+    def poll(self) -> bool:
+        """Whether every right-hand side has stopped: one host read of the done
+        flag.  The operator's status word (bounded waits inside its passes that
+        gave up) is copied to pinned memory ahead of that read and checked after
+        it, so a lost transfer ends the solve with ``NativeError`` at no extra
+        synchronisation."""
+        import torch
+
+        src = self.op.status_word(self.batch) if hasattr(self.op, "status_word") else None
+        if src is not None:
+            if getattr(self, "_status_host", None) is None:
+                self._status_host = torch.zeros(1, dtype=torch.int32).pin_memory()
+            self._status_host.copy_(src, non_blocking=True)
+        done = self.state.done()
+        if src is not None and int(self._status_host[0]) != 0:
+            self.op.check_status()
+        return done
 
 
 def _status_name(code: int) -> str:
@@ -588,6 +612,7 @@ def true_relative_residual(operator, solution, rhs) -> float:
     _lib.call("em3d_vec_axpby", eng.dt, eng.n, res.data_ptr(), 1.0, 0.0, res.data_ptr(), -1.0, 0.0,
               eng.rhs.data_ptr(), eng.stream())
     rn = eng.norm(res)
+    _check_status(operator)
     return rn if rhs_norm == 0.0 else rn / rhs_norm
 
 
@@ -716,6 +741,7 @@ class DefectCorrection:
                 _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0,
                           r.data_ptr(), eng.stream())
                 rel = eng.norms(r) / fs
+                _check_status(operator)
             if outer == 0 and x0 is not None and self.guess_fallback:
                 for b in range(batch):
                     if status[b] is None and not rel[b] < 1.0:
@@ -899,11 +925,14 @@ class MixedBiCGStab:
             mv64[list(active)] += 1
             _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0,
                       r.data_ptr(), stream)
-            return eng.norms(r) / fs
+            rel_ = eng.norms(r) / fs
+            _check_status(operator)
+            return rel_
 
         hist = [[] for _ in range(batch)]
         counts = [[] for _ in range(batch)]
         rejected = [False] * batch
+        estimated = [False] * batch  # history holds only the FP32 estimate
         u32, r32, rh, p, v, s, tt = (V[k] for k in ("u", "r", "r_hat", "p", "v", "s", "t"))
         mv32 = np.zeros(batch, dtype=np.int64)
         r32_ready = False  # the first cycle starts from r32 as it stands
@@ -938,6 +967,9 @@ class MixedBiCGStab:
                                   row(r32, b).data_ptr(), 0, stream)
                     rel[b] = 1.0
                     rejected[b] = True
+                # residual_history[0] of an accepted guess is this FP32-operator
+                # estimate; the reported final residual is always an FP64 one
+                estimated[b] = r32_ready and not rejected[b]
                 hist[b].append(float(rel[b]))
                 counts[b].append(int(mv64[b] + mv32[b]))
                 if not np.isfinite(rel[b]):
@@ -1046,6 +1078,16 @@ class MixedBiCGStab:
                 if status[b] is None and stalled[b] >= 2:
                     status[b] = inner if inner not in ("converged", "running") else "max_iter"
                 restart[b] = int(st.pending) != 0 or inner not in ("converged", "max_iter")
+            for b in running:
+                estimated[b] = False
+        # a solve that ended before any cycle (no budget) still reports the FP64
+        # true residual of its guess as the final residual
+        final = {b: float(hist[b][-1]) for b in range(batch) if hist[b]}
+        late = [b for b in range(batch) if estimated[b]]
+        if late:
+            rel_t = true_residual(late)
+            for b in late:
+                final[b] = float(rel_t[b])
         u = x.clone()  # the cached buffer is reused by the next solve
         out = []
         for b in range(batch):
@@ -1058,7 +1100,7 @@ class MixedBiCGStab:
             out.append(DefectCorrectionResult(
                 u=ub, iterations=int(total_its[b]), residual_history=hist[b], converged=status[b] == "converged",
                 matvec_count=int(mv64[b] + mv32[b]), rmatvec_count=0, residual_action_counts=counts[b],
-                status=status[b], true_final_residual=float(hist[b][-1]), outer_iterations=len(cycles[b]),
+                status=status[b], true_final_residual=final[b], outer_iterations=len(cycles[b]),
                 inner_iterations=cycles[b], fp64_matvecs=int(mv64[b]), fp32_matvecs=int(mv32[b]),
                 guess_rejected=rejected[b]))
         return out

@@ -107,6 +107,15 @@ int em3d_em_spectrum_build(const em3d_grid* g, double k, int dtype, void* spectr
 int em3d_acoustic_spectrum_build(const em3d_grid* g, double k0, int dtype, void* spectrum,
                                  void* build_ws, size_t build_ws_bytes, void* stream);
 
+/* The spectrum `src` (built for grid g and operator `kind` in `src_dtype`)
+ * copied into `dst` (em3d_spectrum_bytes(g, kind, dst_dtype) bytes) in
+ * `dst_dtype`.  complex128 -> complex64 gives exactly the bytes of a
+ * complex64 build, without sampling or transforming again: the FP32 twin of
+ * an FP64 operator (PreparedEMKernel.build, src/em3d/operator.py:171-223,
+ * for the same grid and k in the other precision). */
+int em3d_spectrum_convert(const em3d_grid* g, int kind, int src_dtype, const void* src, int dst_dtype,
+                          void* dst, void* stream);
+
 /* Full reference-layout EM spectrum (3,3,2Nx,2Ny,2Nz) in `dtype`, exactly
  * PreparedEMKernel.kernel_hat (adjoint = 0) or kernel_hat_adjoint = fftn(conj K)
  * (adjoint = 1) of src/em3d/operator.py:202-211.  Diagnostic export only; the

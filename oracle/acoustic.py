@@ -70,6 +70,42 @@ def matvec(chi, u, khat, N):
     return (u - big[:nx, :ny, :nz]).astype(cdt, copy=False)
 
 
+def matvec_streamed(chi, u, N, L, k0: float, adjoint: bool = False, precision: str = "double"):
+    """``AcousticOperator.matvec`` / ``rmatvec`` for large grids (256^3: a
+    512^3 doubled grid), one spectrum at a time and without the three
+    meshgrid coordinate arrays: the same kernel values as
+    :func:`kernel_on_doubled_grid` (``R`` from per-axis squares added in the
+    same order), its ``fftn`` (of ``conj K`` for the adjoint), one forward
+    and one inverse transform of the field.  Restates reference
+    ``src/em3d/acoustics/operator.py:40-67`` with ``acoustics/kernel.py:21-58``."""
+    from .em import _fftn
+
+    _, cdt = precision_dtypes(precision)
+    sx, sy, sz = doubled_offsets(N, L)
+    R = np.sqrt(sx[:, None, None] * sx[:, None, None] + sy[None, :, None] * sy[None, :, None]
+                + sz[None, None, :] * sz[None, None, :])
+    is_self = R < 1e-15
+    R[is_self] = 1.0
+    ik = cdt(1j * float(k0))
+    dv = cell_volume(N, L)
+    K = (float(k0) ** 2) * dv * np.exp(ik * R) / (4.0 * np.pi * R)
+    del R
+    K[is_self] = cdt(self_cell_coefficient(float(k0), dv))
+    K = K.astype(cdt, copy=False)
+    if adjoint:
+        K = np.conj(K)
+    khat = _fftn(K).astype(cdt, copy=False)
+    del K
+    u = np.asarray(u, dtype=cdt)
+    src = u if adjoint else chi * u
+    big = _fftn(khat * _fftn(_pad(src, N)), inverse=True)
+    nx, ny, nz = N
+    y = big[:nx, :ny, :nz]
+    if adjoint:
+        y = np.conj(chi) * y
+    return (u - y).astype(cdt, copy=False)
+
+
 def rmatvec(chi, v, khat_conj, N):
     """Restates ``AcousticOperator.rmatvec`` (reference ``src/em3d/acoustics/operator.py:56-67``)."""
     cdt = khat_conj.dtype

@@ -60,6 +60,18 @@ def kernel_blocks(N, L, k: float, precision="double"):
     C1 = 3/r^2 - 3ik/r - k^2, C2 = k^2 + ik/r - 1/r^2, and the self cell
     replaced by -1/3 on the diagonal and 0 off it.
     """
+    geo = kernel_geometry(N, L, k, precision)
+    out = np.empty((3, 3) + geo["radius"].shape, dtype=geo["cdt"])
+    for r in range(3):
+        for c in range(3):
+            out[r, c] = kernel_block(geo, r, c)
+    return out
+
+
+def kernel_geometry(N, L, k: float, precision="double"):
+    """Distances, self-cell mask and the factors shared by the nine blocks.
+
+    Restates ``_kernel_geometry`` (reference ``src/em3d/operator.py:28-58``)."""
     _, cdt = precision_dtypes(precision)
     sx, sy, sz = doubled_offsets(N, L)
     dv = cell_volume(N, L)
@@ -74,21 +86,68 @@ def kernel_blocks(N, L, k: float, precision="double"):
     wg = (np.exp(ik * radius) / (4.0 * np.pi * radius) * dv).astype(cdt, copy=False)
     c1 = (3.0 * inv_r * inv_r - 3.0 * ik * inv_r - k * k).astype(cdt, copy=False)
     c2 = (k * k + ik * inv_r - inv_r * inv_r).astype(cdt, copy=False)
-    offsets = (sx, sy, sz)
+    return dict(cdt=cdt, offsets=(sx, sy, sz), radius=radius, is_self=is_self, inv_r=inv_r, wg=wg, c1=c1, c2=c2)
+
+
+def kernel_block(geo, r: int, c: int):
+    """One dyadic block (r, c) on the doubled grid.
+
+    Restates ``_kernel_block_from_geometry`` (reference ``src/em3d/operator.py:61-84``)."""
     shapes = ((-1, 1, 1), (1, -1, 1), (1, 1, -1))
-    out = np.empty((3, 3) + radius.shape, dtype=cdt)
+    offsets, inv_r, wg, is_self = geo["offsets"], geo["inv_r"], geo["wg"], geo["is_self"]
+    a_r = offsets[r].reshape(shapes[r]) * inv_r
+    a_c = offsets[c].reshape(shapes[c]) * inv_r
+    blk = wg * geo["c1"] * a_r * a_c
+    if r == c:
+        blk = blk + wg * geo["c2"]
+        blk = np.where(is_self, -1.0 / 3.0, blk)
+    else:
+        blk = np.where(is_self, 0.0, blk)
+    return blk.astype(geo["cdt"], copy=False)
+
+
+def _fftn(x, inverse: bool = False):
+    """``numpy.fft.fftn`` / ``ifftn`` over the last three axes, computed by the
+    same pocketfft library through ``scipy.fft`` on every host core (the
+    results agree with NumPy's to round-off), so that checks at 128^3 and
+    256^3 finish in seconds."""
+    import os
+
+    import scipy.fft as sfft
+
+    fn = sfft.ifftn if inverse else sfft.fftn
+    return fn(x, axes=(-3, -2, -1), workers=os.cpu_count() or 1)
+
+
+def matvec_streamed(chi, u, N, L, k: float, adjoint: bool = False, precision: str = "double"):
+    """``Operator.matvec`` (``adjoint=False``) or ``Operator.rmatvec`` with the
+    explicit adjoint spectrum (``adjoint=True``), with the block spectra built
+    one at a time as in ``_build_kernel_hat_streamed`` (reference
+    ``src/em3d/operator.py:110-138``) and applied as soon as they exist, so
+    that the full (3,3,2N,2N,2N) spectrum is never held (2.4 GB at 128^3).
+
+    matvec (reference ``operator.py:353-363``): ``u - crop(ifftn(sum_c K_rc fftn(pad(chi u)_c)))``;
+    rmatvec (``:365-398``): ``v - chi^H crop(ifftn(sum_c fftn(conj K_rc) fftn(pad v)_c))``."""
+    _, cdt = precision_dtypes(precision)
+    u = np.asarray(u)
+    src = u if adjoint else np.einsum("ab...,b...->a...", chi, u)
+    spec = [_fftn(_pad(src[c:c + 1], N)[0]) for c in range(3)]
+    geo = kernel_geometry(N, L, k, precision)
+    acc = [None, None, None]
     for r in range(3):
         for c in range(3):
-            a_r = offsets[r].reshape(shapes[r]) * inv_r
-            a_c = offsets[c].reshape(shapes[c]) * inv_r
-            blk = wg * c1 * a_r * a_c
-            if r == c:
-                blk = blk + wg * c2
-                blk = np.where(is_self, -1.0 / 3.0, blk)
-            else:
-                blk = np.where(is_self, 0.0, blk)
-            out[r, c] = blk.astype(cdt, copy=False)
-    return out
+            blk = kernel_block(geo, r, c)
+            if adjoint:
+                blk = np.conj(blk)
+            term = _fftn(blk).astype(cdt, copy=False) * spec[c]
+            acc[r] = term if acc[r] is None else acc[r] + term
+            del blk, term
+    del geo, spec
+    nx, ny, nz = N
+    y = np.stack([_fftn(acc[r], inverse=True)[:nx, :ny, :nz] for r in range(3)])
+    if adjoint:
+        y = np.einsum("ab...,b...->a...", np.conj(chi).swapaxes(0, 1), y)
+    return (u - y).astype(cdt, copy=False)
 
 
 def kernel_hat(N, L, k: float, precision="double", adjoint: bool = False):

@@ -1,7 +1,7 @@
 """Generate ``gamma0.json``: the reference's spectrum localisation and its
 coarse-operator gamma0 estimates, by running the unmodified reference em3d.
 
-    python tests/golden/make_gamma0_golden.py /root/reference/src
+    python tests/golden/make_gamma0_golden.py <reference checkout>/src
 
 Spectrum cases are seeded point sets (clusters, a ring around the origin, two
 points, a single repeated point); problem cases reuse the committed input

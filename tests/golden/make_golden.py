@@ -3,7 +3,7 @@
 Run from the repository root, in a container where the reference source is
 available read-only:
 
-    python tests/golden/make_golden.py /root/reference/src
+    python tests/golden/make_golden.py <reference checkout>/src
 
 It imports the UNMODIFIED reference package (qwerty29544/em3d v0.8.0) from the
 given path, runs its own public functions on seeded inputs, and writes small

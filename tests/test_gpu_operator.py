@@ -80,6 +80,7 @@ def test_em_kernel_hat_full_matches_reference(tag, prec):
     tol = 1e-12 if prec == "double" else 1e-5
     assert rel_err(be.to_host(pk.kernel_hat), g[f"kernel_hat_{prec}"]) < tol
     assert rel_err(be.to_host(pk.kernel_hat_adjoint), g[f"kernel_hat_adjoint_{prec}"]) < tol
+    pk.release_full_spectra()  # the octant alone is what the operator keeps
     assert pk.persistent_nbytes < g[f"kernel_hat_{prec}"].nbytes
 
 
@@ -369,3 +370,84 @@ def test_tma_field_slab_completes(prec):
             set_xpass_variant(-1)
         torch.cuda.synchronize()
         assert int(op.workspace(2)[-256:].view(torch.int32)[0]) == 0
+
+
+def test_lost_transfer_count_raises_and_resets():
+    """The give-up count at the end of the apply workspace (bounded waits on
+    TMA transfers that never completed) turns into ``NativeError`` in the
+    public matvec / rmatvec and in a solve.  The count is planted from the
+    host; nothing is made to fail on the device."""
+    import torch
+    import em3d_b200 as e
+    from em3d_b200 import _lib
+    from em3d_b200.solvers import BiCGStab, MixedBiCGStab, SolverConfig
+
+    g = golden("em_aniso12.npz")
+    be, grid, prob = _em_problem(g, "double")
+    op = e.Operator(prob)
+    ref = op.matvec(prob.wave)
+    for adjoint in (False, True):
+        op.status_word(1).fill_(3)
+        with pytest.raises(_lib.NativeError, match="3 bounded wait"):
+            op.rmatvec(prob.wave) if adjoint else op.matvec(prob.wave)
+        assert int(op.status_word(1).item()) == 0  # reset: the operator stays usable
+    assert rel_err(be.to_host(op.matvec(prob.wave)), be.to_host(ref)) == 0.0
+    # a solve reads the count together with its done flag
+    op.status_word(1).fill_(1)
+    with pytest.raises(_lib.NativeError, match="bounded wait"):
+        BiCGStab(SolverConfig(max_iter=50, rtol=1e-8)).solve(op, prob.wave)
+    op32 = op.with_precision(e.Precision.SINGLE)
+    op32.status_word(1).fill_(2)
+    with pytest.raises(_lib.NativeError, match="bounded wait"):
+        MixedBiCGStab(SolverConfig(max_iter=50, rtol=1e-8)).solve(op, prob.wave, operator_low=op32)
+    res = MixedBiCGStab(SolverConfig(max_iter=50, rtol=1e-8)).solve(op, prob.wave, operator_low=op32)
+    assert res.converged
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("kind", ["em", "acoustic"])
+def test_fp32_twin_spectrum_is_the_complex64_build(kind):
+    """``with_precision`` rounds the FP64 spectrum instead of rebuilding it;
+    the bytes equal those of a complex64 build."""
+    import torch
+    import em3d_b200 as e
+    from em3d_b200 import acoustics as ea
+
+    N = (12, 10, 16)
+    be64, be32 = _be("double"), _be("single")
+    g64 = e.Grid(N=N, L=(1.0, 0.9, 1.1), center=(0.0, 0.0, 0.0), backend=be64)
+    g32 = e.Grid(N=N, L=(1.0, 0.9, 1.1), center=(0.0, 0.0, 0.0), backend=be32)
+    if kind == "em":
+        chi = torch.randn((3, 3) + N, dtype=torch.complex128, device="cuda") * 0.3
+        u = torch.randn((3,) + N, dtype=torch.complex128, device="cuda")
+        op64 = e.Operator(e.Problem(grid=g64, eps_tensor=chi, wave=u, k0=7.0, volume=1.0))
+        twin = op64.with_precision(e.Precision.SINGLE)
+        built = e.PreparedEMKernel.build(g32, k=7.0)
+        assert torch.equal(twin.prepared_kernel.spectrum, built.spectrum)
+        assert twin.prepared_kernel.precision == "single"
+    else:
+        eta = (1.0 + torch.rand(N, dtype=torch.complex128, device="cuda")).contiguous()
+        op64 = ea.AcousticOperator(ea.make_acoustic_problem(g64, eta, k0=9.0))
+        twin = op64.with_precision(e.Precision.SINGLE)
+        built = ea.AcousticOperator(ea.make_acoustic_problem(g32, eta.to(torch.complex64), k0=9.0))
+        assert torch.equal(twin._spectrum, built._spectrum)
+        u = torch.randn(N, dtype=torch.complex128, device="cuda")
+    y64 = op64.matvec(u)
+    y32 = twin.matvec(u.to(be32.precision.torch_complex))
+    assert rel_err(be32.to_host(y32), be64.to_host(y64)) < 1e-5
+
+
+def test_persistent_nbytes_counts_materialised_full_spectra():
+    import em3d_b200 as e
+
+    g = golden("em_kernel_hat_4x3x3.npz")
+    N, L, k = tuple(int(v) for v in g["N"]), tuple(float(v) for v in g["L"]), float(g["k"])
+    grid = e.Grid(N=N, L=L, center=(0.0, 0.0, 0.0), backend=_be("double"))
+    pk = e.PreparedEMKernel.build(grid, k=k)
+    octant = pk.persistent_nbytes
+    full = pk.kernel_hat
+    assert pk.persistent_nbytes == octant + full.numel() * full.element_size()
+    pk.kernel_hat_adjoint
+    assert pk.persistent_nbytes == octant + 2 * full.numel() * full.element_size()
+    pk.release_full_spectra()
+    assert pk.persistent_nbytes == octant

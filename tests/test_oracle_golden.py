@@ -187,3 +187,29 @@ def test_twostep_two_update_recurrence():
     det = a00 * a11 - a01 * a01
     t, h = (b0 * a11 - b1 * a01) / det, (a00 * b1 - a01 * b0) / det
     assert np.allclose(out["u"], u1 - t * (u1 - u0) - h * g1, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("case", ["aniso12", "odd567", "sphere16"])
+@pytest.mark.parametrize("prec", ["double", "single"])
+def test_streamed_em_oracle_matches_reference(case, prec):
+    """The block-at-a-time oracle (used at 96^3 and 128^3 on the GPU box)
+    against the reference's own matvec / explicit-adjoint rmatvec."""
+    g = golden(f"em_{case}.npz")
+    N, L, k = tuple(int(v) for v in g["N"]), tuple(float(v) for v in g["L"]), float(g["k"])
+    tol = 1e-13 if prec == "double" else 2e-6
+    chi, u = g[f"chi_{prec}"], g[f"u_{prec}"]
+    assert rel_err(oem.matvec_streamed(chi, u, N, L, k, precision=prec), g[f"matvec_u_{prec}"]) < tol
+    assert rel_err(oem.matvec_streamed(chi, u, N, L, k, adjoint=True, precision=prec),
+                   g[f"rmatvec_u_{prec}"]) < tol
+
+
+@pytest.mark.parametrize("case", ["sphere332", "spheres16", "odd765"])
+def test_streamed_acoustic_oracle_matches_reference(case):
+    """The lean acoustic oracle (used at 256^3 on the GPU box) against the
+    reference's own matvec and rmatvec."""
+    g = golden(f"ac_{case}.npz")
+    N, L, k0 = tuple(int(v) for v in g["N"]), tuple(float(v) for v in g["L"]), float(g["k0"])
+    chi = g["eta_double"] - 1.0
+    u = g["u_double"]
+    assert rel_err(oac.matvec_streamed(chi, u, N, L, k0), g["matvec_u_double"]) < 1e-13
+    assert rel_err(oac.matvec_streamed(chi, u, N, L, k0, adjoint=True), g["rmatvec_u_double"]) < 1e-13
