@@ -26,9 +26,11 @@ independent replicas (weak scaling) and reports the total solve rate.
 
 ``--impl reference`` times the reference's own NumPy CPU path (the installed
 copy in baseline/_ref when importable, otherwise the CPU oracle port) on the
-first scene: each step is one complex128 ``Operator.matvec``, converted to
-solves/s with the mean matvec count of the FP64 BiCGStab solves of these
-scenes measured on B200.
+first scene: the reference's unmodified BiCGStab first solves it once to true
+rtol 1e-6 (its matvec count, status, true residual and wall time are
+reported), then each timed step is one complex128 ``Operator.matvec``; the
+line's value is 1 / (median matvec time x that solve's matvec count), marked
+``"extrapolated": true``, with the directly measured solve time beside it.
 """
 from __future__ import annotations
 
@@ -49,11 +51,9 @@ RTOL = 1e-6
 METRIC = "time_to_true_rtol1e-6_128^3_mixed+nn_solves_per_s"
 UNIT = "solves/s"
 SCENE_SEEDS = list(range(10000, 10008))
-# Mean FP64 BiCGStab matvecs per solve to true rtol 1e-6 of the scenes a
-# default run times (seeds 10000..10007, each twice; measured on B200 by this
-# script's fp64 leg); used only by the reference arm to convert a CPU matvec
-# timing into solves/s.
-FP64_MATVECS_PER_SOLVE = 23.375
+# The configuration both arms report (the driver compares the two lines'
+# ``config``); what each arm runs is under ``solver`` / ``cpu_baseline``.
+CONFIG = {"workload": f"warmstart_heldout_scenes_{N_GRID}^3", "scenes": SCENE_SEEDS, "rtol_true": RTOL}
 # dram__bytes_read.sum + dram__bytes_write.sum per complex64 EM matvec at
 # 128^3 (all five passes, default x-pass variant) from an ncu launch list of
 # the same operator (-k regex:kf_, second matvec of the run).
@@ -64,6 +64,12 @@ def byte_model(n: int, c: int) -> int:
     """Algorithmic bytes of one EM matvec with the octant spectrum:
     66 N^3 c (field, contrast and intermediate passes) + 6 (N+1)^3 c (spectrum)."""
     return 66 * n ** 3 * c + 6 * (n + 1) ** 3 * c
+
+
+def acoustic_byte_model(n: int, c: int) -> int:
+    """Algorithmic bytes of one acoustic matvec with the octant spectrum:
+    20 N^3 c (field, contrast and intermediate passes) + (N+1)^3 c (spectrum)."""
+    return 20 * n ** 3 * c + (n + 1) ** 3 * c
 
 
 def load_peaks():
@@ -181,8 +187,11 @@ def max_over_ranks(world, value: float) -> float:
 # reference / CPU legs
 # ---------------------------------------------------------------------------
 
-def reference_matvec_timer(case):
-    """Return (callable doing one complex128 matvec on the CPU, kind, build_s)."""
+def reference_matvec_timer(case, with_solver: bool = False):
+    """Return (callable doing one complex128 matvec on the CPU, kind, build_s,
+    solve) where ``solve()`` (with ``with_solver``) runs the reference's own
+    BiCGStab to true rtol 1e-6 on the case and returns (result, seconds,
+    true relative residual)."""
     import numpy as np
 
     ref_dir = os.path.join(ROOT, "baseline", "_ref")
@@ -198,15 +207,36 @@ def reference_matvec_timer(case):
             pk = em3d.PreparedEMKernel.build(grid, k=case.k0, include_adjoint=False, build_strategy="streamed")
             build_s = time.perf_counter() - t0
             op = em3d.Operator(prob, prepared_kernel=pk)
-            return (lambda: op.matvec(case.wave)), "reference", build_s
+
+            def solve():
+                t1 = time.perf_counter()
+                res = em3d.BiCGStab(em3d.SolverConfig(max_iter=2000, rtol=RTOL)).solve(op, case.wave)
+                dt = time.perf_counter() - t1
+                r = op.matvec(res.u) - case.wave
+                return res, dt, float(np.linalg.norm(r) / np.linalg.norm(case.wave))
+
+            return (lambda: op.matvec(case.wave)), "reference", build_s, solve
         except Exception:
             pass
     from oracle import em as oem
+    from oracle import solvers as osol
 
     t0 = time.perf_counter()
     kh = oem.kernel_hat(case.N, case.L, case.k0)
     build_s = time.perf_counter() - t0
-    return (lambda: oem.matvec(case.chi, case.wave, kh, case.N)), "port", build_s
+
+    def mv(x):
+        return oem.matvec(case.chi, x, kh, case.N)
+
+    def solve_port():
+        from types import SimpleNamespace
+
+        t1 = time.perf_counter()
+        res = SimpleNamespace(**osol.bicgstab(mv, case.wave, max_iter=2000, rtol=RTOL))
+        dt = time.perf_counter() - t1
+        return res, dt, float(np.linalg.norm(mv(res.u) - case.wave) / np.linalg.norm(case.wave))
+
+    return (lambda: mv(case.wave)), "port", build_s, solve_port
 
 
 def scene_case(seed: int, n: int = N_GRID):
@@ -232,7 +262,11 @@ def run_reference(args, world, rank):
     import numpy as np
 
     case = scene_case(SCENE_SEEDS[0])
-    fn, kind, build_s = reference_matvec_timer(case)
+    fn, kind, build_s, solve = reference_matvec_timer(case, with_solver=True)
+    # one full solve with the reference's own BiCGStab (untimed by the
+    # steps): its matvec count converts the step timings into solves/s
+    res, solve_s, true_rel = solve()
+    mps = int(res.matvec_count)
     for _ in range(args.warmup):
         fn()
     times = []
@@ -241,20 +275,24 @@ def run_reference(args, world, rank):
         fn()
         times.append(time.perf_counter() - t0)
     t_mv = float(np.median(times))
-    mps = FP64_MATVECS_PER_SOLVE
     value = 1.0 / (t_mv * mps)
     sample = (f"one complex128 Operator.matvec per step on scene {SCENE_SEEDS[0]} at {N_GRID}^3 (NumPy, "
-              f"single-threaded FFT), x {mps} matvecs per FP64 BiCGStab solve to true rtol {RTOL} (mean over "
-              f"the benchmark scenes, measured on B200); kernel build {build_s:.1f} s excluded")
+              f"single-threaded FFT) x {mps} matvecs, the count of the reference's own BiCGStab solve of that "
+              f"scene to true rtol {RTOL} run once in this process (status {res.status}, {res.iterations} "
+              f"iterations, true residual {true_rel:.2e}, {solve_s:.1f} s); kernel build {build_s:.1f} s excluded")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mv * 1e3 * mps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": f"warmstart_heldout_scenes_{N_GRID}^3", "scene": SCENE_SEEDS[0], "rtol_true": RTOL,
-                   "precision": "complex128", "solver": "reference NumPy matvec x FP64 BiCGStab matvec count"},
+        "config": CONFIG,
+        "solver": "reference NumPy complex128 BiCGStab (matvec time x its measured matvec count)",
+        "extrapolated": True,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_matvec_s": t_mv,
+        "reference_solve": {"scene": SCENE_SEEDS[0], "seconds": solve_s, "solves_per_s": 1.0 / solve_s,
+                            "matvec_count": mps, "iterations": int(res.iterations), "status": res.status,
+                            "true_relative_residual": true_rel},
     }
     print(json.dumps(line), flush=True)
 
@@ -313,6 +351,13 @@ def run_ours(args, world, rank, local):
         op64 = e.Operator(prob)
         scenes.append((prob, op64, op64.with_precision(e.Precision.SINGLE)))
     K = len(scenes)
+    # x-pass choice per operator (tile width, threads, radix plan, pipelining), timed on the operators
+    from em3d_b200.tune import autotune
+
+    tuning = {"fp32": autotune(scenes[0][2]), "fp64": autotune(scenes[0][1])}
+    for _, o64_, o32_ in scenes:
+        autotune(o64_)
+        autotune(o32_)
     cfg = SolverConfig(max_iter=2000, rtol=RTOL)
     dc = MixedBiCGStab(cfg)
     dc.max_cached = K + 1
@@ -402,6 +447,8 @@ def run_ours(args, world, rank, local):
     p2 = e.Problem(grid=g2, eps_tensor=case.chi, wave=case.wave, k0=case.k0, volume=1.0)
     a64 = e.Operator(p2)
     a32 = a64.with_precision(e.Precision.SINGLE)
+    autotune(a64)
+    autotune(a32)
     dc2 = MixedBiCGStab(cfg)
     bic2 = BiCGStab(cfg)
     for _ in range(2):
@@ -449,6 +496,8 @@ def run_ours(args, world, rank, local):
     p3 = e.Problem(grid=g3, eps_tensor=c3.chi, wave=c3.wave, k0=c3.k0, volume=1.0)
     o64 = e.Operator(p3)
     o32 = o64.with_precision(e.Precision.SINGLE)
+    autotune(o64)
+    tuning["multi_rhs_fp32_batch32"] = autotune(o32, batch=32)
     dirs3 = workloads.fibonacci_directions(64)
     waves3 = torch.empty((128, 3) + c3.N, dtype=torch.complex128, device=dev)
     for i, d3 in enumerate(dirs3):
@@ -527,22 +576,43 @@ def run_ours(args, world, rank, local):
     pA = ea.make_acoustic_problem(gA, workloads.acoustic_spheres_device(gA, count=200, seed=0), k0=20.0)
     oA64 = ea.AcousticOperator(pA)
     oA32 = oA64.with_precision(e.Precision.SINGLE)
+    tuning["acoustic_fp32"] = autotune(oA32)
+    tuning["acoustic_fp64"] = autotune(oA64)
     mxA, bA, tA = MixedBiCGStab(cfg), BiCGStab(cfg), TwoStep(cfg)
+    dcA = DefectCorrection(cfg, inner="twostep")
     acoustic = {"workload": "acoustic_200_spheres_256^3", "k0": 20.0}
     for name, fn in (("mixed", lambda: mxA.solve(oA64, pA.wave, operator_low=oA32)),
                      ("fp64_bicgstab", lambda: bA.solve(oA64, pA.wave)),
-                     ("fp64_twostep", lambda: tA.solve(oA64, pA.wave))):
+                     ("fp64_twostep", lambda: tA.solve(oA64, pA.wave)),
+                     ("mixed_twostep", lambda: dcA.solve(oA64, pA.wave, operator_low=oA32))):
         fn()
         t_ms, rA = _events_ms(fn)
         acoustic[name] = {"ms": t_ms, "iterations": rA.iterations, "status": rA.status,
                           "true_residual": float(true_relative_residual(oA64, rA.u, pA.wave))}
+        if name == "mixed_twostep":
+            acoustic[name].update(outer_iterations=rA.outer_iterations, fp64_matvecs=rA.fp64_matvecs,
+                                  fp32_matvecs=rA.fp32_matvecs, fp32_rmatvecs=rA.fp32_rmatvecs)
         if name == "mixed":
             uA = rA.u
     farfield.pattern_plane(uA, pA, plane="xz", n_angles=360)
     pat_ms, _ = _events_ms(lambda: farfield.pattern_plane(uA, pA, plane="xz", n_angles=360))
     acoustic["pattern_xz_360_ms"] = pat_ms
     acoustic["speedup_mixed_vs_fp64_bicgstab"] = acoustic["fp64_bicgstab"]["ms"] / acoustic["mixed"]["ms"]
-    del oA64, oA32, mxA, bA, tA, uA
+    acoustic["speedup_mixed_twostep_vs_fp64_twostep"] = (acoustic["fp64_twostep"]["ms"]
+                                                          / acoustic["mixed_twostep"]["ms"])
+    # the acoustic operator's roofline: octant byte model 20 N^3 c + (N+1)^3 c
+    peak_a, _ = load_peaks()
+    for prec_name, opA, c in (("fp32", oA32, 8), ("fp64", oA64, 16)):
+        xa = opA.problem.wave
+        oa = torch.empty_like(xa)
+        for _ in range(3):
+            opA.apply_into(xa, oa)
+        ms_a, _ = _events_ms(lambda: [opA.apply_into(xa, oa) for _ in range(10)])
+        ms_a /= 10
+        ba = acoustic_byte_model(256, c)
+        acoustic[f"matvec_{prec_name}"] = {"ms": ms_a, "bytes": ba, "gbs": ba / (ms_a * 1e-3) / 1e9,
+                                          "frac": ba / (ms_a * 1e-3) / 1e9 / peak_a}
+    del oA64, oA32, mxA, bA, tA, dcA, uA
     torch.cuda.empty_cache()
 
     # -- 5. matvec timing (dominant kernel): CUDA events on the launching stream
@@ -565,7 +635,7 @@ def run_ours(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        fn, kind, build_s = reference_matvec_timer(scene_case(SCENE_SEEDS[0]))
+        fn, kind, build_s, _ = reference_matvec_timer(scene_case(SCENE_SEEDS[0]))
         fn()
         t0 = time.perf_counter()
         fn()
@@ -589,13 +659,14 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 inner / c128 outer, bf16 network", "data": "synthetic",
-        "config": {"workload": f"warmstart_heldout_scenes_{N_GRID}^3", "scenes": SCENE_SEEDS, "rtol_true": RTOL,
-                   "solver": "network guess (network on the 64^3 grid, output interpolated to 128^3) + FP32 BiCGStab with FP64 reliable updates (true residual in FP64)",
-                   "network": {"layers": 4, "width": 32, "modes": 12, "train_scenes": args.train_scenes,
-                               "train_grid": 64, "eval_grid": N_GRID // 2, "epochs": args.epochs, "loss_first_last": [hist[0], hist[-1]],
-                               "generate_s": gen_s, "train_s": train_s},
-                   "parallelism": f"replicas x{world}",
-                   "l2": "each solve's operator, fields and workspaces (~2 GB) exceed the 126 MB L2"},
+        "config": CONFIG,
+        "solver": "network guess (network on the 64^3 grid, output interpolated to 128^3) + FP32 BiCGStab with "
+                  "FP64 reliable updates (true residual in FP64)",
+        "network": {"layers": 4, "width": 32, "modes": 12, "train_scenes": args.train_scenes,
+                    "train_grid": 64, "eval_grid": N_GRID // 2, "epochs": args.epochs,
+                    "loss_first_last": [hist[0], hist[-1]], "generate_s": gen_s, "train_s": train_s},
+        "parallelism": f"replicas x{world}",
+        "l2": "each solve's operator, fields and workspaces (~2 GB) exceed the 126 MB L2",
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT,
                 "h2d_bytes_per_step": int(host_rhs[0].numel() * host_rhs[0].element_size()),
                 "d2h_bytes_per_step": int(host_u.numel() * host_u.element_size())},
@@ -606,6 +677,7 @@ def run_ours(args, world, rank, local):
         "clocks": clocks,
         "clocks_comparison_legs": leg_clocks,
         "gpu_launches": launches,
+        "autotune_ms": {k: {str(v): t for v, t in d.items()} for k, d in tuning.items()},
         "mixed_nn": summary(res_nn),
         "fp64": dict(summary(res64), ms=fp64_ms, solves_per_s=world * 1000.0 / fp64_ms),
         "mixed_zero": dict(summary(res0), ms=zero_ms, solves_per_s=world * 1000.0 / zero_ms),

@@ -123,7 +123,7 @@ class AcousticOperator(_Applier):
             g, ws = _build_workspace(grid)
             dt = self._be.precision.native_dtype
             nbytes = _lib.load().em3d_spectrum_bytes(ctypes_ref(g), _lib.EM3D_ACOUSTIC, dt)
-            spec = _uint8(nbytes, self._be.torch_device)
+            spec = _uint8(nbytes, self._be.torch_device).zero_()  # alignment padding is deterministic
             _lib.call("em3d_acoustic_spectrum_build", ctypes_ref(g), float(problem.k0), dt, spec.data_ptr(),
                       ws.data_ptr(), ws.numel(), _lib.stream_handle())
             del ws

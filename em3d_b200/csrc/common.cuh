@@ -29,6 +29,20 @@ template <typename C> __host__ __device__ __forceinline__ C cmulcj(C a, C b) {
   C r; r.x = a.x * b.x + a.y * b.y; r.y = a.x * b.y - a.y * b.x; return r;
 }
 template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+
+// Complex add / subtract for the FFT butterflies: one packed FP32x2
+// instruction (sm_100's FADD2: two lanes per issue slot, each rounded like a
+// scalar add) for complex64, the scalar pair for complex128.  Used where both
+// operands are plain complex values; sums involving a value multiplied by
+// +-i mix the lanes and stay scalar.
+template <typename C> __device__ __forceinline__ C vadd(C a, C b) { return cadd(a, b); }
+template <typename C> __device__ __forceinline__ C vsub(C a, C b) { return csub(a, b); }
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+template <> __device__ __forceinline__ float2 vadd<float2>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 vsub<float2>(float2 a, float2 b) {
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));
+}
+#endif
 template <typename C, typename S> __host__ __device__ __forceinline__ C cscale(C a, S s) { a.x *= s; a.y *= s; return a; }
 // multiply by -i (forward) or +i (inverse)
 template <typename C> __host__ __device__ __forceinline__ C mul_mi(C a) { C r; r.x = a.y; r.y = -a.x; return r; }

@@ -59,13 +59,16 @@ template <bool INV, typename C> __device__ __forceinline__ C rot_q(C a) {  // ti
   return INV ? mul_pi(a) : mul_mi(a);
 }
 
+// Butterfly sums use vadd / vsub (packed FP32x2 for complex64) wherever both
+// operands are plain complex values; a sum with a value multiplied by -+i
+// mixes real and imaginary lanes and uses the scalar cadd / csub.
 template <bool INV, typename C> __device__ __forceinline__ void dft2(C& a0, C& a1) {
-  C t = a0; a0 = cadd(t, a1); a1 = csub(t, a1);
+  C t = a0; a0 = vadd(t, a1); a1 = vsub(t, a1);
 }
 
 template <bool INV, typename C> __device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3) {
-  C t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = rot_q<INV>(csub(a1, a3));
-  a0 = cadd(t0, t2); a2 = csub(t0, t2); a1 = cadd(t1, t3); a3 = csub(t1, t3);
+  C t0 = vadd(a0, a2), t1 = vsub(a0, a2), t2 = vadd(a1, a3), t3 = rot_q<INV>(vsub(a1, a3));
+  a0 = vadd(t0, t2); a2 = vsub(t0, t2); a1 = cadd(t1, t3); a3 = csub(t1, t3);
 }
 
 // radix 8 = two radix 4 on even/odd inputs, combined with w8^q
@@ -81,10 +84,10 @@ template <bool INV, typename C> __device__ __forceinline__ void dft8(C* a) {
   if (!INV) { w1 = mk<R>(h * (o1.x + o1.y), h * (o1.y - o1.x)); w3 = mk<R>(h * (o3.y - o3.x), -h * (o3.x + o3.y)); }
   else      { w1 = mk<R>(h * (o1.x - o1.y), h * (o1.y + o1.x)); w3 = mk<R>(-h * (o3.x + o3.y), h * (o3.x - o3.y)); }
   C w2 = rot_q<INV>(o2);
-  a[0] = cadd(e0, o0); a[4] = csub(e0, o0);
-  a[1] = cadd(e1, w1); a[5] = csub(e1, w1);
+  a[0] = vadd(e0, o0); a[4] = vsub(e0, o0);
+  a[1] = vadd(e1, w1); a[5] = vsub(e1, w1);
   a[2] = cadd(e2, w2); a[6] = csub(e2, w2);
-  a[3] = cadd(e3, w3); a[7] = csub(e3, w3);
+  a[3] = vadd(e3, w3); a[7] = vsub(e3, w3);
 }
 
 // radix 16 = two radix 8 on even/odd inputs, combined with w16^q
@@ -103,11 +106,16 @@ template <bool INV, typename C> __device__ __forceinline__ void dft16(C* a) {
   for (int q = 0; q < 8; ++q) {
     // w16^q = cos(2 pi q/16) -+ i sin(2 pi q/16); q = 0 and q = 4 are exact
     C t;
+    if (q == 4) {
+      t = rot_q<INV>(o[4]);
+      a[q] = cadd(e[q], t);
+      a[q + 8] = csub(e[q], t);
+      continue;
+    }
     if (q == 0) t = o[0];
-    else if (q == 4) t = rot_q<INV>(o[4]);
     else t = cmul(o[q], mk<R>(cs[q], INV ? sn[q] : -sn[q]));
-    a[q] = cadd(e[q], t);
-    a[q + 8] = csub(e[q], t);
+    a[q] = vadd(e[q], t);
+    a[q + 8] = vsub(e[q], t);
   }
 }
 
@@ -121,7 +129,7 @@ template <int RX, bool INV, typename C> __device__ __forceinline__ void dft_fixe
   } else if constexpr (RX == 4) {
     C a0 = a[0], a1 = a[1];
     C w1 = rot_q<INV>(a1);
-    a[0] = cadd(a0, a1); a[2] = cadd(a0, w1); a[1] = csub(a0, a1); a[3] = csub(a0, w1);
+    a[0] = vadd(a0, a1); a[2] = cadd(a0, w1); a[1] = vsub(a0, a1); a[3] = csub(a0, w1);
     // natural order: y0 = E0, y1 = O0, y2 = E1, y3 = O1
     C y0 = a[0], y1 = a[2], y2 = a[1], y3 = a[3];
     a[0] = y0; a[1] = y1; a[2] = y2; a[3] = y3;
@@ -159,30 +167,30 @@ template <int RX, bool INV, typename C> __device__ __forceinline__ void dft_fixe
 template <bool INV, typename C> __device__ __forceinline__ void dft3(C& a0, C& a1, C& a2) {
   using R = decltype(a0.x);
   const R s = (R)0.86602540378443864676;  // sqrt(3)/2
-  C t = cadd(a1, a2), d = csub(a1, a2);
+  C t = vadd(a1, a2), d = vsub(a1, a2);
   C m = mk<R>(a0.x - (R)0.5 * t.x, a0.y - (R)0.5 * t.y);
-  a0 = cadd(a0, t);
+  a0 = vadd(a0, t);
   // forward: y1 = m - i s d, y2 = m + i s d
   C isd = mk<R>(-s * d.y, s * d.x);  // i s d
-  if (!INV) { a1 = csub(m, isd); a2 = cadd(m, isd); }
-  else      { a1 = cadd(m, isd); a2 = csub(m, isd); }
+  if (!INV) { a1 = vsub(m, isd); a2 = vadd(m, isd); }
+  else      { a1 = vadd(m, isd); a2 = vsub(m, isd); }
 }
 
 template <bool INV, typename C> __device__ __forceinline__ void dft5(C* a) {
   using R = decltype(a[0].x);
   const R c1 = (R)0.30901699437494742410, c2 = (R)-0.80901699437494742410;
   const R s1 = (R)0.95105651629515357212, s2 = (R)0.58778525229247312917;
-  C t1 = cadd(a[1], a[4]), t2 = cadd(a[2], a[3]);
-  C d1 = csub(a[1], a[4]), d2 = csub(a[2], a[3]);
+  C t1 = vadd(a[1], a[4]), t2 = vadd(a[2], a[3]);
+  C d1 = vsub(a[1], a[4]), d2 = vsub(a[2], a[3]);
   C a0 = a[0];
   C b1 = mk<R>(a0.x + c1 * t1.x + c2 * t2.x, a0.y + c1 * t1.y + c2 * t2.y);
   C b2 = mk<R>(a0.x + c2 * t1.x + c1 * t2.x, a0.y + c2 * t1.y + c1 * t2.y);
   C e1 = mk<R>(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y);
   C e2 = mk<R>(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y);
   C ie1 = mk<R>(-e1.y, e1.x), ie2 = mk<R>(-e2.y, e2.x);
-  a[0] = cadd(a0, cadd(t1, t2));
-  if (!INV) { a[1] = csub(b1, ie1); a[4] = cadd(b1, ie1); a[2] = csub(b2, ie2); a[3] = cadd(b2, ie2); }
-  else      { a[1] = cadd(b1, ie1); a[4] = csub(b1, ie1); a[2] = cadd(b2, ie2); a[3] = csub(b2, ie2); }
+  a[0] = vadd(a0, vadd(t1, t2));
+  if (!INV) { a[1] = vsub(b1, ie1); a[4] = vadd(b1, ie1); a[2] = vsub(b2, ie2); a[3] = vadd(b2, ie2); }
+  else      { a[1] = vadd(b1, ie1); a[4] = vsub(b1, ie1); a[2] = vadd(b2, ie2); a[3] = vsub(b2, ie2); }
 }
 
 // cos and sin of 2 pi m / n for n in {6, 10, 12} (compile-time m): the

@@ -123,8 +123,8 @@ extern "C" {
 
 int em3d_set_tuning(int key, int value) {
   if (key < 0 || key >= EM3D_TUNE_COUNT) { em3d_set_last_error("unknown tuning key"); return EM3D_ERR_INVALID; }
-  if (key == EM3D_TUNE_XPASS_VARIANT && (value < -1 || value > 6)) {
-    em3d_set_last_error("x-pass variant must be -1 (automatic) or 0 .. 6");
+  if (key == EM3D_TUNE_XPASS_VARIANT && (value < -1 || value > 10)) {
+    em3d_set_last_error("x-pass variant must be -1 (automatic) or 0 .. 10");
     return EM3D_ERR_INVALID;
   }
   if (key == EM3D_TUNE_FNO_SIMT && value != 0 && value != 1) {

@@ -28,6 +28,7 @@
 #include "common.cuh"
 #include "fft.cuh"
 #include "passes_fast.cuh"
+#include "passes_x.cuh"
 
 namespace em3d {
 
@@ -771,11 +772,11 @@ static int go_xmul(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d,
   return EM3D_OK;
 }
 
-template <typename R, int L, int C, bool ADJ, int E, int NTT, bool TMAF>
+template <typename R, int L, int C, bool ADJ, int E, int NTT, bool TMAF, int MINB = 1>
 static int go_xpipe(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
                     cudaStream_t st, BatchStrides bs) {
   using G = XpipeGeom<L, E, C, NTT>;
-  auto kern = kf_xmul_pipe<R, L, C, ADJ, E, NTT, TMAF>;
+  auto kern = kf_xmul_pipe<R, L, C, ADJ, E, NTT, TMAF, MINB>;
   EM3D_CUDA_TRY(allow_smem(kern));
   const size_t smem = (size_t)G::TOTAL * sizeof(cx<R>) + G::BYTES_EXTRA;
   const int ntz = (2 * d.nz + G::P - 1) / G::P;
@@ -814,6 +815,49 @@ static int go_xpipe(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d
   return EM3D_OK;
 }
 
+// T2 as 8-byte words (2 Nz W, 2 Ny, batch C Nx), one box of P W words x 1 x
+// Nx per component and tile (see go_xpipe).
+template <typename R, int C, int P>
+static int encode_field_map(CUtensorMap* fmap, cx<R>* T2, const Dims& d, int batch) {
+  auto enc = tensor_map_encoder();
+  if (enc == nullptr) { em3d_set_last_error("cuTensorMapEncodeTiled is unavailable"); return EM3D_ERR_CUDA; }
+  constexpr cuuint64_t W = sizeof(cx<R>) / 8;
+  const cuuint64_t dims[3] = {(cuuint64_t)2 * d.nz * W, (cuuint64_t)2 * d.ny, (cuuint64_t)batch * C * d.nx};
+  const cuuint64_t strides[2] = {(cuuint64_t)2 * d.nz * sizeof(cx<R>), (cuuint64_t)4 * d.ny * d.nz * sizeof(cx<R>)};
+  const cuuint32_t box[3] = {(cuuint32_t)(P * W), 1u, (cuuint32_t)d.nx};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  memset(fmap, 0, sizeof *fmap);
+  const CUresult r = enc(fmap, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, (void*)T2, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) { em3d_set_last_error("cuTensorMapEncodeTiled rejected the field slab map"); return EM3D_ERR_CUDA; }
+  return EM3D_OK;
+}
+
+template <typename R, int L, int C, bool ADJ, int E, int NTT, bool ROT>
+static int go_xrot(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
+                   cudaStream_t st, BatchStrides bs) {
+  using G = XrotGeom<L, E, C, NTT>;
+  static_assert(G::P % 2 == 0 && L / 2 <= 256, "TMA field slab: even tile width, at most 256 rows per box");
+  auto kern = kf_xmul_rot<R, L, C, ADJ, E, NTT, ROT>;
+  EM3D_CUDA_TRY(allow_smem(kern));
+  const size_t smem = (size_t)G::TOTAL * sizeof(cx<R>) + G::BYTES_EXTRA;
+  const int ntz = (2 * d.nz + G::P - 1) / G::P;
+  const long long ntiles = (long long)(batch / xpipe_entries_per_unit(batch, bs.spec == 0)) * (d.ny + 1) * ntz;
+  int sms = 0;
+  EM3D_CUDA_TRY(sm_count(&sms));
+  int per_sm = 0;
+  EM3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, G::NT, smem));
+  if (per_sm < 1) per_sm = 1;
+  const long long grid = std::min<long long>(ntiles, (long long)sms * per_sm);
+  if (grid <= 0) return EM3D_OK;
+  CUtensorMap fmap;
+  if (int rc = encode_field_map<R, C, G::P>(&fmap, T2, d, batch)) return rc;
+  kern<<<(unsigned)grid, G::NT, smem, st>>>(T2, spec, tw, d.ny, d.nz, ntz, batch, bs, skip, fmap, bs.status);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
 template <typename R, int L, bool ADJ, int E>
 static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& d, int batch, const int* skip,
                      cudaStream_t st, BatchStrides bs) {
@@ -832,15 +876,21 @@ static int go_xsplit(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const Dims& 
 // in registers, 256-thread CTAs; 1 = the same with 128-thread CTAs (two per
 // SM); 2 = component-split threads (EM only); 3 = persistent CTAs with the
 // next tile's field and spectrum prefetched by cp.async, 256 threads; 4 = the
-// same with 128 threads; 5 and 6 = 3 and 4 with the field slab loaded by TMA.
-// -1 (the default) picks, per operator kind and x length, the fastest
-// measured on B200: EM 6 (both precisions; 128^3, 96^3, 80^3); acoustic 5 on
-// 512-point axes (256^3) and 0 on shorter ones (128^3).
+// same with 128 threads; 5 and 6 = 3 and 4 with the field slab loaded by TMA;
+// 7, 8 and 9 = 6 with register twiddles and single-barrier exchanges
+// (kf_xmul_rot; plans equal to their reverse only): 7 with one copy of the
+// transform code rotating the three components, 8 without, 9 = 8 with
+// 256-thread CTAs; 10 = 6 with 8 elements per thread (complex64, power-of-two
+// axes) in 256-thread CTAs limited to 128 registers, two per SM.  -1 (the
+// default) picks, per operator kind and x length, the fastest
+// measured on B200: EM 6 (both precisions; 128^3, 96^3, 80^3); acoustic 9 on
+// 512-point axes (256^3: 1.35 vs 1.36-1.54 ms for variant 5 in complex64, 2.46
+// vs 2.67-3.03 ms in complex128) and 0 on shorter ones (128^3).
 static int xmul_variant(int C, int L) {
   const int v = g_tuning[EM3D_TUNE_XPASS_VARIANT];
   if (v >= 0) return v;
   if (C == 3) return 6;
-  return L >= 512 ? 5 : 0;
+  return L >= 512 ? 9 : 0;
 }
 
 // Shared memory of each x-pass variant; a variant that does not fit in the
@@ -856,6 +906,12 @@ static size_t xvariant_smem(int v) {
     case 2: return C == 3 ? (size_t)(L + 3 * XsplitGeom<L, E>::REGION) * sizeof(cx<R>) : ~(size_t)0;
     case 3: case 5: return (size_t)XpipeGeom<L, E, C, 256>::TOTAL * sizeof(cx<R>) + 16;
     case 4: case 6: return (size_t)XpipeGeom<L, E, C, 128>::TOTAL * sizeof(cx<R>) + 16;
+    case 7: case 8:
+      return SymPlan<L, E>::symmetric() ? (size_t)XrotGeom<L, E, C, 128>::TOTAL * sizeof(cx<R>) + 16 : ~(size_t)0;
+    case 9: return SymPlan<L, E>::symmetric() ? (size_t)XrotGeom<L, E, C, 256>::TOTAL * sizeof(cx<R>) + 16 : ~(size_t)0;
+    case 10:
+      return (sizeof(R) == 4 && (L & (L - 1)) == 0) ? (size_t)XpipeGeom<L, 8, C, 256>::TOTAL * sizeof(cx<R>) + 16
+                                                     : ~(size_t)0;
   }
   return ~(size_t)0;
 }
@@ -878,6 +934,15 @@ static int launch_xmul_len(cx<R>* T2, const cx<R>* spec, const cx<R>* tw, const 
   if (v == 4) return go_xpipe<R, L, C, ADJ, EB, 128, false>(T2, spec, tw, d, batch, skip, st, bs);
   if (v == 5) return go_xpipe<R, L, C, ADJ, EB, 256, true>(T2, spec, tw, d, batch, skip, st, bs);
   if (v == 6) return go_xpipe<R, L, C, ADJ, EB, 128, true>(T2, spec, tw, d, batch, skip, st, bs);
+  if constexpr (SymPlan<L, EB>::symmetric()) {
+    if (v == 7) return go_xrot<R, L, C, ADJ, EB, 128, true>(T2, spec, tw, d, batch, skip, st, bs);
+    if (v == 8) return go_xrot<R, L, C, ADJ, EB, 128, false>(T2, spec, tw, d, batch, skip, st, bs);
+    if (v == 9) return go_xrot<R, L, C, ADJ, EB, 256, false>(T2, spec, tw, d, batch, skip, st, bs);
+  }
+  if constexpr (sizeof(R) == 4 && (L & (L - 1)) == 0) {
+    // 8 elements per thread, two 256-thread CTAs per SM (16 warps)
+    if (v == 10) return go_xpipe<R, L, C, ADJ, 8, 256, true, 2>(T2, spec, tw, d, batch, skip, st, bs);
+  }
   if (v == 1) return go_xmul<R, L, C, ADJ, EB, 128>(T2, spec, tw, d, batch, skip, st, bs);
   return go_xmul<R, L, C, ADJ, EB, 256>(T2, spec, tw, d, batch, skip, st, bs);
 }

@@ -411,8 +411,8 @@ template <int L, int E, int C, int NTT> struct XpipeGeom {
 // TMAF: the field slab arrives by TMA (one tile load per component, issued by
 // thread 0 and completed on an mbarrier; `fmap` describes T2 as (kz words,
 // ky, batch * C * Nx rows)) instead of per-thread cp.async copies.
-template <typename R, int L, int C, bool ADJ, int E, int NTT, bool TMAF>
-__global__ void __launch_bounds__(XpipeGeom<L, E, C, NTT>::NT)
+template <typename R, int L, int C, bool ADJ, int E, int NTT, bool TMAF, int MINB = 1>
+__global__ void __launch_bounds__(XpipeGeom<L, E, C, NTT>::NT, MINB)
 kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
              int nb, BatchStrides bs, const int* skip, const __grid_constant__ CUtensorMap fmap, int* status) {
   using T = cx<R>;

@@ -22,7 +22,7 @@ from typing import Sequence
 import numpy as np
 
 from . import _lib
-from .operator import _build_workspace, _uint8, ctypes_ref, raise_on_failed_waits, status_word
+from .operator import _build_workspace, _uint8, ctypes_ref, raise_on_failed_waits, status_word, tuned
 
 
 def _align(n: int, a: int = 256) -> int:
@@ -99,11 +99,19 @@ class _Group:
             raise ValueError(f"a group of {len(self)} problems applies to {len(self)} fields of shape "
                              f"{self._field_shape()}, got shape {tuple(x.shape)}")
         ws = self.workspace(len(self))
-        _lib.call(self._names[1 if adjoint else 0], ctypes_ref(self._grid_c), self._dt, len(self),
-                  self._spectra.data_ptr(), self._stride, self._chis.data_ptr(), x.data_ptr(), out.data_ptr(),
-                  ws.data_ptr(), ws.numel(), skip_ptr, entry_done[0] if entry_done else None,
-                  int(entry_done[1]) if entry_done else 0, _lib.stream_handle(stream))
+        with tuned(self.xpass_variant):
+            _lib.call(self._names[1 if adjoint else 0], ctypes_ref(self._grid_c), self._dt, len(self),
+                      self._spectra.data_ptr(), self._stride, self._chis.data_ptr(), x.data_ptr(), out.data_ptr(),
+                      ws.data_ptr(), ws.numel(), skip_ptr, entry_done[0] if entry_done else None,
+                      int(entry_done[1]) if entry_done else 0, _lib.stream_handle(stream))
         return out
+
+    # x-pass choice of ``em3d_b200.tune.autotune`` (None: the process-wide setting)
+    xpass_variant = None
+
+    def _grid_key(self):
+        g = self._grid_c
+        return (g.nx, g.ny, g.nz, g.lx, g.ly, g.lz)
 
     def status_word(self, batch: int = 0):
         """Device int32 counting the failed bounded waits of this group's

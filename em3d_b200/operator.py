@@ -43,10 +43,36 @@ def convert_spectrum(spectrum, grid: Grid, kind: int, src_precision, dst_precisi
     nbytes = _lib.load().em3d_spectrum_bytes(ctypes_ref(g), kind, dst_precision.native_dtype)
     if nbytes == 0:
         _lib.check(_lib.EM3D_ERR_INVALID, "em3d_spectrum_bytes")
-    out = _uint8(nbytes, spectrum.device)
+    out = _uint8(nbytes, spectrum.device).zero_()  # alignment padding is deterministic
     _lib.call("em3d_spectrum_convert", ctypes_ref(g), kind, src_precision.native_dtype, spectrum.data_ptr(),
               dst_precision.native_dtype, out.data_ptr(), _lib.stream_handle())
     return out
+
+
+class tuned:
+    """Context that selects an operator's autotuned x-pass choice for the
+    launches inside it and restores the process-wide setting afterwards
+    (``None``: leave the setting alone)."""
+
+    def __init__(self, choice):
+        self.choice = choice
+        self.saved = None
+
+    def __enter__(self):
+        if self.choice is not None:
+            from .tune import apply_choice
+
+            lib = _lib.load()
+            self.saved = (int(lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT)),
+                          int(lib.em3d_get_tuning(_lib.EM3D_TUNE_FFT_GENERIC)))
+            apply_choice(self.choice)
+        return self
+
+    def __exit__(self, *exc):
+        if self.saved is not None:
+            _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_XPASS_VARIANT, self.saved[0])
+            _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, self.saved[1])
+        return False
 
 
 def _build_workspace(grid: Grid):
@@ -121,7 +147,7 @@ class PreparedEMKernel:
         g, ws = _build_workspace(grid)
         dt = be.precision.native_dtype
         nbytes = _lib.load().em3d_spectrum_bytes(ctypes_ref(g), _lib.EM3D_EM, dt)
-        spec = _uint8(nbytes, be.torch_device)
+        spec = _uint8(nbytes, be.torch_device).zero_()  # alignment padding is deterministic
         _lib.call("em3d_em_spectrum_build", ctypes_ref(g), float(k), dt, spec.data_ptr(), ws.data_ptr(),
                   ws.numel(), _lib.stream_handle())
         del ws
@@ -258,9 +284,18 @@ class _Applier:
         b = self._batch_of(x)
         ws = self.workspace(b)
         name = self._native_names[1 if adjoint else 0]
-        _lib.call(name, ctypes_ref(self._grid_c), self._dt, b, self._spectrum.data_ptr(), self._chi.data_ptr(),
-                  x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(), skip_ptr, _lib.stream_handle(stream))
+        with tuned(self.xpass_variant):
+            _lib.call(name, ctypes_ref(self._grid_c), self._dt, b, self._spectrum.data_ptr(), self._chi.data_ptr(),
+                      x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(), skip_ptr, _lib.stream_handle(stream))
         return out
+
+    # x-pass implementation chosen for this operator by ``em3d_b200.tune.autotune``
+    # (None: the library's process-wide setting)
+    xpass_variant = None
+
+    def _grid_key(self):
+        g = self._grid_c
+        return (g.nx, g.ny, g.nz, g.lx, g.ly, g.lz)
 
     def _apply_checked(self, x, out, adjoint: bool = False):
         """``apply_into`` followed by :meth:`check_status`: the public

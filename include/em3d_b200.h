@@ -56,11 +56,15 @@ const char* em3d_last_error(void);
  * in the reference, which has no native code to tune.
  * ------------------------------------------------------------------------ */
 enum em3d_tune_key {
-  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: EM 6, acoustic 5 at 512 points, else 0), 0 register 256-thread, 1 register
+  EM3D_TUNE_XPASS_VARIANT = 0, /* x pass: -1 automatic (default: EM 6, acoustic 9 at 512 points, else 0), 0 register 256-thread, 1 register
                                    128-thread, 2 component-split, 3 persistent cp.async-pipelined 256-thread,
                                    4 the same 128-thread, 5 and 6 = 3 and 4 with the field slab loaded by
-                                   TMA; a variant whose shared memory does not fit is
-                                   replaced by the first that fits in the order 6, 4, 1, 2, 0, 5, 3 */
+                                   TMA, 7 / 8 / 9 = 6 with register twiddles and single-barrier exchanges
+                                   (component loop / inlined components / 256 threads; plans equal to their
+                                   reverse), 10 = 6 with 8 elements per thread in two 256-thread CTAs per SM
+                                   (complex64, power-of-two axes); a variant that does not apply or whose
+                                   shared memory does not fit is replaced by the first that fits in the
+                                   order 6, 4, 1, 2, 0, 5, 3 */
   EM3D_TUNE_FFT_GENERIC = 1,   /* 1 = use the generic shared-memory FFT passes for every axis length */
   EM3D_TUNE_FNO_SIMT = 2,      /* 1 = FNO row pass on CUDA cores even where the tensor-core one applies */
   EM3D_TUNE_FNO_CONTRACT = 3,  /* FNO truncated-DFT contractions: 0 automatic, else outputs per thread (2, 4, 8, 12, 24) */

@@ -101,8 +101,24 @@ def test_tuning_keys_validate_without_gpu():
 
     lib = _lib.load()
     assert lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT) == -1   # automatic by default
-    assert lib.em3d_set_tuning(_lib.EM3D_TUNE_XPASS_VARIANT, 7) == _lib.EM3D_ERR_INVALID
+    assert lib.em3d_set_tuning(_lib.EM3D_TUNE_XPASS_VARIANT, 11) == _lib.EM3D_ERR_INVALID
     assert "variant" in _lib.last_error()
-    for v in (5, 6, 3, 4, 0, -1):
+    for v in (5, 6, 3, 4, 7, 8, 9, 10, 0, -1):
         assert lib.em3d_set_tuning(_lib.EM3D_TUNE_XPASS_VARIANT, v) == 0
         assert lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT) == v
+
+
+def test_tuned_context_restores_the_process_setting():
+    from em3d_b200 import _lib
+    from em3d_b200.operator import tuned
+
+    lib = _lib.load()
+    before = (lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT), lib.em3d_get_tuning(_lib.EM3D_TUNE_FFT_GENERIC))
+    with tuned(7):
+        assert lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT) == 7
+    with tuned("generic"):
+        assert lib.em3d_get_tuning(_lib.EM3D_TUNE_FFT_GENERIC) == 1
+    with tuned(None):
+        assert lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT) == before[0]
+    assert (lib.em3d_get_tuning(_lib.EM3D_TUNE_XPASS_VARIANT),
+            lib.em3d_get_tuning(_lib.EM3D_TUNE_FFT_GENERIC)) == before

@@ -217,7 +217,7 @@ def test_register_fft_path_matches_generic_path(prec, kind, monkeypatch):
         _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 1)
         gen_mv, gen_rmv = op.matvec(u), op.rmatvec(u)
         _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 0)
-        for v in (0, 1, 2, 3, 4, 5, 6):
+        for v in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10):
             set_xpass_variant(v)
             fast_mv, fast_rmv = op.matvec(u), op.rmatvec(u)
             assert rel_err(be.to_host(fast_mv), be.to_host(gen_mv)) < tol, (N, v)
@@ -254,7 +254,7 @@ def test_mixed_radix_register_path_matches_generic_path(prec, kind):
         gen_mv, gen_rmv = op.matvec(u), op.rmatvec(u)
         _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FFT_GENERIC, 0)
         try:
-            for v in (-1, 0, 1, 2, 3, 4, 5, 6):
+            for v in (-1, 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10):
                 set_xpass_variant(v)
                 fast_mv, fast_rmv = op.matvec(u), op.rmatvec(u)
                 assert rel_err(be.to_host(fast_mv), be.to_host(gen_mv)) < tol, (N, v)
@@ -327,7 +327,7 @@ def test_batched_matvec_equals_single_register_path(N, prec):
     tol = 1e-14 if prec == "double" else 1e-6
     from em3d_b200.tune import set_xpass_variant
 
-    for v in (0, 3, 4):
+    for v in (0, 3, 4, 7, 8):
         set_xpass_variant(v)
         Y, Ya = op.matvec(U), op.rmatvec(U)
         for b in range(7):
@@ -362,7 +362,7 @@ def test_tma_field_slab_completes(prec):
         try:
             set_xpass_variant(3)
             ref, ref_a = op.matvec(u), op.rmatvec(u)
-            for v in (5, 6):
+            for v in (5, 6, 7, 8, 9, 10):
                 set_xpass_variant(v)
                 assert rel_err(be.to_host(op.matvec(u)), be.to_host(ref)) < tol, (N, v)
                 assert rel_err(be.to_host(op.rmatvec(u)), be.to_host(ref_a)) < tol, (N, v)
