@@ -23,6 +23,9 @@ EM3D_C64 = 0
 EM3D_C128 = 1
 EM3D_ACOUSTIC = 1
 EM3D_EM = 3
+EM3D_CHI_ISOTROPIC = 1
+EM3D_CHI_SYMMETRIC = 6
+EM3D_CHI_FULL = 9
 EM3D_TUNE_XPASS_VARIANT = 0
 EM3D_TUNE_FFT_GENERIC = 1
 EM3D_TUNE_FNO_SIMT = 2
@@ -55,6 +58,10 @@ SIGNATURES = {
                                c_void_p, c_void_p]),
     "em3d_em_rmatvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
                                 c_void_p, c_void_p]),
+    "em3d_em_matvec_chi": (c_int, [_GRID, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                   c_size_t, c_void_p, c_void_p]),
+    "em3d_em_rmatvec_chi": (c_int, [_GRID, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_size_t, c_void_p, c_void_p]),
     "em3d_acoustic_matvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                      c_size_t, c_void_p, c_void_p]),
     "em3d_acoustic_rmatvec": (c_int, [_GRID, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
@@ -169,6 +176,8 @@ def check(status: int, what: str) -> None:
 # kernels each entry point launches (the operator passes count five)
 LAUNCHES = {
     "em3d_em_matvec": 5, "em3d_em_rmatvec": 5, "em3d_acoustic_matvec": 5, "em3d_acoustic_rmatvec": 5,
+    "em3d_em_matvec_chi": 5, "em3d_em_rmatvec_chi": 5, "em3d_em_matvec_grouped": 5, "em3d_em_rmatvec_grouped": 5,
+    "em3d_acoustic_matvec_grouped": 5, "em3d_acoustic_rmatvec_grouped": 5,
 }
 # Kernels launched by this process (graph replays add their captured counts).
 # Host threads update it under a lock; a thread that is capturing a graph

@@ -67,7 +67,12 @@ struct BatchStrides {
   size_t done_stride;
   int outer;
   int* status;  // this application's status words (bounded waits that gave up), or null
+  int chi_layout = 9;  // EM contrast components stored per cell: 9 (full), 6 (symmetric) or 1 (isotropic)
 };
+
+// Index of entry (r, c) of a symmetric 3x3 contrast stored as its six
+// distinct entries xx yy zz xy xz yz.
+__host__ __device__ constexpr int sym_index(int r, int c) { return r == c ? r : 2 + r + c; }
 
 __device__ __forceinline__ bool entry_done(const BatchStrides& bs, int b) {
   return bs.done != nullptr && *(volatile const int*)(bs.done + (size_t)b * bs.done_stride) != 0;

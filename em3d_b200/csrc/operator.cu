@@ -89,6 +89,28 @@ static int apply_grouped(const em3d_grid* g, int dtype, int batch, const void* s
   return apply<double, C, ADJ>(d, batch, spectra, chis, u, out, ws, wsb, skip, st, bs);
 }
 
+// EM application with the contrast stored as 9, 6 (symmetric) or 1
+// (isotropic) components per cell.
+template <bool ADJ>
+static int em_apply_layout(const em3d_grid* g, int dtype, int batch, const void* spectrum, int chi_layout,
+                           const void* chi, const void* u, void* out, void* ws, size_t wsb, const int* skip,
+                           void* stream) {
+  Dims d;
+  int rc = check_grid(g, &d);
+  if (rc) return rc;
+  if (chi_layout != EM3D_CHI_FULL && chi_layout != EM3D_CHI_SYMMETRIC && chi_layout != EM3D_CHI_ISOTROPIC) {
+    em3d_set_last_error("chi_layout must be EM3D_CHI_FULL (9), EM3D_CHI_SYMMETRIC (6) or EM3D_CHI_ISOTROPIC (1)");
+    return EM3D_ERR_INVALID;
+  }
+  BatchStrides bs{};
+  bs.chi_layout = chi_layout;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == EM3D_C64) return apply<float, 3, ADJ>(d, batch, spectrum, chi, u, out, ws, wsb, skip, st, bs);
+  if (dtype == EM3D_C128) return apply<double, 3, ADJ>(d, batch, spectrum, chi, u, out, ws, wsb, skip, st, bs);
+  em3d_set_last_error("dtype must be EM3D_C64 or EM3D_C128");
+  return EM3D_ERR_INVALID;
+}
+
 template <typename S, typename D> __global__ void k_round_copy(const S* __restrict__ src, D* __restrict__ dst, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     dst[i] = from_c64<decltype(dst[0].x)>(to_c64(src[i]));
@@ -253,6 +275,18 @@ int em3d_acoustic_rmatvec_grouped(const em3d_grid* g, int dtype, int batch, cons
     size_t entry_done_stride, void* stream) {
   return apply_grouped<1, true>(g, dtype, batch, spectra, spectrum_stride, chis, v, out, ws, wsb, skip, entry_done,
                                  entry_done_stride, stream);
+}
+
+int em3d_em_matvec_chi(const em3d_grid* g, int dtype, int batch, const void* spectrum, int chi_layout,
+                       const void* chi, const void* u, void* out, void* ws, size_t wsb, const int* skip,
+                       void* stream) {
+  return em_apply_layout<false>(g, dtype, batch, spectrum, chi_layout, chi, u, out, ws, wsb, skip, stream);
+}
+
+int em3d_em_rmatvec_chi(const em3d_grid* g, int dtype, int batch, const void* spectrum, int chi_layout,
+                        const void* chi, const void* v, void* out, void* ws, size_t wsb, const int* skip,
+                        void* stream) {
+  return em_apply_layout<true>(g, dtype, batch, spectrum, chi_layout, chi, v, out, ws, wsb, skip, stream);
 }
 
 int em3d_em_matvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi, const void* u,

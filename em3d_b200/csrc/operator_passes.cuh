@@ -96,8 +96,9 @@ template <typename C> __device__ __forceinline__ void load_twiddles(C* tws, cons
   for (int i = threadIdx.x; i < L; i += blockDim.x) tws[i] = twg[i];
 }
 
-enum { LD_PLAIN = 0, LD_EM_CHI = 1, LD_AC_CHI = 2 };
-enum { ST_PLAIN = 0, ST_SUB = 1, ST_EM_ADJ = 2, ST_AC_ADJ = 3 };
+// Load / store modes of the generic row pass (see FLD_* / FST_* in passes_fast.cuh).
+enum { LD_PLAIN = 0, LD_EM_CHI = 1, LD_AC_CHI = 2, LD_EM_CHI6 = 3, LD_EM_CHI1 = 4 };
+enum { ST_PLAIN = 0, ST_SUB = 1, ST_EM_ADJ = 2, ST_AC_ADJ = 3, ST_EM_ADJ6 = 4, ST_EM_ADJ1 = 5 };
 
 // Rows along the contiguous axis.  Row g of batch b, component c lives at
 // ((b*C + c) * rows_pb + row) * len.
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(kThreads) k_rows(const cx<R>* in, const cx<R>*
     for (int c = 0; c < C; ++c) v[c] = mk<R>(0, 0);
     if (g < nrows && !row_done(g)) {
       const int b = g / rows_pb, row = g - b * rows_pb;
-      if constexpr (LD == LD_EM_CHI) {
+      if constexpr (LD == LD_EM_CHI || LD == LD_EM_CHI6) {
         T uu[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) uu[c] = in[((size_t)(b * 3 + c) * rows_pb + row) * Lin + k];
@@ -143,9 +144,16 @@ __global__ void __launch_bounds__(kThreads) k_rows(const cx<R>* in, const cx<R>*
         for (int a = 0; a < 3; ++a) {
           T acc = mk<R>(0, 0);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) acc = cadd(acc, cmul((chi + (size_t)b * bs.chi)[((size_t)(a * 3 + c) * rows_pb + row) * Lin + k], uu[c]));
+          for (int c = 0; c < 3; ++c) {
+            const int ci = LD == LD_EM_CHI ? a * 3 + c : sym_index(a, c);
+            acc = cadd(acc, cmul((chi + (size_t)b * bs.chi)[((size_t)ci * rows_pb + row) * Lin + k], uu[c]));
+          }
           v[a] = acc;
         }
+      } else if constexpr (LD == LD_EM_CHI1) {
+        const T s = (chi + (size_t)b * bs.chi)[(size_t)row * Lin + k];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = cmul(s, in[((size_t)(b * 3 + c) * rows_pb + row) * Lin + k]);
       } else if constexpr (LD == LD_AC_CHI) {
         v[0] = cmul((chi + (size_t)b * bs.chi)[(size_t)row * Lin + k], in[((size_t)b * rows_pb + row) * Lin + k]);
       } else {
@@ -180,15 +188,24 @@ __global__ void __launch_bounds__(kThreads) k_rows(const cx<R>* in, const cx<R>*
         const size_t o = ((size_t)(b * C + c) * rows_pb + row) * Lout + k;
         out[o] = csub(base[o], y[c]);
       }
-    } else if constexpr (ST == ST_EM_ADJ) {
+    } else if constexpr (ST == ST_EM_ADJ || ST == ST_EM_ADJ6) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         T acc = mk<R>(0, 0);
 #pragma unroll
-        for (int c = 0; c < 3; ++c)  // (chi^H)[a][c] = conj((chi + (size_t)b * bs.chi)[c][a])
-          acc = cadd(acc, cmulcj((chi + (size_t)b * bs.chi)[((size_t)(c * 3 + a) * rows_pb + row) * Lout + k], y[c]));
+        for (int c = 0; c < 3; ++c) {  // (chi^H)[a][c] = conj(chi[c][a])
+          const int ci = ST == ST_EM_ADJ ? c * 3 + a : sym_index(c, a);
+          acc = cadd(acc, cmulcj((chi + (size_t)b * bs.chi)[((size_t)ci * rows_pb + row) * Lout + k], y[c]));
+        }
         const size_t o = ((size_t)(b * 3 + a) * rows_pb + row) * Lout + k;
         out[o] = csub(base[o], acc);
+      }
+    } else if constexpr (ST == ST_EM_ADJ1) {
+      const T s = (chi + (size_t)b * bs.chi)[(size_t)row * Lout + k];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const size_t o = ((size_t)(b * 3 + a) * rows_pb + row) * Lout + k;
+        out[o] = csub(base[o], cmulcj(s, y[a]));
       }
     } else if constexpr (ST == ST_AC_ADJ) {
       const size_t o = ((size_t)b * rows_pb + row) * Lout + k;
@@ -999,13 +1016,23 @@ int apply(const Dims& d, int batch, const void* spectrum, const void* chi, const
   constexpr int FLDF = C == 3 ? FLD_EM_CHI : FLD_AC_CHI;
   constexpr int STA = C == 3 ? ST_EM_ADJ : ST_AC_ADJ;
   constexpr int FSTA = C == 3 ? FST_EM_ADJ : FST_AC_ADJ;
-  // pass 1: rows along z, chi applied on load (matvec) or plain (rmatvec)
+  // pass 1: rows along z, chi applied on load (matvec) or plain (rmatvec);
+  // an EM contrast stored as 6 or 1 components per cell has its own load mode
+  const int chil = C == 3 ? bs.chi_layout : 9;
   if (fz) {
-    if (!ADJ) rc = launch_rows_fast<R, C, FLDF, FST_PLAIN, false>(Lz, uu, ch, nullptr, T1, twz, rows, nrows, skip, st, bs);
-    else rc = launch_rows_fast<R, C, FLD_PLAIN, FST_PLAIN, false>(Lz, uu, nullptr, nullptr, T1, twz, rows, nrows, skip, st, bs);
+    if (ADJ) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_PLAIN, false>(Lz, uu, nullptr, nullptr, T1, twz, rows, nrows, skip, st, bs);
+    else if constexpr (C == 3) {
+      if (chil == 6) rc = launch_rows_fast<R, C, FLD_EM_CHI6, FST_PLAIN, false>(Lz, uu, ch, nullptr, T1, twz, rows, nrows, skip, st, bs);
+      else if (chil == 1) rc = launch_rows_fast<R, C, FLD_EM_CHI1, FST_PLAIN, false>(Lz, uu, ch, nullptr, T1, twz, rows, nrows, skip, st, bs);
+      else rc = launch_rows_fast<R, C, FLDF, FST_PLAIN, false>(Lz, uu, ch, nullptr, T1, twz, rows, nrows, skip, st, bs);
+    } else rc = launch_rows_fast<R, C, FLDF, FST_PLAIN, false>(Lz, uu, ch, nullptr, T1, twz, rows, nrows, skip, st, bs);
   } else {
-    if (!ADJ) rc = launch_rows<R, C, LDF, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st, bs);
-    else rc = launch_rows<R, C, LD_PLAIN, ST_PLAIN, false>(uu, nullptr, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st, bs);
+    if (ADJ) rc = launch_rows<R, C, LD_PLAIN, ST_PLAIN, false>(uu, nullptr, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st, bs);
+    else if constexpr (C == 3) {
+      if (chil == 6) rc = launch_rows<R, C, LD_EM_CHI6, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st, bs);
+      else if (chil == 1) rc = launch_rows<R, C, LD_EM_CHI1, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st, bs);
+      else rc = launch_rows<R, C, LDF, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st, bs);
+    } else rc = launch_rows<R, C, LDF, ST_PLAIN, false>(uu, ch, nullptr, T1, twz, Lz, rows, nrows, d.nz, Lz, skip, st, bs);
   }
   if (rc) return rc;
   // pass 2: (batch*C*Nx, Ny, 2Nz) -> (batch*C*Nx, 2Ny, 2Nz)
@@ -1023,10 +1050,18 @@ int apply(const Dims& d, int batch, const void* spectrum, const void* chi, const
   // pass 5: rows along z, crop and combine
   if (fz) {
     if (!ADJ) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_SUB, true>(Lz, T1, nullptr, uu, o, twz, rows, nrows, skip, st, bs);
-    else rc = launch_rows_fast<R, C, FLD_PLAIN, FSTA, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st, bs);
+    else if constexpr (C == 3) {
+      if (chil == 6) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_EM_ADJ6, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st, bs);
+      else if (chil == 1) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_EM_ADJ1, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st, bs);
+      else rc = launch_rows_fast<R, C, FLD_PLAIN, FSTA, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st, bs);
+    } else rc = launch_rows_fast<R, C, FLD_PLAIN, FSTA, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st, bs);
   } else {
     if (!ADJ) rc = launch_rows<R, C, LD_PLAIN, ST_SUB, true>(T1, nullptr, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st, bs);
-    else rc = launch_rows<R, C, LD_PLAIN, STA, true>(T1, ch, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st, bs);
+    else if constexpr (C == 3) {
+      if (chil == 6) rc = launch_rows<R, C, LD_PLAIN, ST_EM_ADJ6, true>(T1, ch, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st, bs);
+      else if (chil == 1) rc = launch_rows<R, C, LD_PLAIN, ST_EM_ADJ1, true>(T1, ch, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st, bs);
+      else rc = launch_rows<R, C, LD_PLAIN, STA, true>(T1, ch, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st, bs);
+    } else rc = launch_rows<R, C, LD_PLAIN, STA, true>(T1, ch, uu, o, twz, Lz, rows, nrows, Lz, d.nz, skip, st, bs);
   }
   return rc;
 }

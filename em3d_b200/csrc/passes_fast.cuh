@@ -12,8 +12,12 @@
 
 namespace em3d {
 
-enum { FLD_PLAIN = 0, FLD_EM_CHI = 1, FLD_AC_CHI = 2 };
-enum { FST_PLAIN = 0, FST_SUB = 1, FST_EM_ADJ = 2, FST_AC_ADJ = 3 };
+// Row-pass load modes: plain, chi u with the EM contrast stored as 9
+// (full), 6 (symmetric: xx yy zz xy xz yz) or 1 (isotropic: chi = s I)
+// components per cell, scalar acoustic chi u.  Store modes: plain, u - y,
+// v - chi^H y for the three EM layouts, v - conj(chi) y (acoustic).
+enum { FLD_PLAIN = 0, FLD_EM_CHI = 1, FLD_AC_CHI = 2, FLD_EM_CHI6 = 3, FLD_EM_CHI1 = 4 };
+enum { FST_PLAIN = 0, FST_SUB = 1, FST_EM_ADJ = 2, FST_AC_ADJ = 3, FST_EM_ADJ6 = 4, FST_EM_ADJ1 = 5 };
 
 // Elements per thread: power-of-two axes 16 (complex64) or 8 (complex128);
 // mixed axes 12 (3 x 2^k) or 20 (5 x 2^k).
@@ -78,6 +82,15 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
           const T* ub = in + (size_t)b * 3 * cs;
 #pragma unroll
           for (int k = 0; k < 3; ++k) v = cadd(v, cmul(chb[(size_t)(c * 3 + k) * cs + o], ub[k * cs + o]));
+        } else if constexpr (LD == FLD_EM_CHI6) {
+          const size_t o = (size_t)row * LIN + pos;
+          const size_t cs = (size_t)rows_pb * LIN;
+          const T* ub = in + (size_t)b * 3 * cs;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) v = cadd(v, cmul(chb[(size_t)sym_index(c, k) * cs + o], ub[k * cs + o]));
+        } else if constexpr (LD == FLD_EM_CHI1) {
+          const size_t o = (size_t)row * LIN + pos;
+          v = cmul(chb[o], in[((size_t)(b * 3 + c) * rows_pb) * LIN + o]);
         } else if constexpr (LD == FLD_AC_CHI) {
           v = cmul(chb[(size_t)row * LIN + pos], in[((size_t)b * rows_pb + row) * LIN + pos]);
         } else {
@@ -91,7 +104,7 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
   const LayRows lay{pen * G::PSTRIDE, G::PSTRIDE};
   reg_fft<L, E, INV, false, 1, !INV>(a, t, sm, tw, lay);
 
-  if constexpr (ST == FST_EM_ADJ) {
+  if constexpr (ST == FST_EM_ADJ || ST == FST_EM_ADJ6) {
     // v - chi^H y needs all three components of y at each z: stage y through
     // shared memory (the last exchange ended with a sync).
 #pragma unroll
@@ -114,7 +127,8 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           const T yk = sm[(k * RPB + rl) * G::PSTRIDE + pos + (pos >> 4)];
-          acc = cadd(acc, cmulcj(chb[(size_t)(k * 3 + c) * cs + o], yk));
+          const int ci = ST == FST_EM_ADJ ? k * 3 + c : sym_index(k, c);
+          acc = cadd(acc, cmulcj(chb[(size_t)ci * cs + o], yk));
         }
         const size_t oo = (size_t)(b * 3 + c) * cs + o;
         out[oo] = csub(base[oo], acc);
@@ -134,7 +148,8 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
         const size_t oo = ((size_t)(b * C + c) * rows_pb + row) * LOUT + pos;
         if constexpr (ST == FST_PLAIN) out[oo] = y;
         else if constexpr (ST == FST_SUB) out[oo] = csub(base[oo], y);
-        else if constexpr (ST == FST_AC_ADJ) out[oo] = csub(base[oo], cmulcj(chb[(size_t)row * LOUT + pos], y));
+        else if constexpr (ST == FST_AC_ADJ || ST == FST_EM_ADJ1)  // chi^H y = conj(s) y per component
+          out[oo] = csub(base[oo], cmulcj(chb[(size_t)row * LOUT + pos], y));
       }
     }
   }

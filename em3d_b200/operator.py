@@ -49,6 +49,24 @@ def convert_spectrum(spectrum, grid: Grid, kind: int, src_precision, dst_precisi
     return out
 
 
+def compact_contrast(chi):
+    """``(layout, tensor)``: the EM contrast (3,3,Nx,Ny,Nz) in the smallest
+    storage that holds it exactly: isotropic ``chi = s I`` as s (Nx,Ny,Nz),
+    symmetric ``chi = chi^T`` as (6,Nx,Ny,Nz) (xx yy zz xy xz yz), otherwise
+    the full tensor.  The passes that apply chi then read 1/9 or 6/9 of its
+    bytes; the problem keeps the full tensor."""
+    import torch
+
+    c = chi
+    symmetric = all(torch.equal(c[a, b], c[b, a]) for a, b in ((0, 1), (0, 2), (1, 2)))
+    if not symmetric:
+        return _lib.EM3D_CHI_FULL, c.contiguous()
+    diagonal = not any(bool(torch.any(c[a, b] != 0)) for a, b in ((0, 1), (0, 2), (1, 2)))
+    if diagonal and torch.equal(c[0, 0], c[1, 1]) and torch.equal(c[0, 0], c[2, 2]):
+        return _lib.EM3D_CHI_ISOTROPIC, c[0, 0].contiguous()
+    return _lib.EM3D_CHI_SYMMETRIC, torch.stack([c[0, 0], c[1, 1], c[2, 2], c[0, 1], c[0, 2], c[1, 2]]).contiguous()
+
+
 class tuned:
     """Context that selects an operator's autotuned x-pass choice for the
     launches inside it and restores the process-wide setting afterwards
@@ -230,10 +248,11 @@ class _Applier:
 
     _kind = _lib.EM3D_EM
 
-    def _setup_native(self, grid: Grid, spectrum, chi):
+    def _setup_native(self, grid: Grid, spectrum, chi, chi_layout: int = 9):
         self._grid_c = _lib.make_grid(grid.N, grid.L)
         self._spectrum = spectrum
         self._chi = chi.contiguous()
+        self._chi_layout = int(chi_layout)
         self._workspaces = {}
         self._dt = self._be.precision.native_dtype
         self._tc = self._be.precision.torch_complex
@@ -285,8 +304,14 @@ class _Applier:
         ws = self.workspace(b)
         name = self._native_names[1 if adjoint else 0]
         with tuned(self.xpass_variant):
-            _lib.call(name, ctypes_ref(self._grid_c), self._dt, b, self._spectrum.data_ptr(), self._chi.data_ptr(),
-                      x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(), skip_ptr, _lib.stream_handle(stream))
+            if self._chi_layout == _lib.EM3D_CHI_FULL:
+                _lib.call(name, ctypes_ref(self._grid_c), self._dt, b, self._spectrum.data_ptr(),
+                          self._chi.data_ptr(), x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(), skip_ptr,
+                          _lib.stream_handle(stream))
+            else:
+                _lib.call(name + "_chi", ctypes_ref(self._grid_c), self._dt, b, self._spectrum.data_ptr(),
+                          self._chi_layout, self._chi.data_ptr(), x.data_ptr(), out.data_ptr(), ws.data_ptr(),
+                          ws.numel(), skip_ptr, _lib.stream_handle(stream))
         return out
 
     # x-pass implementation chosen for this operator by ``em3d_b200.tune.autotune``
@@ -323,7 +348,14 @@ class Operator(_Applier):
         self._prepared_kernel = prepared_kernel
         self._be = grid.backend
         self._N = tuple(grid.N)
-        self._setup_native(grid, prepared_kernel.spectrum, problem.eps_tensor)
+        layout, chi = compact_contrast(problem.eps_tensor)
+        self._setup_native(grid, prepared_kernel.spectrum, chi, layout)
+
+    @property
+    def chi_layout(self) -> str:
+        """How the passes read the contrast: ``"isotropic"`` (chi = s I, one
+        value per cell), ``"symmetric"`` (six) or ``"full"`` (nine)."""
+        return {1: "isotropic", 6: "symmetric", 9: "full"}[self._chi_layout]
 
     @property
     def backend(self):
@@ -381,20 +413,33 @@ class Operator(_Applier):
         out = torch.empty_like(x)
         return self._apply_checked(x, out, adjoint=True)
 
+    def _flat(self, vector):
+        """A flat vector (host or device) as a device tensor of the operator's dtype."""
+        import torch
+
+        if not isinstance(vector, torch.Tensor):
+            vector = torch.as_tensor(np.asarray(vector))
+        return vector.to(device=self._be.torch_device, dtype=self._tc)
+
     def matvec_flat(self, vector):
+        """``A`` on a cell-major, component-minor flat vector (reference
+        ``src/em3d/operator.py:400-402``); returns a device vector."""
         from .layout import flatten_field, unflatten_field
 
-        return flatten_field(self.matvec(unflatten_field(vector, self._N)))
+        return flatten_field(self.matvec(unflatten_field(self._flat(vector), self._N)))
 
     def rmatvec_flat(self, vector):
+        """``A*`` on a flat vector (reference ``src/em3d/operator.py:404-406``)."""
         from .layout import flatten_field, unflatten_field
 
-        return flatten_field(self.rmatvec(unflatten_field(vector, self._N)))
+        return flatten_field(self.rmatvec(unflatten_field(self._flat(vector), self._N)))
 
     def iteration_matvec_flat(self, vector, *, mu: complex):
+        """``x - A x / mu`` (reference ``src/em3d/operator.py:408-409``)."""
         if abs(mu) == 0.0:
             raise ValueError("mu must be non-zero")
-        return vector - self.matvec_flat(vector) / complex(mu)
+        v = self._flat(vector)
+        return v - self.matvec_flat(v) / complex(mu)
 
     def to_dense_operator(self):
         raise RuntimeError("dense matrix construction requires a NumPy backend")

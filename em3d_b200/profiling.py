@@ -5,10 +5,13 @@ the benchmark step (network guess on the half-resolution grid +
 ``MixedBiCGStab`` to true rtol 1e-6 on a held-out warm-start scene, untrained
 network of the benchmark's shape) twice
 and brackets a third run with ``cudaProfilerStart/Stop`` for
-``ncu --profile-from-start off``.
+``ncu --profile-from-start off``; ``guess-curve`` times the mixed solve from
+initial guesses of controlled relative error (what a warm start must achieve
+to save iterations).
 
     python -m em3d_b200.profiling matvec --precision single --n 128
     python -m em3d_b200.profiling step --n 128 --seed 10001
+    python -m em3d_b200.profiling guess-curve --n 128 --seeds 10000,10001,10002,10003
 """
 from __future__ import annotations
 
@@ -73,9 +76,25 @@ def main(argv=None) -> int:
     s = sub.add_parser("step")
     s.add_argument("--n", type=int, default=128)
     s.add_argument("--seed", type=int, default=10001)
+    c = sub.add_parser("guess-curve", help="mixed-solve iterations and time against the relative error of "
+                                           "the initial guess (warmstart.iterations_vs_guess_error)")
+    c.add_argument("--n", type=int, default=128)
+    c.add_argument("--seeds", default="10000,10001,10002,10003")
+    c.add_argument("--out", default=None, help="JSON rows path")
     args = ap.parse_args(argv)
     if args.what == "matvec":
         print("ok", matvec(args.precision, args.n, args.reps))
+    elif args.what == "guess-curve":
+        import json
+
+        from .warmstart import iterations_vs_guess_error
+
+        rows = iterations_vs_guess_error([int(v) for v in args.seeds.split(",")], args.n)
+        for r in rows:
+            print(json.dumps(r), flush=True)
+        if args.out:
+            with open(args.out, "w") as fh:
+                json.dump(rows, fh, indent=1)
     else:
         res = step(args.n, args.seed)
         print("ok", res.iterations, res.inner_iterations, res.status)

@@ -339,6 +339,55 @@ def summarize(records: Sequence[EvalRecord]) -> dict:
     return s
 
 
+def iterations_vs_guess_error(seeds: Sequence[int], N: int = 128, *,
+                              errors=(1.0, 0.5, 0.3, 0.2, 0.1, 0.05, 0.02, 0.01, 3e-3, 1e-3, 1e-4),
+                              rtol: float = 1e-6, device_index: int = 0, noise_seed: int = 0) -> list:
+    """What a guess of a given accuracy saves: for each scene, the mixed
+    solve (FP32 BiCGStab, FP64 reliable updates) to true ``rtol`` from
+    ``x0 = u* - e ||u*|| d`` for every relative error ``e``, with ``u*`` the
+    FP64 solution (true residual 1e-10) and ``d`` a unit direction of two
+    kinds: ``"scattered"`` (along the scattered field ``u* - f``, the error a
+    network that under- or over-shoots the scattering makes; ``e`` equal to
+    ``||u* - f|| / ||u*||`` is the guess ``u = f``) and ``"white"`` (complex
+    Gaussian noise, every mode of the grid).  Rows: seed, kind, e, the guess's
+    true residual, iterations, matvecs and ms (CUDA events), beside the
+    zero-guess solve."""
+    import torch
+
+    grid = unit_grid(N, Precision.DOUBLE, device_index)
+    solver = MixedBiCGStab(SolverConfig(max_iter=4000, rtol=rtol))
+    gen = torch.Generator(device=grid.backend.torch_device).manual_seed(noise_seed)
+    rows = []
+    for seed in seeds:
+        prob = scene_problem(random_scene(seed), grid)
+        op64 = Operator(prob)
+        op32 = op64.with_precision(Precision.SINGLE)
+        f = prob.wave
+        ustar = BiCGStab(SolverConfig(max_iter=4000, rtol=1e-10)).solve(op64, f).u
+        un = torch.linalg.vector_norm(ustar)
+        scat = ustar - f
+        dirs = {"scattered": scat / torch.linalg.vector_norm(scat)}
+        w = torch.randn(ustar.shape, dtype=ustar.dtype, device=ustar.device, generator=gen)
+        dirs["white"] = w / torch.linalg.vector_norm(w)
+        solver.solve(op64, f, operator_low=op32)  # warm the engines and graphs
+        res, ms = _timed(lambda: solver.solve(op64, f, operator_low=op32), 1)
+        rows.append({"seed": int(seed), "kind": "zero", "error": 1.0, "guess_residual": 1.0,
+                     "iterations": int(res.iterations), "matvecs": int(res.matvec_count), "ms": ms,
+                     "scattered_error_of_f": float(torch.linalg.vector_norm(scat) / un)})
+        for kind, d in dirs.items():
+            for e in errors:
+                x0 = (ustar - (float(e) * un) * d).contiguous()
+                r0 = true_relative_residual(op64, x0, f)
+                solver.solve(op64, f, x0=x0, operator_low=op32)
+                res, ms = _timed(lambda: solver.solve(op64, f, x0=x0, operator_low=op32), 1)
+                rows.append({"seed": int(seed), "kind": kind, "error": float(e), "guess_residual": float(r0),
+                             "iterations": int(res.iterations), "matvecs": int(res.matvec_count), "ms": ms,
+                             "converged": bool(res.converged), "guess_rejected": bool(res.guess_rejected)})
+        del op64, op32, ustar
+        torch.cuda.empty_cache()
+    return rows
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--train", type=int, default=len(TRAIN_SEEDS), help="training scenes (seeds 0..)")

@@ -41,6 +41,11 @@ enum em3d_status {
 
 enum em3d_dtype { EM3D_C64 = 0, EM3D_C128 = 1 };
 enum em3d_kind { EM3D_ACOUSTIC = 1, EM3D_EM = 3 };
+/* Storage of an EM contrast: components per cell.  FULL is the reference's
+ * (3,3,Nx,Ny,Nz); SYMMETRIC keeps chi_xx, chi_yy, chi_zz, chi_xy, chi_xz,
+ * chi_yz as (6,Nx,Ny,Nz) for chi = chi^T (rotated anisotropic media);
+ * ISOTROPIC keeps s as (Nx,Ny,Nz) for chi = s I (isotropic media). */
+enum em3d_chi_layout { EM3D_CHI_ISOTROPIC = 1, EM3D_CHI_SYMMETRIC = 6, EM3D_CHI_FULL = 9 };
 
 /* Uniform Cartesian grid: cells per axis and box edge lengths. */
 typedef struct em3d_grid {
@@ -144,6 +149,20 @@ int em3d_em_matvec(const em3d_grid* g, int dtype, int batch, const void* spectru
  * Replaces Operator.rmatvec (src/em3d/operator.py:365-398), both adjoint storages. */
 int em3d_em_rmatvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi,
                     const void* v, void* out, void* ws, size_t ws_bytes, const int* skip, void* stream);
+
+/* em3d_em_matvec / em3d_em_rmatvec with the contrast in `chi_layout`
+ * (em3d_chi_layout).  The symmetric and isotropic storages read 6/9 and 1/9
+ * of the contrast bytes in the passes that apply chi (the first pass of a
+ * matvec, the last of an rmatvec); the result is that of the full storage
+ * of the same contrast.  Same operator as Operator.matvec / rmatvec
+ * (src/em3d/operator.py:353-398), whose Problem keeps the full tensor
+ * (src/em3d/problem.py:19-32). */
+int em3d_em_matvec_chi(const em3d_grid* g, int dtype, int batch, const void* spectrum, int chi_layout,
+                       const void* chi, const void* u, void* out, void* ws, size_t ws_bytes, const int* skip,
+                       void* stream);
+int em3d_em_rmatvec_chi(const em3d_grid* g, int dtype, int batch, const void* spectrum, int chi_layout,
+                        const void* chi, const void* v, void* out, void* ws, size_t ws_bytes, const int* skip,
+                        void* stream);
 
 /* EM matvec for callers that cannot allocate device memory (no counterpart
  * in the reference).  Same result as em3d_em_matvec with batch = 1, but the

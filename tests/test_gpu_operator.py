@@ -451,3 +451,34 @@ def test_persistent_nbytes_counts_materialised_full_spectra():
     assert pk.persistent_nbytes == octant + 2 * full.numel() * full.element_size()
     pk.release_full_spectra()
     assert pk.persistent_nbytes == octant
+
+
+@pytest.mark.parametrize("N", [(32, 16, 32), (12, 10, 9)])
+@pytest.mark.parametrize("kind", ["isotropic", "symmetric", "full"])
+def test_compact_contrast_storage_against_oracle(kind, N):
+    """The operator stores an isotropic contrast as one value per cell and a
+    symmetric one as six; matvec and rmatvec still equal the oracle's on the
+    full tensor (register passes at (32,16,32), generic at (12,10,9))."""
+    import em3d_b200 as e
+    from oracle import em as oem
+
+    rng = np.random.default_rng(21)
+    L, k = (1.0, 0.8, 1.2), 5.5
+    s = (rng.standard_normal(N) + 1j * rng.standard_normal(N)) * 0.4
+    if kind == "isotropic":
+        chi = np.einsum("ab,...->ab...", np.eye(3), s)
+    else:
+        chi = (rng.standard_normal((3, 3) + N) + 1j * rng.standard_normal((3, 3) + N)) * 0.3
+        if kind == "symmetric":
+            chi = 0.5 * (chi + chi.swapaxes(0, 1))
+    u = rng.standard_normal((3,) + N) + 1j * rng.standard_normal((3,) + N)
+    kh = oem.kernel_hat(N, L, k)
+    ref, ref_a = oem.matvec(chi, u, kh, N), oem.rmatvec(chi, u, N, khat=kh)
+    for prec, tol in (("double", 1e-12), ("single", 1e-5)):
+        be = _be(prec)
+        cdt = be.complex_dtype
+        grid = e.Grid(N=N, L=L, center=(0.0, 0.0, 0.0), backend=be)
+        op = e.Operator(e.Problem(grid=grid, eps_tensor=chi.astype(cdt), wave=u.astype(cdt), k0=k, volume=1.0))
+        assert op.chi_layout == kind
+        assert rel_err(be.to_host(op.matvec(u.astype(cdt))), ref) < tol, prec
+        assert rel_err(be.to_host(op.rmatvec(u.astype(cdt))), ref_a) < tol, prec

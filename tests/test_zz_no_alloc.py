@@ -41,8 +41,9 @@ def _static_call(op, u, out):
     from em3d_b200 import _lib
 
     g = _lib.make_grid(op.problem.grid.N, op.problem.grid.L)
+    chi = op.problem.eps_tensor.contiguous()  # the full (3,3,Nx,Ny,Nz) contrast this entry point takes
     _lib.call("em3d_em_matvec_static_scratch", ctypes.byref(g), op._dt, op._spectrum.data_ptr(),
-              op._chi.data_ptr(), u.data_ptr(), out.data_ptr(), None, _lib.stream_handle())
+              chi.data_ptr(), u.data_ptr(), out.data_ptr(), None, _lib.stream_handle())
     return out
 
 
