@@ -12,13 +12,14 @@ to save iterations).
     python -m em3d_b200.profiling matvec --precision single --n 128
     python -m em3d_b200.profiling step --n 128 --seed 10001
     python -m em3d_b200.profiling guess-curve --n 128 --seeds 10000,10001,10002,10003
+    python -m em3d_b200.profiling delta-sweep --n 128
 """
 from __future__ import annotations
 
 import argparse
 
 
-def matvec(precision: str, n: int, reps: int) -> float:
+def matvec(precision: str, n: int, reps: int, xpass_variant=None) -> float:
     import torch
 
     from . import workloads
@@ -31,6 +32,8 @@ def matvec(precision: str, n: int, reps: int) -> float:
     grid = Grid(N=case.N, L=case.L, center=case.center, backend=be)
     prob = Problem(grid=grid, eps_tensor=case.chi, wave=case.wave, k0=case.k0, volume=1.0)
     op = Operator(prob)
+    if xpass_variant is not None:
+        op.xpass_variant = xpass_variant
     out = torch.empty_like(prob.wave)
     for _ in range(reps):
         op.apply_into(prob.wave, out)
@@ -66,6 +69,41 @@ def step(n: int, seed: int):
     return res
 
 
+def delta_sweep(n: int, seeds, deltas) -> list:
+    """MixedBiCGStab to true rtol 1e-6 on the warm-start scenes for each
+    reliable-update threshold ``delta`` (the FP32 residual reduction after
+    which the correction goes into the FP64 solution and the FP64 true
+    residual is formed): time, FP32 iterations, FP64 applications."""
+    import torch
+
+    from . import warmstart as ws
+    from .backend import Precision
+    from .operator import Operator
+    from .solvers import MixedBiCGStab, SolverConfig
+
+    grid = ws.unit_grid(n, Precision.DOUBLE, 0)
+    rows = []
+    for seed in seeds:
+        prob = ws.scene_problem(ws.random_scene(seed), grid)
+        op64 = Operator(prob)
+        op32 = op64.with_precision(Precision.SINGLE)
+        for d in deltas:
+            solver = MixedBiCGStab(SolverConfig(max_iter=2000, rtol=1e-6), delta=d)
+            solver.solve(op64, prob.wave, operator_low=op32)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            res = solver.solve(op64, prob.wave, operator_low=op32)
+            b.record()
+            torch.cuda.synchronize()
+            rows.append({"seed": int(seed), "delta": float(d), "ms": a.elapsed_time(b),
+                         "iterations": int(res.iterations), "cycles": list(res.inner_iterations),
+                         "fp64_matvecs": int(res.fp64_matvecs), "status": res.status,
+                         "true_residual": float(res.true_final_residual)})
+        del op64, op32
+        torch.cuda.empty_cache()
+    return rows
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     sub = ap.add_subparsers(dest="what", required=True)
@@ -73,6 +111,8 @@ def main(argv=None) -> int:
     m.add_argument("--precision", choices=("single", "double"), default="single")
     m.add_argument("--n", type=int, default=128)
     m.add_argument("--reps", type=int, default=4)
+    m.add_argument("--xpass-variant", default=None,
+                   help="x-pass choice for this operator (EM3D_TUNE_XPASS_VARIANT value or 'generic')")
     s = sub.add_parser("step")
     s.add_argument("--n", type=int, default=128)
     s.add_argument("--seed", type=int, default=10001)
@@ -81,9 +121,22 @@ def main(argv=None) -> int:
     c.add_argument("--n", type=int, default=128)
     c.add_argument("--seeds", default="10000,10001,10002,10003")
     c.add_argument("--out", default=None, help="JSON rows path")
+    dsw = sub.add_parser("delta-sweep", help="MixedBiCGStab time and FP64 applications against the "
+                                             "reliable-update threshold")
+    dsw.add_argument("--n", type=int, default=128)
+    dsw.add_argument("--seeds", default="10000,10001,10002,10003,10004,10005,10006,10007")
+    dsw.add_argument("--deltas", default="1e-2,1e-3,1e-4,1e-5,3e-6")
     args = ap.parse_args(argv)
     if args.what == "matvec":
-        print("ok", matvec(args.precision, args.n, args.reps))
+        v = args.xpass_variant
+        v = None if v is None else (v if v == "generic" else int(v))
+        print("ok", matvec(args.precision, args.n, args.reps, v))
+    elif args.what == "delta-sweep":
+        import json
+
+        for r in delta_sweep(args.n, [int(v) for v in args.seeds.split(",")],
+                             [float(v) for v in args.deltas.split(",")]):
+            print(json.dumps(r), flush=True)
     elif args.what == "guess-curve":
         import json
 
