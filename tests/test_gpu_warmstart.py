@@ -46,5 +46,28 @@ def test_trained_warm_start_gains_over_zero_guess():
     # a guess whose true residual is not below ||f|| falls back to the zero
     # guess; that is rare and those solves converge like the others
     assert trained["mixed_nn"]["guess_rejected"] <= 3
-    assert trained["fp64_nn"]["iterations_mean"] <= trained["fp64_zero"]["iterations_mean"] + 0.25
+    # what the guess saves: iterations (no slack), and more than the same
+    # network untrained does; the solve time including the network's
+    # forward is reported, not asserted (at this scene distribution a 20-25%
+    # accurate guess is worth about one iteration, see iterations_vs_guess_error)
+    assert trained["fp64_nn"]["iterations_mean"] <= trained["fp64_zero"]["iterations_mean"]
+    assert trained["fp64_nn"]["iterations_mean"] < untrained["fp64_nn"]["iterations_mean"]
+    print("ms fp64 zero / nn incl. forward", trained["fp64_zero"]["ms_mean"],
+          trained["fp64_nn"]["ms_mean"] + trained["nn_ms_mean"])
     assert np.isfinite(trained["nn_ms_mean"])
+
+
+def test_solve_time_falls_with_guess_error():
+    """The mechanism a warm start relies on: the mixed solve from a guess of
+    relative error e needs fewer iterations the smaller e is, and a guess as
+    coarse as the network's (e ~ 0.2) saves about one iteration."""
+    from em3d_b200 import warmstart as ws
+
+    rows = ws.iterations_vs_guess_error([10000, 10001], 32, errors=(0.2, 1e-2, 1e-4))
+    for seed in (10000, 10001):
+        its = {(r["kind"], r["error"]): r["iterations"] for r in rows if r["seed"] == seed}
+        zero = its[("zero", 1.0)]
+        for kind in ("scattered", "white"):
+            assert its[(kind, 0.2)] <= zero + 1
+            assert its[(kind, 1e-4)] < its[(kind, 1e-2)] <= its[(kind, 0.2)]
+    assert all(r.get("converged", True) for r in rows)
