@@ -604,16 +604,44 @@ def run_ours(args, world, rank, local):
 
     one_by_one()
     single48_ms, res1 = _events_ms(one_by_one)
+    # all 48 problems in one uneven group: every operator pass is one launch over all four sizes
+    gone = GroupedSolver(probs, lambda: MixedBiCGStab(cfg), low_precision=e.Precision.SINGLE, single_launch=True)
+    gone.solve()
+    one_launch_ms, reso = _events_ms(lambda: gone.solve())
+    ugroup = gone.lows["uneven"]
+    xu = ugroup.waves()
+    yu = torch.zeros_like(xu)
+    ugroup.apply_into(xu, yu)
+    uneven_apply_ms = _events_ms(lambda: [ugroup.apply_into(xu, yu) for _ in range(10)])[0] / 10
+    lows = [gsolver.lows[k] for k in groups]
+    xg = [g.waves() for g in lows]
+    yg = [torch.empty_like(v) for v in xg]
+
+    def per_size_applications():
+        for g, xv, yv in zip(lows, xg, yg):
+            g.apply_into(xv, yv)
+
+    per_size_applications()
+    per_size_apply_ms = _events_ms(lambda: [per_size_applications() for _ in range(10)])[0] / 10
     uneven = {"workload": "uneven_spheres_48_N32-80", "sizes": {str(k[0][0]): len(v[0]) for k, v in groups.items()},
               "solver": "MixedBiCGStab grouped by grid size (the groups on their own streams at the same time) "
-                        "vs one problem at a time",
+                        "vs one problem at a time vs all sizes in one uneven group (one launch per pass)",
               "grouped_ms": grouped_ms, "grouped_sequential_ms": grouped_seq_ms, "one_by_one_ms": single48_ms,
               "gain": single48_ms / grouped_ms,
               "grouped_solves_per_s": len(probs) * 1000.0 / grouped_ms,
               "converged": int(sum(r.converged for r in resg)),
               "true_residual_max": max(float(r.true_final_residual) for r in resg),
-              "iterations_equal_one_by_one": all(a.iterations == b.iterations for a, b in zip(resg, res1))}
-    del probs, groups, gsolver, ops1, ops1_lo, mx1, resg, res1
+              "iterations_equal_one_by_one": all(a.iterations == b.iterations for a, b in zip(resg, res1)),
+              "single_launch": {
+                  "ms": one_launch_ms, "solves_per_s": len(probs) * 1000.0 / one_launch_ms,
+                  "gain_vs_one_by_one": single48_ms / one_launch_ms,
+                  "launches_per_application": 5, "per_size_launches_per_application": 5 * len(groups),
+                  "converged": int(sum(r.converged for r in reso)),
+                  "true_residual_max": max(float(r.true_final_residual) for r in reso),
+                  "iterations_max_diff_vs_grouped": max(abs(a.iterations - b.iterations) for a, b in zip(reso, resg)),
+                  "fp32_application_ms": uneven_apply_ms,
+                  "fp32_per_size_applications_ms": per_size_apply_ms}}
+    del probs, groups, gsolver, gone, ugroup, lows, xg, yg, xu, yu, ops1, ops1_lo, mx1, resg, res1, reso
     torch.cuda.empty_cache()
 
     # -- 4b. the acoustic scene: 200 spheres at 256^3, k0 = 20 (eta sampled on the device)

@@ -39,7 +39,8 @@ def _run(cmd):
 
 
 def build(verbose: bool = False, force: bool = False) -> str:
-    """Compile every ``csrc/*.cu`` (one object each, in parallel) and link them
+    """Compile every ``csrc/*.cu`` (one object each, in parallel; without
+    ``force`` only those older than their source or a header) and link them
     into one shared library; returns its path."""
     from concurrent.futures import ThreadPoolExecutor
 
@@ -50,22 +51,28 @@ def build(verbose: bool = False, force: bool = False) -> str:
     objdir = os.path.join(NATIVE, "obj")
     os.makedirs(objdir, exist_ok=True)
     jobs = []
+    # without force, an object newer than its source and every header is kept
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    newest_header = max((os.path.getmtime(h) for h in headers), default=0.0)
     for src in sources():
         obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
         cmd = [nvcc, *NVCC_FLAGS, "-I", INCLUDE, "-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        jobs.append((cmd, obj))
-    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+        fresh = (not force and os.path.exists(obj)
+                 and os.path.getmtime(obj) > max(os.path.getmtime(src), newest_header))
+        jobs.append((cmd, obj, fresh))
+    todo = [j for j in jobs if not j[2]]
+    workers = max(1, min(len(todo), os.cpu_count() or 1))
     with ThreadPoolExecutor(workers) as pool:
-        logs = list(pool.map(lambda j: _run(j[0]), jobs))
+        logs = list(pool.map(lambda j: _run(j[0]), todo))
     if verbose:
-        for (cmd, _), log in zip(jobs, logs):
+        for (cmd, _, _), log in zip(todo, logs):
             print(" ".join(cmd))
             if log:
                 print(log)
     tmp = LIB + ".tmp"
-    _run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *[o for _, o in jobs]])
+    _run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *[o for _, o, _ in jobs]])
     os.replace(tmp, LIB)
     return LIB
 

@@ -37,6 +37,19 @@ class EmGrid(ctypes.Structure):
                 ("lx", c_double), ("ly", c_double), ("lz", c_double)]
 
 
+EM3D_MAX_SEGMENTS = 8
+
+
+class Segment(ctypes.Structure):
+    """Mirror of ``em3d_segment``: problems of one grid size in an application
+    over uneven sizes (all strides in bytes)."""
+
+    _fields_ = [("grid", EmGrid), ("count", c_int32), ("chi_layout", c_int32),
+                ("spectra", c_void_p), ("spectrum_stride", c_size_t), ("chi", c_void_p), ("chi_stride", c_size_t),
+                ("u", c_void_p), ("out", c_void_p), ("field_stride", c_size_t),
+                ("entry_done", c_void_p), ("entry_done_stride", c_size_t)]
+
+
 class NativeError(RuntimeError):
     """A native entry point returned a non-zero status."""
 
@@ -74,6 +87,14 @@ SIGNATURES = {
         c_void_p, c_size_t, c_void_p]),
     "em3d_acoustic_rmatvec_grouped": (c_int, [_GRID, c_int, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
         c_void_p, c_size_t, c_void_p]),
+    "em3d_segment_size": (c_size_t, []),
+    "em3d_uneven_supported": (c_int, [_GRID, c_int, c_int]),
+    "em3d_uneven_workspace_bytes": (c_size_t, [c_int, c_int, c_int, POINTER(Segment)]),
+    "em3d_em_matvec_uneven": (c_int, [c_int, c_int, POINTER(Segment), c_void_p, c_size_t, c_void_p, c_void_p]),
+    "em3d_em_rmatvec_uneven": (c_int, [c_int, c_int, POINTER(Segment), c_void_p, c_size_t, c_void_p, c_void_p]),
+    "em3d_acoustic_matvec_uneven": (c_int, [c_int, c_int, POINTER(Segment), c_void_p, c_size_t, c_void_p, c_void_p]),
+    "em3d_acoustic_rmatvec_uneven": (c_int, [c_int, c_int, POINTER(Segment), c_void_p, c_size_t, c_void_p,
+                                             c_void_p]),
     "em3d_em_matvec_static_scratch": (c_int, [_GRID, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                               c_void_p]),
     "em3d_static_scratch_bytes": (c_size_t, []),
@@ -178,6 +199,8 @@ LAUNCHES = {
     "em3d_em_matvec": 5, "em3d_em_rmatvec": 5, "em3d_acoustic_matvec": 5, "em3d_acoustic_rmatvec": 5,
     "em3d_em_matvec_chi": 5, "em3d_em_rmatvec_chi": 5, "em3d_em_matvec_grouped": 5, "em3d_em_rmatvec_grouped": 5,
     "em3d_acoustic_matvec_grouped": 5, "em3d_acoustic_rmatvec_grouped": 5,
+    "em3d_em_matvec_uneven": 5, "em3d_em_rmatvec_uneven": 5, "em3d_acoustic_matvec_uneven": 5,
+    "em3d_acoustic_rmatvec_uneven": 5,
 }
 # Kernels launched by this process (graph replays add their captured counts).
 # Host threads update it under a lock; a thread that is capturing a graph

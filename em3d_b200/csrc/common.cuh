@@ -68,6 +68,9 @@ struct BatchStrides {
   int outer;
   int* status;  // this application's status words (bounded waits that gave up), or null
   int chi_layout = 9;  // EM contrast components stored per cell: 9 (full), 6 (symmetric) or 1 (isotropic)
+  // element stride between the entries' fields u / out (register row passes);
+  // 0: back to back (C cells each)
+  size_t field = 0;
 };
 
 // Index of entry (r, c) of a symmetric 3x3 contrast stored as its six

@@ -109,6 +109,12 @@ template <int K> __device__ bool reduce_last(StateView& sv, double (&v)[K], doub
   return true;
 }
 
+// Elements of this right-hand side's vectors in use (n_used; the rest of its
+// n is padding that the step kernels leave alone), all n when n_used is 0.
+__device__ __forceinline__ size_t used_len(const em3d_krylov_state* st, size_t n) {
+  return st->n_used > 0 && (size_t)st->n_used < n ? (size_t)st->n_used : n;
+}
+
 __device__ __forceinline__ bool running(const em3d_krylov_state* st) {
   return *(volatile const int*)&st->status == EM3D_RUNNING;
 }
@@ -157,6 +163,7 @@ __global__ void __launch_bounds__(kThreads) k_dots(size_t n, const cx<R>* x0, co
                                                    const cx<R>* y1, void* state, size_t sstride) {
   StateView sv = view(state, sstride);
   const size_t vo = blockIdx.y * n;
+  n = used_len(sv.st, n);
   x0 += vo; y0 += vo;
   if (x1) { x1 += vo; y1 += vo; }
   double v[4] = {0, 0, 0, 0};
@@ -214,6 +221,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_p(size_t n, void* state, size
   em3d_krylov_state* st = (em3d_krylov_state*)((char*)state + blockIdx.y * sstride);
   if (!running(st)) return;
   { const size_t vo = blockIdx.y * n; r += vo; p += vo; v += vo; }
+  n = used_len(st, n);
   const double2 rho = make_double2(st->rho_re, st->rho_im);
   const double2 omega = make_double2(st->omega_re, st->omega_im);
   int stop = EM3D_RUNNING;
@@ -244,6 +252,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, 
   StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; rh += vo; v += vo; }
+  n = used_len(sv.st, n);
   double a[2] = {0, 0};
   // four strides of loads in flight per thread (this kernel only reads)
   const size_t gs = (size_t)gridDim.x * blockDim.x;
@@ -277,6 +286,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_s(size_t n, void* state, size
   StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; r += vo; v += vo; s += vo; }
+  n = used_len(sv.st, n);
   const cx<R> al = cast_s<R>(sv.st->alpha_re, sv.st->alpha_im);
   double a[1] = {0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -309,6 +319,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_omega(size_t n, void* state, 
   StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; t += vo; s += vo; }
+  n = used_len(sv.st, n);
   double a[3] = {0, 0, 0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const cx<R> ti = t[i];
@@ -347,6 +358,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_update(size_t n, void* state,
   StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; u += vo; p += vo; s += vo; t += vo; r += vo; rh += vo; }
+  n = used_len(sv.st, n);
   const cx<R> al = cast_s<R>(sv.st->alpha_re, sv.st->alpha_im);
   const cx<R> om = cast_s<R>(sv.st->omega_re, sv.st->omega_im);
   double a[3] = {0, 0, 0};
@@ -387,6 +399,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_finalize(size_t n, void* stat
   StateView sv = view(state, sstride);
   if (*(volatile int*)&sv.st->pending != 1) return;
   { const size_t vo = blockIdx.y * n; u += vo; p += vo; }
+  n = used_len(sv.st, n);
   const cx<R> al = cast_s<R>(sv.st->alpha_re, sv.st->alpha_im);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     u[i] = cadd(u[i], cmul(al, p[i]));
@@ -404,6 +417,7 @@ __global__ void __launch_bounds__(kThreads) k_sim_residual(size_t n, void* state
   StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; res += vo; f += vo; }
+  n = used_len(sv.st, n);
   double a[1] = {0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const cx<R> ri = csub(res[i], f[i]);
@@ -431,6 +445,7 @@ __global__ void __launch_bounds__(kThreads) k_sim_update(size_t n, void* state, 
   StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; u += vo; res += vo; }
+  n = used_len(sv.st, n);
   const cx<R> g = cast_s<R>(sv.st->gamma_re, sv.st->gamma_im);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     u[i] = csub(u[i], cmul(g, res[i]));
@@ -448,6 +463,7 @@ __global__ void __launch_bounds__(kThreads) k_ts_residual(size_t n, void* state,
   StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; r += vo; f += vo; }
+  n = used_len(sv.st, n);
   double a[1] = {0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const cx<R> ri = csub(r[i], f[i]);
@@ -480,6 +496,7 @@ __global__ void __launch_bounds__(kThreads) k_ts_coeffs(size_t n, void* state, s
   StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; r += vo; rp += vo; g += vo; hg += vo; }
+  n = used_len(sv.st, n);
   const bool first = sv.st->first != 0;
   double a[5] = {0, 0, 0, 0, 0};  // a11, gg | a00, a01, b0, b1
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -528,6 +545,7 @@ __global__ void __launch_bounds__(kThreads) k_ts_update(size_t n, void* state, s
   StateView sv = view(state, sstride);
   if (!running(sv.st)) return;
   { const size_t vo = blockIdx.y * n; u += vo; up += vo; r += vo; rp += vo; g += vo; }
+  n = used_len(sv.st, n);
   const bool first = sv.st->first != 0;
   const R t = (R)sv.st->t, h = (R)sv.st->h;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {

@@ -25,9 +25,10 @@ template <typename R, int L> struct FastE {
   static constexpr int E = (L & (L - 1)) == 0 ? (sizeof(R) == 4 ? 16 : 8) : (L % 5 == 0 ? 20 : 12);
 };
 
-template <int L, int E, int C> struct RowsGeom {
+// NTGT: the CTA size aimed at (C * RPB * TT threads, RPB rows per CTA).
+template <int L, int E, int C, int NTGT = 256> struct RowsGeom {
   static constexpr int TT = L / E;
-  static constexpr int RPB = (256 / (C * TT)) > 0 ? (256 / (C * TT)) : 1;
+  static constexpr int RPB = (NTGT / (C * TT)) > 0 ? (NTGT / (C * TT)) : 1;
   static constexpr int NT = C * RPB * TT;
   static constexpr int PSTRIDE = rows_pencil_stride(L);
 };
@@ -35,13 +36,17 @@ template <int L, int E, int C> struct RowsGeom {
 // Rows along z.  Forward (INV = false): input rows of length L/2 (pruned),
 // output rows of length L.  Inverse: input rows of length L, output the
 // first L/2 (crop).  One thread handles one (component, row) pencil slice.
-template <typename R, int L, int C, int LD, int ST, bool INV>
-__global__ void __launch_bounds__(RowsGeom<L, FastE<R, L>::E, C>::NT)
-kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>* out,
-        const cx<R>* __restrict__ twg, int rows_pb, int nrows, BatchStrides bs, const int* skip) {
+// The body works on CTA `blk` of the pass (blockIdx.x in its own launch, a
+// CTA of one segment in an application over problems of uneven sizes).
+// Entries' fields (the forward pass's input, the inverse pass's output and
+// base) lie bs.field elements apart, or back to back when bs.field is 0.
+template <typename R, int L, int C, int LD, int ST, bool INV, int NTGT>
+__device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base,
+                                          cx<R>* out, const cx<R>* __restrict__ twg, int rows_pb, int nrows,
+                                          const BatchStrides& bs, const int* skip, int blk) {
   using T = cx<R>;
   constexpr int E = FastE<R, L>::E;
-  using G = RowsGeom<L, E, C>;
+  using G = RowsGeom<L, E, C, NTGT>;
   using P = RegPlan<L, E>;
   constexpr int TT = G::TT, RPB = G::RPB;
   constexpr int R1 = P::first(false), RL = P::last(false);
@@ -50,7 +55,7 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
   constexpr int LOUT = INV ? L / 2 : L;
   if (skip_launch(skip)) return;
   {
-    const int g0 = blockIdx.x * RPB, g1 = min(g0 + RPB, nrows) - 1;
+    const int g0 = blk * RPB, g1 = min(g0 + RPB, nrows) - 1;
     if (entries_done(bs, g0 / rows_pb, g1 / rows_pb)) return;
   }
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -60,12 +65,15 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
   const int t = threadIdx.x % TT;
   const int pen = threadIdx.x / TT;
   const int c = pen / RPB, rl = pen - c * RPB;
-  const int g = blockIdx.x * RPB + rl;
+  const int g = blk * RPB + rl;
   // rows of stopped entries are treated like rows past the end (no loads, no stores)
   const bool valid = g < nrows && !entry_done(bs, g / rows_pb);
   const int b = valid ? g / rows_pb : 0;
   const int row = valid ? g - b * rows_pb : 0;
   const cx<R>* chb = chi ? chi + (size_t)b * bs.chi : nullptr;
+  // element offsets of entry b's input and output
+  const size_t ib = (size_t)b * ((!INV && bs.field) ? bs.field : (size_t)C * rows_pb * LIN);
+  const size_t ob = (size_t)b * ((INV && bs.field) ? bs.field : (size_t)C * rows_pb * LOUT);
 
   T a[1][E];
 #pragma unroll
@@ -79,22 +87,22 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
         if constexpr (LD == FLD_EM_CHI) {
           const size_t o = (size_t)row * LIN + pos;
           const size_t cs = (size_t)rows_pb * LIN;
-          const T* ub = in + (size_t)b * 3 * cs;
+          const T* ub = in + ib;
 #pragma unroll
           for (int k = 0; k < 3; ++k) v = cadd(v, cmul(chb[(size_t)(c * 3 + k) * cs + o], ub[k * cs + o]));
         } else if constexpr (LD == FLD_EM_CHI6) {
           const size_t o = (size_t)row * LIN + pos;
           const size_t cs = (size_t)rows_pb * LIN;
-          const T* ub = in + (size_t)b * 3 * cs;
+          const T* ub = in + ib;
 #pragma unroll
           for (int k = 0; k < 3; ++k) v = cadd(v, cmul(chb[(size_t)sym_index(c, k) * cs + o], ub[k * cs + o]));
         } else if constexpr (LD == FLD_EM_CHI1) {
           const size_t o = (size_t)row * LIN + pos;
-          v = cmul(chb[o], in[((size_t)(b * 3 + c) * rows_pb) * LIN + o]);
+          v = cmul(chb[o], in[ib + (size_t)c * rows_pb * LIN + o]);
         } else if constexpr (LD == FLD_AC_CHI) {
-          v = cmul(chb[(size_t)row * LIN + pos], in[((size_t)b * rows_pb + row) * LIN + pos]);
+          v = cmul(chb[(size_t)row * LIN + pos], in[ib + (size_t)row * LIN + pos]);
         } else {
-          v = in[((size_t)(b * C + c) * rows_pb + row) * LIN + pos];
+          v = in[ib + ((size_t)c * rows_pb + row) * LIN + pos];
         }
       }
       a[0][q * R1 + r] = v;
@@ -130,7 +138,7 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
           const int ci = ST == FST_EM_ADJ ? k * 3 + c : sym_index(k, c);
           acc = cadd(acc, cmulcj(chb[(size_t)ci * cs + o], yk));
         }
-        const size_t oo = (size_t)(b * 3 + c) * cs + o;
+        const size_t oo = ob + (size_t)c * cs + o;
         out[oo] = csub(base[oo], acc);
       }
     }
@@ -145,7 +153,7 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
         if (INV && r >= RL / 2) continue;
         const int pos = j + r * ML;
         const T y = a[0][q * RL + r];
-        const size_t oo = ((size_t)(b * C + c) * rows_pb + row) * LOUT + pos;
+        const size_t oo = ob + ((size_t)c * rows_pb + row) * LOUT + pos;
         if constexpr (ST == FST_PLAIN) out[oo] = y;
         else if constexpr (ST == FST_SUB) out[oo] = csub(base[oo], y);
         else if constexpr (ST == FST_AC_ADJ || ST == FST_EM_ADJ1)  // chi^H y = conj(s) y per component
@@ -153,6 +161,13 @@ kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>
       }
     }
   }
+}
+
+template <typename R, int L, int C, int LD, int ST, bool INV>
+__global__ void __launch_bounds__(RowsGeom<L, FastE<R, L>::E, C>::NT)
+kf_rows(const cx<R>* in, const cx<R>* __restrict__ chi, const cx<R>* base, cx<R>* out,
+        const cx<R>* __restrict__ twg, int rows_pb, int nrows, BatchStrides bs, const int* skip) {
+  rows_body<R, L, C, LD, ST, INV, 256>(in, chi, base, out, twg, rows_pb, nrows, bs, skip, blockIdx.x);
 }
 
 template <int L, int E> struct StridedGeom {
@@ -163,10 +178,10 @@ template <int L, int E> struct StridedGeom {
 };
 
 // Pencils along y: in (outer, L/2 or L, inner) -> out (outer, L or L/2, inner).
+// The body works on CTA `blk` of the pass (see rows_body).
 template <typename R, int L, bool INV>
-__global__ void __launch_bounds__(StridedGeom<L, FastE<R, L>::E>::NT)
-kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner, int ntiles, BatchStrides bs,
-           const int* skip) {
+__device__ __forceinline__ void strided_body(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner,
+                                             int ntiles, const BatchStrides& bs, const int* skip, int blk) {
   using T = cx<R>;
   constexpr int E = FastE<R, L>::E;
   using G = StridedGeom<L, E>;
@@ -177,14 +192,14 @@ kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner
   constexpr int LIN = INV ? L : L / 2;
   constexpr int LOUT = INV ? L / 2 : L;
   if (skip_launch(skip)) return;
-  if (bs.done && entry_done(bs, (int)(blockIdx.x / ntiles) / bs.outer)) return;
+  if (bs.done && entry_done(bs, (blk / ntiles) / bs.outer)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tw = reinterpret_cast<T*>(smem_raw);
   T* sm = tw + L;
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
   const int p = threadIdx.x % PP, t = threadIdx.x / PP;
-  const int o = blockIdx.x / ntiles;
-  const int i = (blockIdx.x - o * ntiles) * PP + p;
+  const int o = blk / ntiles;
+  const int i = (blk - o * ntiles) * PP + p;
   const bool valid = i < inner;
   const T* src = in + (size_t)o * LIN * inner + i;
   T a[1][E];
@@ -211,6 +226,13 @@ kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner
       dst[(size_t)(j + r * ML) * inner] = a[0][q * RL + r];
     }
   }
+}
+
+template <typename R, int L, bool INV>
+__global__ void __launch_bounds__(StridedGeom<L, FastE<R, L>::E>::NT)
+kf_strided(const cx<R>* in, cx<R>* out, const cx<R>* __restrict__ twg, int inner, int ntiles, BatchStrides bs,
+           const int* skip) {
+  strided_body<R, L, INV>(in, out, twg, inner, ntiles, bs, skip, blockIdx.x);
 }
 
 template <int L, int E, int C, int NTT = 256> struct XmulGeom {
@@ -271,10 +293,11 @@ __device__ __forceinline__ int kfold(int k, int n) { return k <= n ? k : 2 * n -
 
 // Pencils along x for one (batch, ky, kz tile): forward FFT, spectrum multiply
 // in registers, reversed-plan inverse FFT, crop to x < Nx, in place in T2.
+// The body works on CTA `blk` of the pass (see rows_body).
 template <typename R, int L, int C, bool ADJ, int E, int NTT>
-__global__ void __launch_bounds__(XmulGeom<L, E, C, NTT>::NT)
-kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
-        int nb, BatchStrides bs, const int* skip) {
+__device__ __forceinline__ void xmul_body(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg,
+                                          int Ny, int Nz, int ntz, int nb, const BatchStrides& bs, const int* skip,
+                                          int blk) {
   using T = cx<R>;
   using G = XmulGeom<L, E, C, NTT>;
   using PL = RegPlan<L, E>;
@@ -289,7 +312,7 @@ kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
   const int p = threadIdx.x % PP, t = threadIdx.x / PP;
   // batch index fastest: consecutive CTAs share one spectrum tile in L2
-  int idx = blockIdx.x;
+  int idx = blk;
   const int b = idx % nb;
   idx /= nb;
   const int tile = idx % ntz;
@@ -366,6 +389,13 @@ kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg
       for (int c = 0; c < C; ++c) col[((size_t)c * Nx + x) * xstride] = a[c][q * R1 + r];
     }
   }
+}
+
+template <typename R, int L, int C, bool ADJ, int E, int NTT>
+__global__ void __launch_bounds__(XmulGeom<L, E, C, NTT>::NT)
+kf_xmul(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
+        int nb, BatchStrides bs, const int* skip) {
+  xmul_body<R, L, C, ADJ, E, NTT>(T2, spec, twg, Ny, Nz, ntz, nb, bs, skip, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------

@@ -7,12 +7,14 @@ network of the benchmark's shape) twice
 and brackets a third run with ``cudaProfilerStart/Stop`` for
 ``ncu --profile-from-start off``; ``guess-curve`` times the mixed solve from
 initial guesses of controlled relative error (what a warm start must achieve
-to save iterations).
+to save iterations); ``uneven`` applies the 48 uneven sphere problems
+(N in 32..80) as one uneven group (``--per-size``: one group per size).
 
     python -m em3d_b200.profiling matvec --precision single --n 128
     python -m em3d_b200.profiling step --n 128 --seed 10001
     python -m em3d_b200.profiling guess-curve --n 128 --seeds 10000,10001,10002,10003
     python -m em3d_b200.profiling delta-sweep --n 128
+    python -m em3d_b200.profiling uneven --precision single --count 48
 """
 from __future__ import annotations
 
@@ -37,6 +39,34 @@ def matvec(precision: str, n: int, reps: int, xpass_variant=None) -> float:
     out = torch.empty_like(prob.wave)
     for _ in range(reps):
         op.apply_into(prob.wave, out)
+    torch.cuda.synchronize()
+    return float(out.abs().sum())
+
+
+def uneven(precision: str, count: int, reps: int, per_size: bool = False) -> float:
+    """``reps`` applications of the ``count`` uneven sphere problems (N in
+    32..80): one :class:`UnevenGroup` application (five launches in all), or
+    with ``per_size`` one grouped application per grid size."""
+    import torch
+
+    from . import workloads
+    from .groups import UnevenGroup, group_by_grid
+
+    probs = workloads.uneven_sphere_problems(precision, count, seed=0)
+    if per_size:
+        groups = [g for _, g in group_by_grid(probs).values()]
+        xs = [g.waves() for g in groups]
+        outs = [torch.empty_like(x) for x in xs]
+        for _ in range(reps):
+            for g, x, o in zip(groups, xs, outs):
+                g.apply_into(x, o)
+        torch.cuda.synchronize()
+        return float(sum(o.abs().sum() for o in outs))
+    group = UnevenGroup(probs)
+    x = group.waves()
+    out = torch.zeros_like(x)
+    for _ in range(reps):
+        group.apply_into(x, out)
     torch.cuda.synchronize()
     return float(out.abs().sum())
 
@@ -113,6 +143,11 @@ def main(argv=None) -> int:
     m.add_argument("--reps", type=int, default=4)
     m.add_argument("--xpass-variant", default=None,
                    help="x-pass choice for this operator (EM3D_TUNE_XPASS_VARIANT value or 'generic')")
+    u = sub.add_parser("uneven", help="applications over the uneven sphere problems (one launch per pass)")
+    u.add_argument("--precision", choices=("single", "double"), default="single")
+    u.add_argument("--count", type=int, default=48)
+    u.add_argument("--reps", type=int, default=3)
+    u.add_argument("--per-size", action="store_true", help="one grouped application per grid size instead")
     s = sub.add_parser("step")
     s.add_argument("--n", type=int, default=128)
     s.add_argument("--seed", type=int, default=10001)
@@ -131,6 +166,8 @@ def main(argv=None) -> int:
         v = args.xpass_variant
         v = None if v is None else (v if v == "generic" else int(v))
         print("ok", matvec(args.precision, args.n, args.reps, v))
+    elif args.what == "uneven":
+        print("ok", uneven(args.precision, args.count, args.reps, args.per_size))
     elif args.what == "delta-sweep":
         import json
 

@@ -85,7 +85,7 @@ class KrylovState(ctypes.Structure):
         ("status", c_int32), ("iter", c_int32), ("matvecs", c_int32), ("rmatvecs", c_int32),
         ("max_iter", c_int32), ("max_actions", c_int32), ("hist_len", c_int32), ("hist_cap", c_int32),
         ("pending", c_int32), ("first", c_int32), ("ticket", c_uint32), ("batch_running", c_int32),
-        ("batch_done", c_int32),
+        ("batch_done", c_int32), ("n_used", c_int32),
     ]
 
 
@@ -218,6 +218,12 @@ class _Engine:
         self.n = int(self.rhs.numel()) // self.batch
         self.dt = _native_dtype(self.rhs)
         self.state = DeviceState(self.rhs.device, hist_cap, self.batch)
+        lens = getattr(operator, "entry_lengths", None)
+        if lens is not None and self.batch > 1:
+            # rows padded beyond their problem's field (UnevenGroup): the step
+            # kernels work on each row's own length
+            for h, m in zip(self.state.hosts, lens):
+                h.n_used = int(m)
         self.native_op = hasattr(operator, "apply_into")
         if self.batch > 1 and not self.native_op:
             raise TypeError("batched solves need an operator with apply_into (em3d_b200.Operator / AcousticOperator)")
@@ -365,6 +371,16 @@ def _load_u(buf, x0):
     return buf
 
 
+def _entry(operator, u, b: int, batch: int):
+    """Right-hand side ``b``'s part of the stacked ``u``: the operator's view
+    of it where the operator stacks fields of different shapes
+    (``UnevenGroup.entry_field``), else ``u[b]``."""
+    if batch == 1:
+        return u
+    view = getattr(operator, "entry_field", None)
+    return view(u, b) if view is not None else u[b]
+
+
 def _batch_of(operator, rhs) -> int:
     """Number of right-hand sides stacked in front of the operator's field shape."""
     fs = operator._field_shape() if hasattr(operator, "_field_shape") else None
@@ -431,7 +447,7 @@ class _KrylovSolver:
         out = []
         u = u.clone()  # the engine's buffer is reused by the next solve
         for b, (st, hist, counts) in enumerate(eng.state.download()):
-            ub = u if eng.batch == 1 else u[b]
+            ub = _entry(eng.op, u, b, eng.batch)
             if trivial[b]:
                 out.append(_trivial_result(ub))
             else:
@@ -789,7 +805,7 @@ class DefectCorrection:
         out = []
         u = u.clone()  # the cached buffer is reused by the next solve
         for b in range(batch):
-            ub = u if batch == 1 else u[b]
+            ub = _entry(operator, u, b, batch)
             h = hist[b] if hist[b] else [0.0]
             out.append(DefectCorrectionResult(
                 u=ub, iterations=int(sum(inner_its[b])), residual_history=h, converged=status[b] == "converged",
@@ -1091,7 +1107,7 @@ class MixedBiCGStab:
         u = x.clone()  # the cached buffer is reused by the next solve
         out = []
         for b in range(batch):
-            ub = row(u, b)
+            ub = _entry(operator, u, b, batch)
             if status[b] == "zero":
                 out.append(DefectCorrectionResult(u=ub, iterations=0, residual_history=[0.0], converged=True,
                                                   matvec_count=0, residual_action_counts=[0], status="converged",

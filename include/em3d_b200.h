@@ -203,6 +203,53 @@ int em3d_acoustic_rmatvec_grouped(const em3d_grid* g, int dtype, int batch, cons
     const void* chis, const void* v, void* out, void* workspace, size_t workspace_bytes, const int* skip,
     const void* entry_done, size_t entry_done_stride, void* stream);
 
+/* Problems of uneven grid sizes in one application: each of the five passes
+ * is ONE launch over every problem of every segment (a segment = `count`
+ * problems on one grid, each with its own spectrum, contrast and field); a
+ * CTA finds its segment and runs the register FFT of that segment's axis
+ * length.  Up to EM3D_MAX_SEGMENTS segments; every doubled axis length
+ * (2 Nx, 2 Ny, 2 Nz) must be one em3d_uneven_supported accepts (32..256:
+ * powers of two, 96, 160, 192, with the exceptions it reports).  All
+ * strides are in bytes and multiples of the element size.  EM segments share
+ * one chi_layout.  Stopped entries (entry_done) are skipped as in the grouped
+ * calls; `skip` is the whole-application flag.  No counterpart call in the
+ * reference, which solves such sets one problem at a time
+ * (src/em3d/operator.py:320-428 per problem). */
+#define EM3D_MAX_SEGMENTS 8
+typedef struct em3d_segment {
+  em3d_grid grid;
+  int32_t count;                /* problems in this segment (>= 1)                   */
+  int32_t chi_layout;           /* EM: EM3D_CHI_FULL / SYMMETRIC / ISOTROPIC; acoustic: ignored */
+  const void* spectra;          /* problem j's spectrum at spectra + j * spectrum_stride */
+  size_t spectrum_stride;       /* >= em3d_spectrum_bytes of this grid              */
+  const void* chi;              /* problem j's contrast at chi + j * chi_stride       */
+  size_t chi_stride;
+  const void* u;                /* problem j's input field at u + j * field_stride    */
+  void* out;                    /* problem j's output at out + j * field_stride       */
+  size_t field_stride;          /* >= C * Nx*Ny*Nz elements                          */
+  const void* entry_done;       /* nullable: problem j's int stop flag at entry_done + j * entry_done_stride */
+  size_t entry_done_stride;
+} em3d_segment;
+
+/* sizeof(em3d_segment) as compiled into the library (ABI check). */
+size_t em3d_segment_size(void);
+/* 1 if a problem on grid g can join an uneven application of this kind and
+ * dtype, else 0. */
+int em3d_uneven_supported(const em3d_grid* g, int kind, int dtype);
+/* Workspace bytes of an uneven application (each segment's two transform
+ * buffers, then 256 bytes of status words as for em3d_apply_workspace_bytes);
+ * only the grids, counts, layouts and strides are read (the array pointers
+ * may still be NULL); 0 for invalid segments. */
+size_t em3d_uneven_workspace_bytes(int kind, int dtype, int nseg, const em3d_segment* segs);
+int em3d_em_matvec_uneven(int dtype, int nseg, const em3d_segment* segs, void* workspace, size_t workspace_bytes,
+                          const int* skip, void* stream);
+int em3d_em_rmatvec_uneven(int dtype, int nseg, const em3d_segment* segs, void* workspace, size_t workspace_bytes,
+                           const int* skip, void* stream);
+int em3d_acoustic_matvec_uneven(int dtype, int nseg, const em3d_segment* segs, void* workspace,
+                                size_t workspace_bytes, const int* skip, void* stream);
+int em3d_acoustic_rmatvec_uneven(int dtype, int nseg, const em3d_segment* segs, void* workspace,
+                                 size_t workspace_bytes, const int* skip, void* stream);
+
 /* Scalar versions.  Replace AcousticOperator.matvec / rmatvec
  * (src/em3d/acoustics/operator.py:40-67). */
 int em3d_acoustic_matvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi,
@@ -266,6 +313,9 @@ typedef struct em3d_krylov_state {
   int32_t batch_running;       /* state 0 only: right-hand sides still running */
   int32_t batch_done;          /* state 0 only: 1 once all have stopped; the
                                   operator's `skip` flag in a solve loop        */
+  int32_t n_used;              /* elements of this right-hand side's n in use;
+                                  the step kernels leave the rest (padding of
+                                  a problem smaller than n) alone; 0: all n    */
 } em3d_krylov_state;
 
 /* sizeof(em3d_krylov_state) as compiled into the library (ABI check). */
