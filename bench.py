@@ -55,9 +55,10 @@ SCENE_SEEDS = list(range(10000, 10008))
 # ``config``); what each arm runs is under ``solver`` / ``cpu_baseline``.
 CONFIG = {"workload": f"warmstart_heldout_scenes_{N_GRID}^3", "scenes": SCENE_SEEDS, "rtol_true": RTOL}
 # dram__bytes_read.sum + dram__bytes_write.sum per complex64 EM matvec at
-# 128^3 (all five passes, default x-pass variant) from an ncu launch list of
-# the same operator (-k regex:kf_, second matvec of the run).
-NCU_TRAFFIC_BYTES = 1405.8e6
+# 128^3 (all five passes, default x-pass variant, the contrast stored as its
+# six symmetric components) from an ncu launch list of the same operator
+# (-k regex:kf_, second matvec of the run).
+NCU_TRAFFIC_BYTES = 1349.6e6
 
 
 def byte_model(n: int, c: int) -> int:

@@ -34,9 +34,11 @@ template <typename R, int L, int C> constexpr bool uneven_rows_ok() {
 template <typename R, int L> constexpr bool uneven_strided_ok() {
   return StridedGeom<L, FastE<R, L>::E>::NT == UnevenNT<1>::strided;
 }
-// complex128 at 160 keeps three 20-element pencils per thread and spills
+// (complex128 at 160 keeps three 20-element pencils per thread and spills
+// part of them to local memory; it joins all the same, so that FP64
+// operators over such sizes stay one launch per pass)
 template <typename R, int L, int C> constexpr bool uneven_x_ok() {
-  return XmulGeom<L, FastE<R, L>::E, C, 128>::NT == UnevenNT<C>::xmul && !(sizeof(R) == 8 && L == 160);
+  return XmulGeom<L, FastE<R, L>::E, C, 128>::NT == UnevenNT<C>::xmul;
 }
 
 #define EM3D_UNEVEN_LENGTHS(X) X(32) X(64) X(96) X(128) X(160) X(192) X(256)
@@ -176,7 +178,6 @@ __global__ void __launch_bounds__(128) ku_xmul(const __grid_constant__ Segs<XSeg
 // host side
 // ---------------------------------------------------------------------------
 
-// Checks one segment; fills its dims and the element strides.
 // Checks one segment (its arrays too when `arrays`); fills its dims and the
 // element strides.
 template <typename R, int C>

@@ -39,6 +39,7 @@ def _problems(sizes, prec="double", acoustic=False, rotated=()):
         if i in rotated:
             rot = np.linalg.qr(np.random.default_rng(i).standard_normal((3, 3)))[0]
             eps_t = rot @ np.diag([eps, 1.5 * eps, 0.8 * eps]) @ rot.T
+            eps_t = 0.5 * (eps_t + eps_t.T)  # exactly symmetric
             shape = scenes.EllipsoidShape(c, (r, 0.8 * r, 0.9 * r), rot, eps_t)
         else:
             shape = scenes.EllipsoidShape(c, (r,) * 3, None, eps)
@@ -67,7 +68,7 @@ def _check_entries(group, probs, x, tol, acoustic=False):
 
 
 @pytest.mark.parametrize("prec,sizes,tol", [
-    ("double", [(32, 32, 32), (16, 16, 16), (16, 32, 48), (32, 32, 32), (48, 48, 48)], 1e-13),
+    ("double", [(32, 32, 32), (16, 16, 16), (16, 32, 48), (80, 80, 80), (32, 32, 32), (48, 48, 48)], 1e-13),
     ("single", [(48, 48, 48), (32, 32, 32), (32, 48, 64), (80, 80, 80), (32, 32, 32)], 2e-6),
 ])
 def test_uneven_em_equals_single_operators(prec, sizes, tol):
@@ -102,9 +103,9 @@ def test_uneven_em_full_contrast():
     """A non-symmetric contrast makes the group store full tensors."""
     import torch
 
-    from em3d_b200.groups import UnevenGroup
-
     import dataclasses
+
+    from em3d_b200.groups import UnevenGroup
 
     probs = _problems([(16, 16, 16), (32, 32, 32)], "double")
     chi = probs[1].eps_tensor.clone()

@@ -34,8 +34,7 @@ def test_supported_grids():
     # a 32-point x pencil in complex64 is two threads wide: no 128-thread CTA shape
     assert not _ok((16, 16, 16), EM, C64)
     assert _ok((16, 16, 16), EM, C128)
-    # the 160-point x pass in complex128 is left out (three 20-element pencils per thread spill)
-    assert not _ok((80, 80, 80), EM, C128)
+    assert _ok((80, 80, 80), EM, C128)
     assert _ok((64, 80, 80), EM, C128)
     # lengths without a register plan, or beyond 256
     assert not _ok((40, 40, 40), EM, C64)
