@@ -432,40 +432,20 @@ def run_ours(args, world, rank, local):
         h.copy_(p.wave.cpu())
     host_u = [torch.empty(host_rhs[0].shape, dtype=host_rhs[0].dtype).pin_memory() for _ in range(2)]
     dev_in = [torch.empty(host_rhs[0].shape, dtype=host_rhs[0].dtype, device=dev) for _ in range(2)]
-    copy_stream = torch.cuda.Stream(device=dev)
 
     def e2e_run(n):
-        """``n`` steps through the public API.  Step s's right-hand side is
-        copied in from pinned host memory on a copy stream one step ahead, and
-        its solution copied out on the copy stream while step s+1 solves; the
-        compute stream waits for each input, and the run ends after the last
-        copy, so every copy lies inside the caller's timed region."""
-        main = torch.cuda.current_stream()
-        ready = [torch.cuda.Event() for _ in range(2)]
-        free = [torch.cuda.Event() for _ in range(2)]
+        """``n`` steps through the public API, each: the right-hand side copied
+        in from pinned host memory, the solve, the solution copied out to
+        pinned host memory, on the solving stream.  (Copies on a second stream
+        overlapping the neighbouring solves were measured slower: a 100 MB
+        transfer on a copy engine delays the solver's own small transfers of
+        its states and stop flags queued behind it.)"""
         held = []
-        with torch.cuda.stream(copy_stream):
-            dev_in[0].copy_(host_rhs[0], non_blocking=True)
-            ready[0].record(copy_stream)
         for s in range(n):
-            b = s % 2
-            if s + 1 < n:
-                nb = (s + 1) % 2
-                with torch.cuda.stream(copy_stream):
-                    if s >= 1:
-                        copy_stream.wait_event(free[nb])  # the solve of step s-1 is done with that buffer
-                    dev_in[nb].copy_(host_rhs[(s + 1) % K], non_blocking=True)
-                    ready[nb].record(copy_stream)
-            main.wait_event(ready[b])
-            res = mixed_nn(s % K, dev_in[b])
-            free[b].record(main)
-            done = torch.cuda.Event()
-            done.record(main)
-            with torch.cuda.stream(copy_stream):
-                copy_stream.wait_event(done)
-                host_u[b].copy_(res.u, non_blocking=True)
+            dev_in[0].copy_(host_rhs[s % K], non_blocking=True)
+            res = mixed_nn(s % K, dev_in[0])
+            host_u[0].copy_(res.u, non_blocking=True)
             held.append(res)  # the solution stays allocated until its copy has run
-        main.wait_stream(copy_stream)
         return held
 
     e2e_run(2)
@@ -751,8 +731,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT,
                 "h2d_bytes_per_step": int(host_rhs[0].numel() * host_rhs[0].element_size()),
                 "d2h_bytes_per_step": int(host_u[0].numel() * host_u[0].element_size()),
-                "copies": "pinned host right-hand side in and solution out every step, on a copy stream "
-                          "overlapping the neighbouring steps' solves"},
+                "copies": "pinned host right-hand side in and solution out every step, on the solving stream"},
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
                      "traffic": NCU_TRAFFIC_BYTES, "kernel": "em3d_em_matvec FP32 (5 fused passes)",
                      "bytes_per_launch": bytes32, "ms_per_launch": mv32_ms, "peak_source": peak_kind,

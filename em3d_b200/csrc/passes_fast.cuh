@@ -456,10 +456,14 @@ template <int L, int E, int C, int NTT> struct XpipeGeom {
 // TMAF: the field slab arrives by TMA (one tile load per component, issued by
 // thread 0 and completed on an mbarrier; `fmap` describes T2 as (kz words,
 // ky, batch * C * Nx rows)) instead of per-thread cp.async copies.
-template <typename R, int L, int C, bool ADJ, int E, int NTT, bool TMAF, int MINB = 1>
-__global__ void __launch_bounds__(XpipeGeom<L, E, C, NTT>::NT, MINB)
-kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
-             int nb, BatchStrides bs, const int* skip, const __grid_constant__ CUtensorMap fmap, int* status) {
+// The body runs as CTA `blk` of `nblk` persistent CTAs (blockIdx.x of gridDim.x
+// in its own launch; a segment's share of CTAs in an application over problems
+// of uneven sizes); `fmap` points to the field map in the parameter block.
+template <typename R, int L, int C, bool ADJ, int E, int NTT, bool TMAF>
+__device__ __forceinline__ void xpipe_body(cx<R>* T2, const cx<R>* __restrict__ spec,
+                                           const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz, int nb,
+                                           const BatchStrides& bs, const int* skip, const CUtensorMap* fmap,
+                                           int* status, int blk, int nblk) {
   using T = cx<R>;
   using G = XpipeGeom<L, E, C, NTT>;
   using PL = RegPlan<L, E>;
@@ -520,7 +524,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
       if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(fbar, (uint32_t)(C * NX * PP * EB));
 #pragma unroll
-        for (int c = 0; c < C; ++c) tma_load_3d(sfield + c * NX * PP, &fmap, fbar, kz0 * W, ky, (b * C + c) * NX);
+        for (int c = 0; c < C; ++c) tma_load_3d(sfield + c * NX * PP, fmap, fbar, kz0 * W, ky, (b * C + c) * NX);
       }
       return;
     }
@@ -552,7 +556,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     }
   };
 
-  int u = blockIdx.x, sub = 0;
+  int u = blk, sub = 0;
   if (u < nunits) issue_field(u, 0);
   cp_async_commit();
   if (u < nunits) issue_spec(u);
@@ -569,7 +573,7 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     // the next tile: the unit's next (entry, ky), else the CTA's next unit
     int nu = u, ns = sub + 1;
     if (ns >= nbu * nmirror(jy)) {
-      nu = u + gridDim.x;
+      nu = u + nblk;
       ns = 0;
     }
     // the same for every thread of the CTA, so the barriers below stay uniform
@@ -662,6 +666,14 @@ kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict_
     sub = ns;
   }
   cp_async_wait_all();
+}
+
+template <typename R, int L, int C, bool ADJ, int E, int NTT, bool TMAF, int MINB = 1>
+__global__ void __launch_bounds__(XpipeGeom<L, E, C, NTT>::NT, MINB)
+kf_xmul_pipe(cx<R>* T2, const cx<R>* __restrict__ spec, const cx<R>* __restrict__ twg, int Ny, int Nz, int ntz,
+             int nb, BatchStrides bs, const int* skip, const __grid_constant__ CUtensorMap fmap, int* status) {
+  xpipe_body<R, L, C, ADJ, E, NTT, TMAF>(T2, spec, twg, Ny, Nz, ntz, nb, bs, skip, &fmap, status, blockIdx.x,
+                                          gridDim.x);
 }
 
 // ---------------------------------------------------------------------------

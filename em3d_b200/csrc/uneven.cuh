@@ -15,6 +15,8 @@
 #pragma once
 
 #include <algorithm>
+#include <cmath>
+#include <cstring>
 
 #include "operator_passes.cuh"
 
@@ -41,6 +43,14 @@ template <typename R, int L, int C> constexpr bool uneven_x_ok() {
   return XmulGeom<L, FastE<R, L>::E, C, 128>::NT == UnevenNT<C>::xmul;
 }
 
+// The pipelined x pass (persistent CTAs, field slab by TMA): same CTA shape
+// rule, and its slabs must fit in a CTA's shared memory.
+template <typename R, int L, int C> constexpr bool uneven_xpipe_ok() {
+  using G = XpipeGeom<L, FastE<R, L>::E, C, 128>;
+  return G::NT == UnevenNT<C>::xmul && G::P % 2 == 0 &&
+         (size_t)G::TOTAL * sizeof(cx<R>) + G::BYTES_EXTRA <= kSmemPerCta;
+}
+
 #define EM3D_UNEVEN_LENGTHS(X) X(32) X(64) X(96) X(128) X(160) X(192) X(256)
 
 // Host-side geometry of one axis length in the three pass kinds.
@@ -52,6 +62,9 @@ struct UnevenLen {
   size_t strided_smem;
   int x_p;             // kz per CTA
   size_t x_smem;
+  bool xpipe_ok;       // the pipelined x pass applies
+  int xpipe_p;
+  size_t xpipe_smem;
 };
 
 template <typename R, int C, int L> static UnevenLen uneven_len_of() {
@@ -69,7 +82,28 @@ template <typename R, int C, int L> static UnevenLen uneven_len_of() {
   u.strided_smem = (size_t)(L + L * GS::S) * sizeof(cx<R>);
   u.x_p = GX::P;
   u.x_smem = (size_t)(L + GX::REGIONS * L * GX::S) * sizeof(cx<R>);
+  using GP = XpipeGeom<L, E, C, 128>;
+  u.xpipe_ok = uneven_xpipe_ok<R, L, C>();
+  u.xpipe_p = GP::P;
+  u.xpipe_smem = (size_t)GP::TOTAL * sizeof(cx<R>) + GP::BYTES_EXTRA;
   return u;
+}
+
+// The TMA map of a segment's T2 for the pipelined x pass (tile width P of its
+// x length).
+template <typename R, int C>
+static int uneven_field_map(int L, CUtensorMap* fmap, cx<R>* T2, const Dims& d, int count) {
+  switch (L) {
+#define EM3D_CASE(LL)                                                                      \
+  case LL:                                                                                 \
+    if constexpr (uneven_xpipe_ok<R, LL, C>())                                             \
+      return encode_field_map<R, C, XpipeGeom<LL, FastE<R, LL>::E, C, 128>::P>(fmap, T2, d, count); \
+    break;
+    EM3D_UNEVEN_LENGTHS(EM3D_CASE)
+#undef EM3D_CASE
+  }
+  em3d_set_last_error("no pipelined x pass for this length");
+  return EM3D_ERR_UNSUPPORTED;
 }
 
 template <typename R, int C> static bool uneven_len(int L, UnevenLen* out) {
@@ -113,6 +147,15 @@ template <typename R> struct XSeg {
   const cx<R>* spec;
   const cx<R>* tw;
   int ny, nz, ntz, nb, L, block0;
+  BatchStrides bs;
+};
+// The map comes first: it needs 64-byte alignment in the parameter block.
+template <typename R> struct XPSeg {
+  CUtensorMap fmap;
+  cx<R>* T2;
+  const cx<R>* spec;
+  const cx<R>* tw;
+  int ny, nz, ntz, nb, L, block0, nblocks;
   BatchStrides bs;
 };
 template <class S> struct Segs {
@@ -168,6 +211,24 @@ __global__ void __launch_bounds__(128) ku_xmul(const __grid_constant__ Segs<XSeg
     if constexpr (uneven_x_ok<R, LL, C>())                                                                   \
       xmul_body<R, LL, C, ADJ, FastE<R, LL>::E, 128>(g.T2, g.spec, g.tw, g.ny, g.nz, g.ntz, g.nb, g.bs, skip, \
                                                      blk);                                                   \
+    break;
+    EM3D_UNEVEN_LENGTHS(EM3D_CASE)
+#undef EM3D_CASE
+  }
+}
+
+// Pipelined x pass: each segment has its own share of persistent CTAs
+// (nblocks) that loop over that segment's tiles.
+template <typename R, int C, bool ADJ>
+__global__ void __launch_bounds__(128) ku_xpipe(const __grid_constant__ Segs<XPSeg<R>> a, const int* skip) {
+  int blk;
+  const XPSeg<R>& g = my_segment(a, &blk);
+  switch (g.L) {
+#define EM3D_CASE(LL)                                                                                          \
+  case LL:                                                                                                     \
+    if constexpr (uneven_xpipe_ok<R, LL, C>())                                                                 \
+      xpipe_body<R, LL, C, ADJ, FastE<R, LL>::E, 128, true>(g.T2, g.spec, g.tw, g.ny, g.nz, g.ntz, g.nb, g.bs, \
+                                                            skip, &g.fmap, g.bs.status, blk, g.nblocks);       \
     break;
     EM3D_UNEVEN_LENGTHS(EM3D_CASE)
 #undef EM3D_CASE
@@ -273,10 +334,20 @@ int apply_uneven(int dtype, int nseg, const em3d_segment* segs, void* ws, size_t
   Segs<RowsSeg<R>> p1{}, p5{};
   Segs<StridedSeg<R>> p2{}, p4{};
   Segs<XSeg<R>> p3{};
-  p1.n = p2.n = p3.n = p4.n = p5.n = nseg;
+  Segs<XPSeg<R>> p3p;
+  memset(&p3p, 0, sizeof p3p);
+  p1.n = p2.n = p3.n = p4.n = p5.n = p3p.n = nseg;
   int b1 = 0, b2 = 0, b3 = 0;
-  size_t sm1 = 0, sm2 = 0, sm3 = 0;
+  size_t sm1 = 0, sm2 = 0, sm3 = 0, sm3p = 0;
   int layout = 0;
+  // the EM x pass runs pipelined (persistent CTAs, field slab by TMA) when
+  // every segment's x length allows it, unless a non-pipelined x-pass
+  // variant (0..2) is selected
+  const int xv = g_tuning[EM3D_TUNE_XPASS_VARIANT];
+  bool pipe = C == 3 && (xv < 0 || xv >= 3);
+  double work[kMaxSegments];
+  long long units[kMaxSegments];
+  Dims dims[kMaxSegments];
   for (int i = 0; i < nseg; ++i) {
     const em3d_segment& s = segs[i];
     Dims d;
@@ -317,6 +388,59 @@ int apply_uneven(int dtype, int nseg, const em3d_segment* segs, void* ws, size_t
     p3.s[i] = XSeg<R>{T2, lay.oct(sp), lay.twx(sp, d), d.ny, d.nz, ntz, s.count, 2 * d.nx, b3, bs};
     b3 += s.count * 2 * d.ny * ntz;
     sm3 = std::max(sm3, lx.x_smem);
+    pipe = pipe && lx.xpipe_ok;
+    {
+      XPSeg<R>& q = p3p.s[i];
+      q.T2 = T2;
+      q.spec = lay.oct(sp);
+      q.tw = lay.twx(sp, d);
+      q.ny = d.ny;
+      q.nz = d.nz;
+      q.ntz = (2 * d.nz + lx.xpipe_p - 1) / lx.xpipe_p;
+      q.nb = s.count;
+      q.L = 2 * d.nx;
+      q.bs = bs;
+      // work units of the persistent loop (one entry per unit: every entry
+      // has its own spectrum, or the segment holds one entry)
+      units[i] = (long long)s.count * (d.ny + 1) * q.ntz;
+      work[i] = (double)units[i] * lx.xpipe_p * (2.0 * d.nx) * std::log2(2.0 * d.nx);
+      dims[i] = d;
+      sm3p = std::max(sm3p, lx.xpipe_smem);
+    }
+  }
+  int b3p = 0;
+  if (pipe) {
+    // Each CTA loops over U of its segment's work units (one spectrum slab, the
+    // ky / 2Ny - ky tiles); the grid is several waves of such CTAs, so the
+    // hardware scheduler balances the segments, and the segments with the
+    // most transform work come first (their CTAs start in the first wave).
+    auto kern = ku_xpipe<R, C, ADJ>;
+    EM3D_CUDA_TRY(allow_smem(kern));
+    int sms = 0, per_sm = 0;
+    EM3D_CUDA_TRY(sm_count(&sms));
+    EM3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, UnevenNT<C>::xmul, sm3p));
+    if (per_sm < 1) per_sm = 1;
+    constexpr long long kWaves = 8;
+    long long all_units = 0;
+    for (int i = 0; i < nseg; ++i) all_units += units[i];
+    const long long U = std::max(2LL, (all_units + kWaves * sms * per_sm - 1) / (kWaves * sms * per_sm));
+    int order[kMaxSegments];
+    for (int i = 0; i < nseg; ++i) order[i] = i;
+    std::sort(order, order + nseg, [&](int a, int b) { return work[a] > work[b]; });
+    Segs<XPSeg<R>> sorted;
+    memset(&sorted, 0, sizeof sorted);
+    sorted.n = nseg;
+    for (int k = 0; k < nseg; ++k) {
+      const int i = order[k];
+      XPSeg<R>& q = sorted.s[k];
+      q = p3p.s[i];
+      q.block0 = b3p;
+      q.nblocks = (int)((units[i] + U - 1) / U);
+      b3p += q.nblocks;
+      const int rc = uneven_field_map<R, C>(q.L, &q.fmap, q.T2, dims[i], q.nb);
+      if (rc) return rc;
+    }
+    p3p = sorted;
   }
   constexpr int NR = UnevenNT<C>::rows;
   int rc;
@@ -333,7 +457,8 @@ int apply_uneven(int dtype, int nseg, const em3d_segment* segs, void* ws, size_t
   if (rc) return rc;
   rc = uneven_launch(ku_strided<R, false>, p2, b2, UnevenNT<C>::strided, sm2, skip, st);
   if (rc) return rc;
-  rc = uneven_launch(ku_xmul<R, C, ADJ>, p3, b3, UnevenNT<C>::xmul, sm3, skip, st);
+  if (pipe) rc = uneven_launch(ku_xpipe<R, C, ADJ>, p3p, b3p, UnevenNT<C>::xmul, sm3p, skip, st);
+  else rc = uneven_launch(ku_xmul<R, C, ADJ>, p3, b3, UnevenNT<C>::xmul, sm3, skip, st);
   if (rc) return rc;
   rc = uneven_launch(ku_strided<R, true>, p4, b2, UnevenNT<C>::strided, sm2, skip, st);
   if (rc) return rc;

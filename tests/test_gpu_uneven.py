@@ -176,6 +176,10 @@ def test_uneven_stopped_entries_are_left_untouched(prec):
 
 
 def test_uneven_bicgstab_matches_problem_by_problem():
+    """Each entry's batched run is its single run: same status, iterations,
+    residual history and solution (the (32, 16, 48) problem stagnates near
+    1e-3 in both, the others converge; the stagnating entry keeps running
+    while the others have stopped and skip their work)."""
     import em3d_b200 as e
     from em3d_b200.groups import UnevenGroup
     from em3d_b200.solvers import BiCGStab, SolverConfig
@@ -188,12 +192,16 @@ def test_uneven_bicgstab_matches_problem_by_problem():
     for b in range(len(group)):
         p = group.problems[b]
         single = s.solve(e.Operator(p), p.wave)
-        assert batch[b].status == single.status == "converged", b
-        assert abs(batch[b].iterations - single.iterations) <= 1, b
+        assert batch[b].status == single.status, b
+        assert batch[b].iterations == single.iterations, b
+        np.testing.assert_allclose(batch[b].residual_history, single.residual_history, rtol=1e-9)
         assert batch[b].u.shape == p.wave.shape
         assert rel_err(batch[b].u.cpu().numpy(), single.u.cpu().numpy()) < 1e-8, b
         iters.append(single.iterations)
-    assert group.true_relative_residuals(group.pack([r.u for r in batch]), group.waves()).max() < 1e-9
+    done = [b for b in range(len(group)) if batch[b].status == "converged"]
+    assert len(done) == 3
+    res = group.true_relative_residuals(group.pack([r.u for r in batch]), group.waves())
+    assert max(res[b] for b in done) < 1e-9
     assert len(set(iters)) > 1
 
 
@@ -257,3 +265,30 @@ def test_uneven_group_rejects_unsupported():
     with pytest.raises(ValueError, match="at most 8"):
         UnevenGroup(_problems([(16, 16, n) for n in (16, 32, 48, 64, 80, 96, 128)] + [(32, 16, 16), (48, 16, 16)],
                               "double"))
+
+
+@pytest.mark.parametrize("variant", [-1, 0, 6])
+def test_uneven_x_pass_choices_agree(variant):
+    """The complex64 EM application runs its x pass pipelined (persistent
+    CTAs, field slab by TMA) by default and one tile per CTA when a
+    non-pipelined x-pass variant is selected; both equal the single
+    operators."""
+    import torch
+
+    from em3d_b200 import tune
+    from em3d_b200.groups import UnevenGroup
+
+    probs = _problems([(64, 64, 64), (32, 32, 32), (80, 80, 80), (48, 48, 48), (32, 32, 32)], "single")
+    group = UnevenGroup(probs)
+    x = group.pack([torch.randn(group.problem_shape(b), dtype=group._tc, device="cuda") for b in range(len(group))])
+    old = tune.get_xpass_variant()
+    try:
+        tune.set_xpass_variant(variant)
+        y = group.matvec(x)
+    finally:
+        tune.set_xpass_variant(old)
+    import em3d_b200 as e
+
+    for b, p in enumerate(group.problems):
+        ref = e.Operator(p).matvec(group.entry_field(x, b))
+        assert rel_err(group.entry_field(y, b).cpu().numpy(), ref.cpu().numpy()) < 2e-6, b
