@@ -1110,6 +1110,135 @@ __global__ void k_contract_blk(size_t outer, int L, int J, int inner, const floa
 
 
 // ---------------------------------------------------------------------------
+// The y and x truncated DFTs of one layer in one pass.  One CTA per
+// (batch x channel, kz mode) slice: forward, the slice Vz[x][y] (X x Y,
+// elements m apart in memory) goes to V[jx][jy] = sum_x fx[x][jx]
+// sum_y Vz[x][y] fy[y][jy] (2m x 2m); inverse, U[jx][jy] goes to
+// Uxy[x][y] = sum_jy iy[jy][y] sum_jx U[jx][jy] ix[jx][x].  The same sums as
+// the two contractions it replaces (k_contract_blk along y, then x), with
+// the intermediate in shared memory instead of global memory.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void cmac(float& re, float& im, float2 a, float2 b) {
+  re += a.x * b.x - a.y * b.y;
+  im += a.x * b.y + a.y * b.x;
+}
+
+// Each thread accumulates kSpecB outputs along the last index (NB apart, so
+// neighbouring threads read neighbouring elements), and a value read from
+// shared memory serves kSpecB products; rows of the slice are padded by one
+// element so the threads of a warp (several rows) hit different banks.
+constexpr int kSpecB = 4;
+
+__global__ void __launch_bounds__(256) k_spec_fwd(int X, int Y, int m, const float2* __restrict__ Vz,
+                                                  const float2* __restrict__ fy, const float2* __restrict__ fx,
+                                                  float2* __restrict__ V) {
+  const int J = 2 * m, NB = (J + kSpecB - 1) / kSpecB, YP = Y + 1;
+  const size_t bw = blockIdx.x;
+  const int k = blockIdx.y;
+  extern __shared__ float2 sh2[];
+  float2* S = sh2;            // X * (Y + 1)
+  float2* T = S + X * YP;     // X * J
+  float2* Fy = T + X * J;     // Y * J
+  float2* Fx = Fy + Y * J;    // X * J
+  const float2* src = Vz + bw * X * Y * m + k;
+  for (int i = threadIdx.x; i < X * Y; i += blockDim.x) {
+    const int x = i / Y;
+    S[i + x] = src[(size_t)i * m];
+  }
+  for (int i = threadIdx.x; i < Y * J; i += blockDim.x) Fy[i] = fy[i];
+  for (int i = threadIdx.x; i < X * J; i += blockDim.x) Fx[i] = fx[i];
+  __syncthreads();
+  // T[x][j] = sum_y S[x][y] Fy[y][j]
+  for (int o = threadIdx.x; o < X * NB; o += blockDim.x) {
+    const int x = o / NB, jb = o - x * NB;
+    float re[kSpecB] = {}, im[kSpecB] = {};
+    const float2* srow = S + x * YP;
+#pragma unroll 4
+    for (int y = 0; y < Y; ++y) {
+      const float2 a = srow[y];
+      const float2* f = Fy + y * J + jb;
+#pragma unroll
+      for (int jj = 0; jj < kSpecB; ++jj)
+        if (jb + jj * NB < J) cmac(re[jj], im[jj], a, f[jj * NB]);
+    }
+#pragma unroll
+    for (int jj = 0; jj < kSpecB; ++jj)
+      if (jb + jj * NB < J) T[x * J + jb + jj * NB] = make_float2(re[jj], im[jj]);
+  }
+  __syncthreads();
+  // V[jx][jy] = sum_x Fx[x][jx] T[x][jy]
+  float2* dst = V + bw * J * J * m + k;
+  for (int o = threadIdx.x; o < J * NB; o += blockDim.x) {
+    const int jx = o / NB, jb = o - jx * NB;
+    float re[kSpecB] = {}, im[kSpecB] = {};
+#pragma unroll 4
+    for (int x = 0; x < X; ++x) {
+      const float2 a = Fx[x * J + jx];
+      const float2* t = T + x * J + jb;
+#pragma unroll
+      for (int jj = 0; jj < kSpecB; ++jj)
+        if (jb + jj * NB < J) cmac(re[jj], im[jj], t[jj * NB], a);
+    }
+#pragma unroll
+    for (int jj = 0; jj < kSpecB; ++jj)
+      if (jb + jj * NB < J) dst[(size_t)(jx * J + jb + jj * NB) * m] = make_float2(re[jj], im[jj]);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_spec_inv(int X, int Y, int m, const float2* __restrict__ U,
+                                                  const float2* __restrict__ ix, const float2* __restrict__ iy,
+                                                  float2* __restrict__ Uxy) {
+  const int J = 2 * m, NB = (J + kSpecB - 1) / kSpecB, NYB = (Y + kSpecB - 1) / kSpecB;
+  const size_t bw = blockIdx.x;
+  const int k = blockIdx.y;
+  extern __shared__ float2 sh2[];
+  float2* Us = sh2;           // J * J
+  float2* T = Us + J * J;     // X * J
+  float2* Ix = T + X * J;     // J * X
+  float2* Iy = Ix + J * X;    // J * Y
+  const float2* src = U + bw * J * J * m + k;
+  for (int i = threadIdx.x; i < J * J; i += blockDim.x) Us[i] = src[(size_t)i * m];
+  for (int i = threadIdx.x; i < J * X; i += blockDim.x) Ix[i] = ix[i];
+  for (int i = threadIdx.x; i < J * Y; i += blockDim.x) Iy[i] = iy[i];
+  __syncthreads();
+  // T[x][jy] = sum_jx Us[jx][jy] Ix[jx][x]
+  for (int o = threadIdx.x; o < X * NB; o += blockDim.x) {
+    const int x = o / NB, jb = o - x * NB;
+    float re[kSpecB] = {}, im[kSpecB] = {};
+#pragma unroll 4
+    for (int jx = 0; jx < J; ++jx) {
+      const float2 a = Ix[jx * X + x];
+      const float2* u = Us + jx * J + jb;
+#pragma unroll
+      for (int jj = 0; jj < kSpecB; ++jj)
+        if (jb + jj * NB < J) cmac(re[jj], im[jj], u[jj * NB], a);
+    }
+#pragma unroll
+    for (int jj = 0; jj < kSpecB; ++jj)
+      if (jb + jj * NB < J) T[x * J + jb + jj * NB] = make_float2(re[jj], im[jj]);
+  }
+  __syncthreads();
+  // Uxy[x][y] = sum_jy T[x][jy] Iy[jy][y]
+  float2* dst = Uxy + bw * X * Y * m + k;
+  for (int o = threadIdx.x; o < X * NYB; o += blockDim.x) {
+    const int x = o / NYB, yb = o - x * NYB;
+    float re[kSpecB] = {}, im[kSpecB] = {};
+#pragma unroll 4
+    for (int jy = 0; jy < J; ++jy) {
+      const float2 a = T[x * J + jy];
+      const float2* f = Iy + jy * Y + yb;
+#pragma unroll
+      for (int yy = 0; yy < kSpecB; ++yy)
+        if (yb + yy * NYB < Y) cmac(re[yy], im[yy], a, f[yy * NYB]);
+    }
+#pragma unroll
+    for (int yy = 0; yy < kSpecB; ++yy)
+      if (yb + yy * NYB < Y) dst[(size_t)(x * Y + yb + yy * NYB) * m] = make_float2(re[yy], im[yy]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Grid resampling for evaluating the network on the half-resolution grid:
 // 2x2x2 cell means down (complex64 or complex128 in, complex64 out) and
 // trilinear interpolation up between cell centres (clamped at the faces, the
@@ -1316,6 +1445,38 @@ int em3d_fno_contract(int kind, int act, size_t outer, int L, int J, int inner, 
   } else {
     em3d_set_last_error("contract kind must be 0 (real->complex), 1 (complex), 2 (complex->real, accumulate)");
     return EM3D_ERR_INVALID;
+  }
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_fno_spectral(int inverse, int BW, int m, int X, int Y, const void* in, const void* mx, const void* my,
+                      void* out, void* stream) {
+  if (BW < 1 || m < 1 || X < 2 * m || Y < 2 * m || !in || !mx || !my || !out) {
+    em3d_set_last_error("em3d_fno_spectral: bad sizes or NULL arrays (need X, Y >= 2 m)");
+    return EM3D_ERR_INVALID;
+  }
+  const size_t J = 2 * (size_t)m;
+  const size_t smem = sizeof(float2) * (inverse ? J * J + 2 * (size_t)X * J + J * Y
+                                                : (size_t)X * (Y + 1) + 2 * (size_t)X * J + (size_t)Y * J);
+  if (smem > 227 * 1024) {
+    em3d_set_last_error("em3d_fno_spectral: slice too large for shared memory (use em3d_fno_contract)");
+    return EM3D_ERR_UNSUPPORTED;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const dim3 grid(BW, m);
+  static bool opted = false;  // both kernels opted in to 227 KB once (first call outside any capture)
+  if (!opted) {
+    EM3D_CUDA_TRY(cudaFuncSetAttribute(k_spec_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    EM3D_CUDA_TRY(cudaFuncSetAttribute(k_spec_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    opted = true;
+  }
+  if (inverse) {
+    k_spec_inv<<<grid, 256, smem, st>>>(X, Y, m, (const float2*)in, (const float2*)mx, (const float2*)my,
+                                        (float2*)out);
+  } else {
+    k_spec_fwd<<<grid, 256, smem, st>>>(X, Y, m, (const float2*)in, (const float2*)my, (const float2*)mx,
+                                        (float2*)out);
   }
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;

@@ -575,6 +575,19 @@ inline int nblocks(size_t n) {
   return (int)(b ? b : 1);
 }
 
+// CTAs per right-hand side of a batched launch: one wave of 256-thread CTAs
+// for a single right-hand side; for a batch, about two waves in all (at least
+// 32 per right-hand side), so that a wide batch does not launch a full wave
+// for every entry (most of whose CTAs would find little to do, or nothing
+// beyond a short entry's n_used).
+inline int nblocks_batch(size_t n, int batch) {
+  const int full = nblocks(n);
+  if (batch <= 1) return full;
+  int share = (2 * kMaxBlocks + batch - 1) / batch;
+  if (share < 32) share = 32;
+  return full < share ? full : share;
+}
+
 #define EM3D_DTYPE_DISPATCH(dtype, CALL)                                          \
   do {                                                                            \
     if ((dtype) == EM3D_C64) { using R = float; CALL; }                          \
@@ -616,7 +629,7 @@ int em3d_vec_dots(int dtype, size_t n, int batch, const void* x0, const void* y0
   if (int rc = check_batch(batch, state_stride)) return rc;
   if (!x0 || !y0 || (x1 && !y1)) { em3d_set_last_error("NULL vector"); return EM3D_ERR_INVALID; }
   cudaStream_t st = (cudaStream_t)stream;
-  const dim3 grid(nblocks(n), batch);
+  const dim3 grid(nblocks_batch(n, batch), batch);
   EM3D_DTYPE_DISPATCH(dtype, (k_dots<R><<<grid, kThreads, 0, st>>>(n, (const cx<R>*)x0, (const cx<R>*)y0,
                                                                      (const cx<R>*)x1, (const cx<R>*)y1, state,
                                                                      state_stride)));
@@ -657,7 +670,7 @@ int em3d_vec_convert(size_t n, int src_dtype, const void* src, int dst_dtype, vo
     if (int rc = check_state(state, n)) return rc;                                    \
     if (int rc = check_batch(batch, sstride)) return rc;                              \
     cudaStream_t st = (cudaStream_t)stream;                                           \
-    const dim3 grid(nblocks(n), batch);                                               \
+    const dim3 grid(nblocks_batch(n, batch), batch);                                  \
     EM3D_DTYPE_DISPATCH(dtype, (KERNEL<R><<<grid, kThreads, 0, st>>> ARGS));          \
     EM3D_LAUNCH_CHECK();                                                              \
     return EM3D_OK;                                                                   \

@@ -158,18 +158,32 @@ class FNO:
             return self._forward_rows(chi, wave, train)
         return self._forward_passes(chi, wave, train)
 
+    # the y and x DFTs of a layer in one launch each way (em3d_fno_spectral);
+    # False: two contractions each way (em3d_fno_contract)
+    fused_spectral = True
+
     def _spectral(self, l, B, N, buf, mats, V):
         """Vz (truncated z-DFT of the layer input) -> Uxy (modes mixed, x and y inverted)."""
         X, Y, Z = N
         W, m = self.W, self.m
         nm = 4 * m * m * m
         st = _lib.stream_handle()
-        self._contract(1, 0, B * W * X, Y, 2 * m, m, buf["Vz"], mats["fy"], buf["Vy"])
-        self._contract(1, 0, B * W, X, 2 * m, 2 * m * m, buf["Vy"], mats["fx"], V)
+        fused = self.fused_spectral and 8 * (X * (Y + 1) + 6 * m * max(X, Y) + 4 * m * m) <= 227 * 1024
+        if fused:
+            # y and x DFTs in one launch (one CTA per channel slice and kz mode)
+            _lib.call("em3d_fno_spectral", 0, B * W, m, X, Y, buf["Vz"].data_ptr(), mats["fx"].data_ptr(),
+                      mats["fy"].data_ptr(), V.data_ptr(), st)
+        else:
+            self._contract(1, 0, B * W * X, Y, 2 * m, m, buf["Vz"], mats["fy"], buf["Vy"])
+            self._contract(1, 0, B * W, X, 2 * m, 2 * m * m, buf["Vy"], mats["fx"], V)
         _lib.call("em3d_fno_modemix", self.act, B, W, nm, V.data_ptr(), self._w(f"Wre{l}").data_ptr(),
                   self._w(f"Wim{l}").data_ptr(), buf["U"].data_ptr(), st)
-        self._contract(1, 0, B * W, 2 * m, X, 2 * m * m, buf["U"], mats["ix"], buf["Ux"])
-        self._contract(1, 0, B * W * X, 2 * m, Y, m, buf["Ux"], mats["iy"], buf["Uxy"])
+        if fused:
+            _lib.call("em3d_fno_spectral", 1, B * W, m, X, Y, buf["U"].data_ptr(), mats["ix"].data_ptr(),
+                      mats["iy"].data_ptr(), buf["Uxy"].data_ptr(), st)
+        else:
+            self._contract(1, 0, B * W, 2 * m, X, 2 * m * m, buf["U"], mats["ix"], buf["Ux"])
+            self._contract(1, 0, B * W * X, 2 * m, Y, m, buf["Ux"], mats["iy"], buf["Uxy"])
 
     def _forward_rows(self, chi, wave, train):
         """Forward with the fused z-row kernel: lift + first z-DFT, then per

@@ -377,6 +377,14 @@ int em3d_fno_lift_bwd(int B, size_t ncell, int W, const void* chi, const void* w
 /* kind 0: real(act) -> complex; 1: complex -> complex; 2: complex -> real, += Re(.) */
 int em3d_fno_contract(int kind, int act, size_t outer, int L, int J, int inner, const void* X, const void* M, void* Y,
                       void* stream);
+/* The y and x truncated DFTs of a layer in one launch, one CTA per (batch x
+ * channel, kz) slice.  inverse = 0: in = Vz (BW, X, Y, m), mx = the x matrix
+ * (X, 2m), my = the y matrix (Y, 2m), out = V (BW, 2m, 2m, m); inverse = 1:
+ * in = U (BW, 2m, 2m, m), mx = (2m, X), my = (2m, Y), out = Uxy (BW, X, Y, m).
+ * Equals em3d_fno_contract along y then x (inverse: x then y) up to FP32
+ * rounding.  EM3D_ERR_UNSUPPORTED when a slice does not fit in shared memory. */
+int em3d_fno_spectral(int inverse, int BW, int m, int X, int Y, const void* in, const void* mx, const void* my,
+                      void* out, void* stream);
 int em3d_fno_modemix(int act, int B, int W, int nm, const void* V, const void* Wre, const void* Wim, void* U,
                      void* stream);
 int em3d_fno_modemix_bwd(int act, int B, int W, int nm, const void* V, const void* dU, const void* Wre,
