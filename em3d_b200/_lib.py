@@ -99,6 +99,7 @@ SIGNATURES = {
                                               c_void_p]),
     "em3d_static_scratch_bytes": (c_size_t, []),
     "em3d_farfield_workspace_bytes": (c_size_t, [_GRID, c_int]),
+    "em3d_fno_failures": (c_int, [c_int]),
     "em3d_fno_spectral": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                   c_void_p]),
     "em3d_em_farfield": (c_int, [_GRID, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_double,

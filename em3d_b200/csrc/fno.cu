@@ -21,6 +21,7 @@
 #include <math.h>
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace em3d {
 namespace fno {
@@ -1325,6 +1326,12 @@ inline int blocks_for(size_t n, int threads = 256) {
   return (int)(b ? b : 1);
 }
 
+#include "fno_umma.cuh"
+
+// Failed bounded waits of the tcgen05 row pass (read and cleared by
+// em3d_fno_failures).
+__device__ unsigned int g_fno_fails = 0;
+
 }  // namespace fno
 }  // namespace em3d
 
@@ -1450,6 +1457,19 @@ int em3d_fno_contract(int kind, int act, size_t outer, int L, int J, int inner, 
   return EM3D_OK;
 }
 
+int em3d_fno_failures(int reset) {
+  unsigned int n = 0;
+  if (cudaMemcpyFromSymbol(&n, g_fno_fails, sizeof n) != cudaSuccess) {
+    em3d_set_last_error("em3d_fno_failures: cannot read the counter");
+    return -1;
+  }
+  if (reset && n) {
+    const unsigned int zero = 0;
+    if (cudaMemcpyToSymbol(g_fno_fails, &zero, sizeof zero) != cudaSuccess) return -1;
+  }
+  return (int)n;
+}
+
 int em3d_fno_spectral(int inverse, int BW, int m, int X, int Y, const void* in, const void* mx, const void* my,
                       void* out, void* stream) {
   if (BW < 1 || m < 1 || X < 2 * m || Y < 2 * m || !in || !mx || !my || !out) {
@@ -1514,6 +1534,20 @@ int em3d_fno_row_forward(int act, int lift, int B, int W, int X, int Y, int Z, i
     const size_t tgroups = ((size_t)B * X * Y + Rt - 1) / Rt;
     const int tgrid = (int)(tgroups < (size_t)148 * 8 ? tgroups : (size_t)148 * 8);
     using BF = __nv_bfloat16;
+    if (!lift && em3d_get_tuning(EM3D_TUNE_FNO_SIMT) == 2) {
+      // the layer pass on tcgen05 (fno_umma.cuh)
+      static unsigned int* fails = nullptr;
+      if (fails == nullptr) EM3D_CUDA_TRY(cudaGetSymbolAddress((void**)&fails, g_fno_fails));
+      const size_t usm = UmmaSmem::TOTAL;
+      if (!allow_dyn_smem((const void*)k_row_fwd_umma, usm)) return EM3D_ERR_CUDA;
+      const size_t tiles = ((size_t)B * X * Y + Rt - 1) / Rt;
+      const int ugrid = (int)(tiles < (size_t)148 * 2 ? tiles : (size_t)148 * 2);
+      k_row_fwd_umma<<<ugrid, 128, usm, st>>>(B, X, Y, Z, m, (const BF*)vin, (const float2*)Uxy, (const BF*)Wt,
+                                               bias, apply_gelu, (BF*)pre_out, (BF*)vout, (float2*)Vz,
+                                               (const BF*)Q, qb, (const float2*)wave, (float2*)u_out, fails);
+      EM3D_LAUNCH_CHECK();
+      return EM3D_OK;
+    }
     if (lift) {
       if (!allow_dyn_smem((const void*)k_row_fwd_tc<true>, tsm)) return EM3D_ERR_CUDA;
       k_row_fwd_tc<true><<<tgrid, 128, tsm, st>>>(B, X, Y, Z, m, (const float2*)chi, (const float2*)wave, nullptr,

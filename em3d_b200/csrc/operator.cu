@@ -149,8 +149,8 @@ int em3d_set_tuning(int key, int value) {
     em3d_set_last_error("x-pass variant must be -1 (automatic) or 0 .. 10");
     return EM3D_ERR_INVALID;
   }
-  if (key == EM3D_TUNE_FNO_SIMT && value != 0 && value != 1) {
-    em3d_set_last_error("FNO row-pass switch must be 0 or 1");
+  if (key == EM3D_TUNE_FNO_SIMT && (value < 0 || value > 2)) {
+    em3d_set_last_error("FNO row-pass switch must be 0, 1 or 2");
     return EM3D_ERR_INVALID;
   }
   if (key == EM3D_TUNE_FNO_CONTRACT && value != 0 && value != 2 && value != 4 && value != 8 && value != 12 &&

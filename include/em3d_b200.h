@@ -71,7 +71,8 @@ enum em3d_tune_key {
                                    shared memory does not fit is replaced by the first that fits in the
                                    order 6, 4, 1, 2, 0, 5, 3 */
   EM3D_TUNE_FFT_GENERIC = 1,   /* 1 = use the generic shared-memory FFT passes for every axis length */
-  EM3D_TUNE_FNO_SIMT = 2,      /* 1 = FNO row pass on CUDA cores even where the tensor-core one applies */
+  EM3D_TUNE_FNO_SIMT = 2,      /* FNO row pass: 0 = warp-level tensor cores (mma.sync) where they apply, 1 = CUDA cores,
+                                   2 = fifth-generation tensor cores (tcgen05, TMEM accumulators) for the layer passes */
   EM3D_TUNE_FNO_CONTRACT = 3,  /* FNO truncated-DFT contractions: 0 automatic, else outputs per thread (2, 4, 8, 12, 24) */
   EM3D_TUNE_COUNT = 4,
 };
@@ -383,6 +384,10 @@ int em3d_fno_contract(int kind, int act, size_t outer, int L, int J, int inner, 
  * in = U (BW, 2m, 2m, m), mx = (2m, X), my = (2m, Y), out = Uxy (BW, X, Y, m).
  * Equals em3d_fno_contract along y then x (inverse: x then y) up to FP32
  * rounding.  EM3D_ERR_UNSUPPORTED when a slice does not fit in shared memory. */
+/* Bounded waits of the tcgen05 row pass that gave up since the last reset (the
+ * outputs of those launches are invalid); reset = 1 clears the count.  Reads a
+ * device counter (synchronous); -1 when it cannot be read. */
+int em3d_fno_failures(int reset);
 int em3d_fno_spectral(int inverse, int BW, int m, int X, int Y, const void* in, const void* mx, const void* my,
                       void* out, void* stream);
 int em3d_fno_modemix(int act, int B, int W, int nm, const void* V, const void* Wre, const void* Wim, void* U,

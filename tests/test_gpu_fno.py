@@ -152,6 +152,44 @@ def test_tensor_core_row_pass_matches_cuda_core_pass(N, m):
             assert float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)) < 3e-2
 
 
+@pytest.mark.parametrize("N,m", [((7, 9, 32), 3), ((24, 26, 64), 12), ((24, 24, 128), 12), ((32, 33, 128), 16)])
+def test_tcgen05_row_pass_matches_mma_sync_pass(N, m):
+    """bf16, width 32: the layer pass on tcgen05 (TMEM accumulators, block-
+    diagonal DFT tables as MMA operands) against the mma.sync one, in
+    inference and training mode (the last tile of (7, 9, 32) is partial);
+    no bounded wait gives up."""
+    import torch
+
+    from em3d_b200 import _lib
+    from em3d_b200.fno import FNO
+
+    rng = np.random.default_rng(13)
+    B = 2
+    chi = torch.as_tensor((_rand(rng, (B, 3, 3) + N) * 0.3).astype(np.complex64), device="cuda")
+    wave = torch.as_tensor(_rand(rng, (B, 3) + N).astype(np.complex64), device="cuda")
+    net = FNO(width=32, modes=m, layers=3, act="bf16", seed=3)
+    _lib.load().em3d_fno_failures(1)
+    out = {}
+    try:
+        for mode in (0, 2):
+            _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FNO_SIMT, mode)
+            for train in (False, True):
+                u = net.forward(chi, wave, train).clone()
+                bufs = net._buffers(B, N, train)
+                acts = [t.float().clone() for t in bufs["v"]] if train else []
+                pre = [t.float().clone() for t in bufs["pre"]] if train else []
+                out[(mode, train)] = (u, acts, pre)
+    finally:
+        _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FNO_SIMT, 0)
+    torch.cuda.synchronize()
+    assert _lib.load().em3d_fno_failures(1) == 0
+    for train in (False, True):
+        a, b = out[(2, train)][0] - wave, out[(0, train)][0] - wave   # the network's output proper
+        assert float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) < 1e-2
+        for x, y in zip(out[(2, train)][1] + out[(2, train)][2], out[(0, train)][1] + out[(0, train)][2]):
+            assert float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)) < 1e-2
+
+
 @pytest.mark.parametrize("src", ["complex64", "complex128"])
 def test_half_grid_resampling_matches_torch(src):
     """2x2x2 means and trilinear interpolation between cell centres against
