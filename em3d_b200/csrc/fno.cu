@@ -34,6 +34,10 @@ template <> __device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat
 template <typename A> __device__ __forceinline__ A st(float v) { return (A)v; }
 template <> __device__ __forceinline__ __nv_bfloat16 st<__nv_bfloat16>(float v) { return __float2bfloat16(v); }
 
+// Row index -> batch entry: the row passes check that B X Y < 2^32, so the
+// division runs in 32 bits (a 64-bit one is a long instruction sequence).
+__device__ __forceinline__ size_t row_batch(size_t row, size_t XY) { return (size_t)((uint32_t)row / (uint32_t)XY); }
+
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float x) {
   return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
@@ -609,7 +613,7 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
         const size_t row = row0 + r;
         float2 val = make_float2(0.0f, 0.0f);
         if (row < nrows && co < W && k < m) {
-          const size_t b = row / XY, xy = row - b * XY;
+          const size_t b = row_batch(row, XY), xy = row - b * XY;
           val = Uxy[((b * W + co) * XY + xy) * m + k];
         }
         sU[i] = val;
@@ -619,7 +623,7 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
     const size_t row = row0 + rr;
     const bool valid = lane_on && row < nrows;
     if (valid) {
-      const size_t b = row / XY, xy = row - b * XY;
+      const size_t b = row_batch(row, XY), xy = row - b * XY;
       const size_t cell = xy * Z + z;
       const size_t base = b * W * ncell + cell;
       float o[kMaxWidth];
@@ -731,7 +735,7 @@ __global__ void __launch_bounds__(kRowThreads) k_row_fwd(
               im[d] += tzz * w.y;
             }
           }
-          const size_t b = rw / XY, xy = rw - b * XY;
+          const size_t b = row_batch(rw, XY), xy = rw - b * XY;
           float2* dst = Vz + ((b * W + co) * XY + xy) * m;
 #pragma unroll
           for (int d = 0; d < 4; ++d)
@@ -874,7 +878,7 @@ __global__ void __launch_bounds__(128) k_row_fwd_tc(
         const size_t row = row0 + r;
         float f[kFeat];
         if (row < nrows) {
-          const size_t b = row / XY, xy = row - b * XY;
+          const size_t b = row_batch(row, XY), xy = row - b * XY;
           cell_features(chi, wave, ncell, (int)b, xy * Z + z, f);
         } else {
 #pragma unroll
@@ -890,7 +894,7 @@ __global__ void __launch_bounds__(128) k_row_fwd_tc(
         const size_t row = row0 + r;
         uint4 val = make_uint4(0, 0, 0, 0);
         if (row < nrows) {
-          const size_t b = row / XY, xy = row - b * XY;
+          const size_t b = row_batch(row, XY), xy = row - b * XY;
           val = *reinterpret_cast<const uint4*>(vin + (b * W + ci) * ncell + xy * Z + q * 8);
         }
         *reinterpret_cast<uint4*>(Vs + ci * kTcCols + r * Z + q * 8) = val;
@@ -901,7 +905,7 @@ __global__ void __launch_bounds__(128) k_row_fwd_tc(
         const size_t row = row0 + r;
         float2 val = make_float2(0.0f, 0.0f);
         if (row < nrows && k < m) {
-          const size_t b = row / XY, xy = row - b * XY;
+          const size_t b = row_batch(row, XY), xy = row - b * XY;
           val = Uxy[((b * W + co) * XY + xy) * m + k];
         }
         sU[i] = val;
@@ -954,7 +958,7 @@ __global__ void __launch_bounds__(128) k_row_fwd_tc(
     // ---- epilogue: bias, GELU, bf16; keep the rounded values for GEMM 2
     const size_t row = row0 + wr;
     const bool valid = row < nrows;
-    const size_t b = valid ? row / XY : 0, xy = valid ? row - b * XY : 0;
+    const size_t b = valid ? row_batch(row, XY) : 0, xy = valid ? row - b * XY : 0;
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -1018,7 +1022,7 @@ __global__ void __launch_bounds__(128) k_row_fwd_tc(
             re += red[(w * 32 + co) * 32 + 2 * k];
             im += red[(w * 32 + co) * 32 + 2 * k + 1];
           }
-          const size_t bb = rw / XY, xyy = rw - bb * XY;
+          const size_t bb = row_batch(rw, XY), xyy = rw - bb * XY;
           Vz[((bb * W + co) * XY + xyy) * m + k] = make_float2(re, im);
         }
       }
@@ -1029,7 +1033,7 @@ __global__ void __launch_bounds__(128) k_row_fwd_tc(
         const int r = i / (32 * chunks), rem = i - r * 32 * chunks, co = rem / chunks, q = rem - co * chunks;
         const size_t rw = row0 + r;
         if (rw < nrows) {
-          const size_t bb = rw / XY, xyy = rw - bb * XY;
+          const size_t bb = row_batch(rw, XY), xyy = rw - bb * XY;
           *reinterpret_cast<uint4*>(vout + (bb * W + co) * ncell + xyy * Z + q * 8) =
               *reinterpret_cast<const uint4*>(Os + co * kTcCols + r * Z + q * 8);
         }
@@ -1049,7 +1053,7 @@ __global__ void __launch_bounds__(128) k_row_fwd_tc(
 #pragma unroll
             for (int j = 0; j < 6; ++j) p[j] += sQ[j * 32 + co] * o;
           }
-          const size_t bb = rw / XY, xyy = rw - bb * XY;
+          const size_t bb = row_batch(rw, XY), xyy = rw - bb * XY;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             const size_t idx = (bb * 3 + c) * ncell + xyy * Z + z;
@@ -1509,6 +1513,10 @@ int em3d_fno_row_forward(int act, int lift, int B, int W, int X, int Y, int Z, i
   if (int rc = check_width(W)) return rc;
   if (Z < 1 || Z > kRowThreads || m < 1 || m > kMaxModes || 2 * m > Z || X < 1 || Y < 1 || B < 1) {
     em3d_set_last_error("row_forward: needs 1 <= Z <= 128, 1 <= modes <= 16, 2 modes <= Z");
+    return EM3D_ERR_UNSUPPORTED;
+  }
+  if ((size_t)B * X * Y >= ((size_t)1 << 32)) {
+    em3d_set_last_error("row_forward: B X Y must stay below 2^32 rows");
     return EM3D_ERR_UNSUPPORTED;
   }
   if (lift ? (!chi || !wave) : (!vin || !Uxy)) {

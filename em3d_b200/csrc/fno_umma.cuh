@@ -171,7 +171,7 @@ k_row_fwd_umma(int B, int X, int Y, int Z, int m, const __nv_bfloat16* __restric
       const size_t row = row0 + r;
       uint4 val = make_uint4(0, 0, 0, 0);
       if (row < nrows) {
-        const size_t b = row / XY, xy = row - b * XY;
+        const size_t b = row_batch(row, XY), xy = row - b * XY;
         val = *reinterpret_cast<const uint4*>(vin + (b * W + ci) * ncell + xy * Z + q * 8);
       }
       const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&val);
@@ -184,7 +184,7 @@ k_row_fwd_umma(int B, int X, int Y, int Z, int m, const __nv_bfloat16* __restric
       const size_t row = row0 + r;
       float2 u = make_float2(0.0f, 0.0f);
       if (row < nrows && k < m) {
-        const size_t b = row / XY, xy = row - b * XY;
+        const size_t b = row_batch(row, XY), xy = row - b * XY;
         u = Uxy[((b * W + co) * XY + xy) * m + k];
       }
       const int col = r * 32 + 2 * k;
@@ -220,7 +220,7 @@ k_row_fwd_umma(int B, int X, int Y, int Z, int m, const __nv_bfloat16* __restric
       const int cell = tid, r = cell / Z, z = cell - r * Z;
       const size_t row = row0 + r;
       const bool valid = row < nrows;
-      const size_t b = valid ? row / XY : 0, xy = valid ? row - b * XY : 0;
+      const size_t b = valid ? row_batch(row, XY) : 0, xy = valid ? row - b * XY : 0;
       const size_t at = xy * Z + z;
       float p[6];
 #pragma unroll
@@ -272,7 +272,7 @@ k_row_fwd_umma(int B, int X, int Y, int Z, int m, const __nv_bfloat16* __restric
         tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 32u, e);
         const size_t row = row0 + warp;
         const bool ok = row < nrows && (lane & 1) == 0 && (lane >> 1) < m;
-        const size_t b = row < nrows ? row / XY : 0, xy = row < nrows ? row - b * XY : 0;
+        const size_t b = row < nrows ? row_batch(row, XY) : 0, xy = row < nrows ? row - b * XY : 0;
 #pragma unroll
         for (int co = 0; co < W; ++co) {
           const float im = __shfl_down_sync(0xffffffffu, e[co], 1);
