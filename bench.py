@@ -487,6 +487,31 @@ def run_ours(args, world, rank, local):
                "mixed_solution_rel_err_vs_fp64": float(torch.linalg.vector_norm(r10.u - b10.u)
                                                        / torch.linalg.vector_norm(b10.u))}
     del dc10, bic10, r10, b10
+    # SIM on the same problem, its step 1/mu from the coarse (4^3) operator's
+    # eigenvalues (gamma0.estimate_from_problem), FP64, to true rtol 1e-6
+    from em3d_b200 import gamma0
+    from em3d_b200.solvers import SIM
+
+    t0 = time.perf_counter()
+    try:
+        g0 = gamma0.estimate_from_problem(p2, coarse_N=(4, 4, 4))
+    except ValueError as exc:  # the reference's estimate raises the same for this spectrum
+        g0, gamma_error = None, str(exc)
+    gamma_s = time.perf_counter() - t0
+    if g0 is None:
+        aniso_sim = {"applicable": False, "reason": gamma_error, "gamma0_ms": 1000.0 * gamma_s}
+    else:
+        sim_cfg = SolverConfig(max_iter=3000, rtol=RTOL, **g0.as_solver_config_kwargs())
+        sim = SIM(sim_cfg)
+        sim.solve(a64, p2.wave)
+        sim_ms, rs = _events_ms(lambda: sim.solve(a64, p2.wave))
+        aniso_sim = {"applicable": True, "rtol_true": RTOL, "mu": [float(np.real(g0.mu)), float(np.imag(g0.mu))],
+                     "radius": float(g0.radius), "gamma0_ms": 1000.0 * gamma_s, "fp64_ms": sim_ms,
+                     "status": rs.status, "iterations": rs.iterations,
+                     "true_residual": float(true_relative_residual(a64, rs.u, p2.wave)),
+                     "solution_rel_err_vs_bicgstab": float(torch.linalg.vector_norm(rs.u - b2.u)
+                                                          / torch.linalg.vector_norm(b2.u))}
+        del sim, rs
 
     # -- 4a. the README sphere (16^3, k0 = 4): RCS against Mie from this library's solve
     from em3d_b200 import mie
@@ -755,7 +780,7 @@ def run_ours(args, world, rank, local):
                             "mixed_true_residual": float(true_relative_residual(a64, r2.u, p2.wave)),
                             "mixed_solution_rel_err_vs_fp64": aniso_err,
                             "fp64_true_residual": float(true_relative_residual(a64, b2.u, p2.wave)),
-                            "rtol_1e-10": aniso10},
+                            "rtol_1e-10": aniso10, "sim": aniso_sim},
         "acoustic_spheres": acoustic,
         "multi_rhs": multi_rhs,
         "uneven_problems": uneven,

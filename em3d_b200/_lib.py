@@ -100,6 +100,10 @@ SIGNATURES = {
     "em3d_static_scratch_bytes": (c_size_t, []),
     "em3d_farfield_workspace_bytes": (c_size_t, [_GRID, c_int]),
     "em3d_fno_failures": (c_int, [c_int]),
+    "em3d_matvec_dot_parts": (c_int, [c_int, _GRID, c_int]),
+    "em3d_matvec_dots": (c_int, [c_int, _GRID, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_size_t, c_void_p, c_void_p, c_void_p]),
+    "em3d_bicgstab_omega_parts": (c_int, [c_int, c_void_p, c_void_p, c_void_p]),
     "em3d_fno_spectral": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                   c_void_p]),
     "em3d_em_farfield": (c_int, [_GRID, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_double,
@@ -203,7 +207,7 @@ LAUNCHES = {
     "em3d_em_matvec_chi": 5, "em3d_em_rmatvec_chi": 5, "em3d_em_matvec_grouped": 5, "em3d_em_rmatvec_grouped": 5,
     "em3d_acoustic_matvec_grouped": 5, "em3d_acoustic_rmatvec_grouped": 5,
     "em3d_em_matvec_uneven": 5, "em3d_em_rmatvec_uneven": 5, "em3d_acoustic_matvec_uneven": 5,
-    "em3d_acoustic_rmatvec_uneven": 5,
+    "em3d_acoustic_rmatvec_uneven": 5, "em3d_matvec_dots": 5,
 }
 # Kernels launched by this process (graph replays add their captured counts).
 # Host threads update it under a lock; a thread that is capturing a graph

@@ -71,6 +71,9 @@ struct BatchStrides {
   // element stride between the entries' fields u / out (register row passes);
   // 0: back to back (C cells each)
   size_t field = 0;
+  // nullable: the last pass of a matvec also writes, per CTA, the partial
+  // sums |t|^2, Re and Im of vdot(t, u) of its output t = u - y (one entry)
+  double* dots = nullptr;
 };
 
 // Index of entry (r, c) of a symmetric 3x3 contrast stored as its six

@@ -1536,13 +1536,14 @@ int em3d_fno_row_forward(int act, int lift, int B, int W, int X, int Y, int Z, i
   const int R = kRowThreads / Z;
   const size_t groups = ((size_t)B * X * Y + R - 1) / R;
   const int grid = (int)(groups < (size_t)148 * 12 ? groups : (size_t)148 * 12);
-  if (act == FNO_BF16 && W == 32 && Z % 32 == 0 && em3d_get_tuning(EM3D_TUNE_FNO_SIMT) == 0) {
+  const int row_mode = em3d_get_tuning(EM3D_TUNE_FNO_SIMT);  // 0 auto, 1 CUDA cores, 2 tcgen05, 3 mma.sync
+  if (act == FNO_BF16 && W == 32 && Z % 32 == 0 && row_mode != 1) {
     const size_t tsm = row_fwd_tc_smem();
     const int Rt = 128 / Z;
     const size_t tgroups = ((size_t)B * X * Y + Rt - 1) / Rt;
     const int tgrid = (int)(tgroups < (size_t)148 * 8 ? tgroups : (size_t)148 * 8);
     using BF = __nv_bfloat16;
-    if (!lift && em3d_get_tuning(EM3D_TUNE_FNO_SIMT) == 2) {
+    if (!lift && row_mode != 3) {
       // the layer pass on tcgen05 (fno_umma.cuh)
       static unsigned int* fails = nullptr;
       if (fails == nullptr) EM3D_CUDA_TRY(cudaGetSymbolAddress((void**)&fails, g_fno_fails));

@@ -313,6 +313,29 @@ __global__ void __launch_bounds__(kThreads) k_bicg_s(size_t n, void* state, size
   }
 }
 
+// omega = ts / tt from tot = (tt, Re ts, Im ts), with the breakdown checks
+// (src/em3d/solvers/bicgstab.py:153-170); one thread.
+__device__ inline void omega_from_dots(StateView& sv, void* state, const double (&tot)[3]) {
+  em3d_krylov_state* st = sv.st;
+  st->matvecs += 1;
+  const double tt = tot[0];
+  int stop = EM3D_RUNNING;
+  if (fabs(tt) < 1e-30 * st->rhs_norm * st->rhs_norm) {
+    stop = EM3D_BREAKDOWN_T;
+  } else {
+    const double2 om = make_double2(tot[1] / tt, tot[2] / tt);
+    st->omega_re = om.x;
+    st->omega_im = om.y;
+    if (cabs2(om) == 0.0) stop = EM3D_BREAKDOWN_OMEGA;
+  }
+  if (stop != EM3D_RUNNING) {
+    record(sv, st->last_rel, st->matvecs);
+    st->iter += 1;
+    st->pending = 1;
+    stop_rhs(st, state, stop);
+  }
+}
+
 // tt = vdot(t, t), ts = vdot(t, s); omega = ts / tt with the breakdown checks.
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_bicg_omega(size_t n, void* state, size_t sstride, const cx<R>* t, const cx<R>* s) {
@@ -327,26 +350,22 @@ __global__ void __launch_bounds__(kThreads) k_bicg_omega(size_t n, void* state, 
     acc_dot(a[1], a[2], ti, s[i]);
   }
   double tot[3];
-  if (reduce_last<3>(sv, a, tot) && threadIdx.x == 0) {
-    em3d_krylov_state* st = sv.st;
-    st->matvecs += 1;
-    const double tt = tot[0];
-    int stop = EM3D_RUNNING;
-    if (fabs(tt) < 1e-30 * st->rhs_norm * st->rhs_norm) {
-      stop = EM3D_BREAKDOWN_T;
-    } else {
-      const double2 om = make_double2(tot[1] / tt, tot[2] / tt);
-      st->omega_re = om.x;
-      st->omega_im = om.y;
-      if (cabs2(om) == 0.0) stop = EM3D_BREAKDOWN_OMEGA;
-    }
-    if (stop != EM3D_RUNNING) {
-      record(sv, st->last_rel, st->matvecs);
-      st->iter += 1;
-      st->pending = 1;
-      stop_rhs(st, state, stop);
-    }
+  if (reduce_last<3>(sv, a, tot) && threadIdx.x == 0) omega_from_dots(sv, state, tot);
+}
+
+// The same omega from per-CTA partial sums (|t|^2, Re / Im of vdot(t, s))
+// that the operator's last pass wrote while it produced t = A s
+// (em3d_matvec_dots): one CTA adds them in a fixed order.
+__global__ void __launch_bounds__(kThreads) k_bicg_omega_parts(int nparts, void* state, const double* parts) {
+  StateView sv = view(state, 0);
+  if (!running(sv.st)) return;
+  double a[3] = {0, 0, 0};
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) a[q] += parts[(size_t)3 * i + q];
   }
+  block_sum<3>(a);
+  if (threadIdx.x == 0) omega_from_dots(sv, state, a);
 }
 
 // u = (u + alpha p) + omega s;  r = s - omega t;  ||r||, vdot(r_hat, r) for the
@@ -685,6 +704,14 @@ EM3D_STEP(em3d_bicgstab_alpha, k_bicg_alpha,
 EM3D_STEP(em3d_bicgstab_s, k_bicg_s,
           (int dtype, size_t n, int batch, void* state, size_t sstride, const void* r, const void* v, void* s, void* stream),
           (n, state, sstride, (const cx<R>*)r, (const cx<R>*)v, (cx<R>*)s))
+int em3d_bicgstab_omega_parts(int nparts, void* state, const double* partials, void* stream) {
+  if (int rc = check_state(state, 1)) return rc;
+  if (nparts < 1 || !partials) { em3d_set_last_error("em3d_bicgstab_omega_parts: no partial sums"); return EM3D_ERR_INVALID; }
+  k_bicg_omega_parts<<<1, kThreads, 0, (cudaStream_t)stream>>>(nparts, state, partials);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
 EM3D_STEP(em3d_bicgstab_omega, k_bicg_omega,
           (int dtype, size_t n, int batch, void* state, size_t sstride, const void* t, const void* s, void* stream),
           (n, state, sstride, (const cx<R>*)t, (const cx<R>*)s))

@@ -149,8 +149,8 @@ int em3d_set_tuning(int key, int value) {
     em3d_set_last_error("x-pass variant must be -1 (automatic) or 0 .. 10");
     return EM3D_ERR_INVALID;
   }
-  if (key == EM3D_TUNE_FNO_SIMT && (value < 0 || value > 2)) {
-    em3d_set_last_error("FNO row-pass switch must be 0, 1 or 2");
+  if (key == EM3D_TUNE_FNO_SIMT && (value < 0 || value > 3)) {
+    em3d_set_last_error("FNO row-pass switch must be 0, 1, 2 or 3");
     return EM3D_ERR_INVALID;
   }
   if (key == EM3D_TUNE_FNO_CONTRACT && value != 0 && value != 2 && value != 4 && value != 8 && value != 12 &&
@@ -287,6 +287,46 @@ int em3d_em_rmatvec_chi(const em3d_grid* g, int dtype, int batch, const void* sp
                         const void* chi, const void* v, void* out, void* ws, size_t wsb, const int* skip,
                         void* stream) {
   return em_apply_layout<true>(g, dtype, batch, spectrum, chi_layout, chi, v, out, ws, wsb, skip, stream);
+}
+
+int em3d_matvec_dot_parts(int kind, const em3d_grid* g, int dtype) {
+  Dims d;
+  if (check_grid(g, &d)) return 0;
+  if (kind != EM3D_EM && kind != EM3D_ACOUSTIC) return 0;
+  const bool f64 = dtype == EM3D_C128;
+  if ((dtype != EM3D_C64 && !f64) || !fast_len(2 * d.nz, f64, false)) return 0;
+  const int nrows = d.nx * d.ny;
+  if (kind == EM3D_EM) return f64 ? rows_fast_ctas<double, 3>(2 * d.nz, nrows) : rows_fast_ctas<float, 3>(2 * d.nz, nrows);
+  return f64 ? rows_fast_ctas<double, 1>(2 * d.nz, nrows) : rows_fast_ctas<float, 1>(2 * d.nz, nrows);
+}
+
+int em3d_matvec_dots(int kind, const em3d_grid* g, int dtype, const void* spectrum, int chi_layout, const void* chi,
+                     const void* u, void* out, void* ws, size_t wsb, const int* skip, double* partials,
+                     void* stream) {
+  Dims d;
+  int rc = check_grid(g, &d);
+  if (rc) return rc;
+  if (!partials) { em3d_set_last_error("partials is NULL"); return EM3D_ERR_INVALID; }
+  BatchStrides bs{};
+  bs.dots = partials;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (kind == EM3D_EM) {
+    if (chi_layout != EM3D_CHI_FULL && chi_layout != EM3D_CHI_SYMMETRIC && chi_layout != EM3D_CHI_ISOTROPIC) {
+      em3d_set_last_error("chi_layout must be EM3D_CHI_FULL (9), EM3D_CHI_SYMMETRIC (6) or EM3D_CHI_ISOTROPIC (1)");
+      return EM3D_ERR_INVALID;
+    }
+    bs.chi_layout = chi_layout;
+    if (dtype == EM3D_C64) return apply<float, 3, false>(d, 1, spectrum, chi, u, out, ws, wsb, skip, st, bs);
+    if (dtype == EM3D_C128) return apply<double, 3, false>(d, 1, spectrum, chi, u, out, ws, wsb, skip, st, bs);
+  } else if (kind == EM3D_ACOUSTIC) {
+    if (dtype == EM3D_C64) return apply<float, 1, false>(d, 1, spectrum, chi, u, out, ws, wsb, skip, st, bs);
+    if (dtype == EM3D_C128) return apply<double, 1, false>(d, 1, spectrum, chi, u, out, ws, wsb, skip, st, bs);
+  } else {
+    em3d_set_last_error("kind must be EM3D_EM or EM3D_ACOUSTIC");
+    return EM3D_ERR_INVALID;
+  }
+  em3d_set_last_error("dtype must be EM3D_C64 or EM3D_C128");
+  return EM3D_ERR_INVALID;
 }
 
 int em3d_em_matvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi, const void* u,

@@ -757,6 +757,19 @@ static int go_strided(const cx<R>* in, cx<R>* out, const cx<R>* tw, int outer, i
   return EM3D_OK;
 }
 
+// CTAs of a register row pass of length L over nrows rows (the partial sums
+// that FST_SUB_DOTS writes); 0 when L has no register plan.
+template <typename R, int C> static int rows_fast_ctas(int L, int nrows) {
+  switch (L) {
+#define EM3D_CASE(LL) \
+  case LL: { constexpr int RPB = RowsGeom<LL, FastE<R, LL>::E, C>::RPB; return (nrows + RPB - 1) / RPB; }
+    EM3D_CASE(32) EM3D_CASE(64) EM3D_CASE(128) EM3D_CASE(256) EM3D_CASE(512) EM3D_CASE(96) EM3D_CASE(160)
+    EM3D_CASE(192)
+#undef EM3D_CASE
+  }
+  return 0;
+}
+
 template <typename R, bool INV>
 static int launch_strided_fast(int L, const cx<R>* in, cx<R>* out, const cx<R>* tw, int outer, int inner,
                                const int* skip, cudaStream_t st, BatchStrides bs) {
@@ -1012,6 +1025,10 @@ int apply(const Dims& d, int batch, const void* spectrum, const void* chi, const
   const int Lz = 2 * d.nz, Ly = 2 * d.ny;
   constexpr bool F64 = sizeof(R) == 8;
   const bool fz = fast_len(Lz, F64, false), fy = fast_len(Ly, F64, false), fx = fast_len(2 * d.nx, F64, true);
+  if (bs.dots && (ADJ || !fz || batch != 1)) {
+    em3d_set_last_error("the fused dot products need a matvec of one right-hand side on a register-FFT z length");
+    return EM3D_ERR_UNSUPPORTED;
+  }
   constexpr int LDF = C == 3 ? LD_EM_CHI : LD_AC_CHI;
   constexpr int FLDF = C == 3 ? FLD_EM_CHI : FLD_AC_CHI;
   constexpr int STA = C == 3 ? ST_EM_ADJ : ST_AC_ADJ;
@@ -1049,7 +1066,15 @@ int apply(const Dims& d, int batch, const void* spectrum, const void* chi, const
   if (rc) return rc;
   // pass 5: rows along z, crop and combine
   if (fz) {
-    if (!ADJ) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_SUB, true>(Lz, T1, nullptr, uu, o, twz, rows, nrows, skip, st, bs);
+    bool fused = false;
+    if constexpr (!ADJ) {
+      if (bs.dots) {
+        rc = launch_rows_fast<R, C, FLD_PLAIN, FST_SUB_DOTS, true>(Lz, T1, nullptr, uu, o, twz, rows, nrows, skip, st, bs);
+        fused = true;
+      }
+    }
+    if (fused) {
+    } else if (!ADJ) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_SUB, true>(Lz, T1, nullptr, uu, o, twz, rows, nrows, skip, st, bs);
     else if constexpr (C == 3) {
       if (chil == 6) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_EM_ADJ6, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st, bs);
       else if (chil == 1) rc = launch_rows_fast<R, C, FLD_PLAIN, FST_EM_ADJ1, true>(Lz, T1, ch, uu, o, twz, rows, nrows, skip, st, bs);

@@ -17,7 +17,8 @@ namespace em3d {
 // components per cell, scalar acoustic chi u.  Store modes: plain, u - y,
 // v - chi^H y for the three EM layouts, v - conj(chi) y (acoustic).
 enum { FLD_PLAIN = 0, FLD_EM_CHI = 1, FLD_AC_CHI = 2, FLD_EM_CHI6 = 3, FLD_EM_CHI1 = 4 };
-enum { FST_PLAIN = 0, FST_SUB = 1, FST_EM_ADJ = 2, FST_AC_ADJ = 3, FST_EM_ADJ6 = 4, FST_EM_ADJ1 = 5 };
+enum { FST_PLAIN = 0, FST_SUB = 1, FST_EM_ADJ = 2, FST_AC_ADJ = 3, FST_EM_ADJ6 = 4, FST_EM_ADJ1 = 5,
+       FST_SUB_DOTS = 6 };  // u - y, and the CTA's partial sums of |t|^2 and vdot(t, u) (t = u - y) into bs.dots
 
 // Elements per thread: power-of-two axes 16 (complex64) or 8 (complex128);
 // mixed axes 12 (3 x 2^k) or 20 (5 x 2^k).
@@ -142,6 +143,43 @@ __device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restri
         out[oo] = csub(base[oo], acc);
       }
     }
+    return;
+  } else if constexpr (ST == FST_SUB_DOTS) {
+    // every thread takes part in the CTA's reduction (no early return); the
+    // exchange buffer, free once the transform is done, holds the partials
+    double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+    if (valid) {
+#pragma unroll
+      for (int q = 0; q < E / RL; ++q) {
+        const int j = t + q * TT;
+#pragma unroll
+        for (int r = 0; r < RL / 2; ++r) {
+          const int pos = j + r * ML;
+          const size_t oo = ob + ((size_t)c * rows_pb + row) * LOUT + pos;
+          const T s = base[oo];
+          const T v = csub(s, a[0][q * RL + r]);
+          out[oo] = v;
+          d0 += (double)v.x * v.x + (double)v.y * v.y;
+          d1 += (double)v.x * s.x + (double)v.y * s.y;
+          d2 += (double)v.x * s.y - (double)v.y * s.x;
+        }
+      }
+    }
+    const int nt = blockDim.x;
+    double* red = reinterpret_cast<double*>(sm);  // 3 x nt doubles
+    __syncthreads();  // every thread is past its last read of the exchange buffer
+    red[threadIdx.x] = d0;
+    red[nt + threadIdx.x] = d1;
+    red[2 * nt + threadIdx.x] = d2;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+      if ((int)threadIdx.x < h && (int)threadIdx.x + h < nt) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) red[k * nt + threadIdx.x] += red[k * nt + threadIdx.x + h];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x < 3) bs.dots[(size_t)blk * 3 + threadIdx.x] = red[threadIdx.x * nt];
     return;
   } else {
     if (!valid) return;

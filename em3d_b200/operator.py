@@ -314,6 +314,26 @@ class _Applier:
                           ws.numel(), skip_ptr, _lib.stream_handle(stream))
         return out
 
+    def dot_parts(self) -> int:
+        """CTAs of the last pass when it also forms BiCGStab's omega inner
+        products (``apply_dots_into``); 0 where that is not available."""
+        n = getattr(self, "_dot_parts", None)
+        if n is None:
+            n = int(_lib.load().em3d_matvec_dot_parts(self._kind, ctypes_ref(self._grid_c), self._dt))
+            self._dot_parts = n
+        return n
+
+    def apply_dots_into(self, x, out, partials, *, skip_ptr=None, stream=None):
+        """``out = A x`` for one right-hand side, the last pass also writing, per
+        CTA, |t|^2 and Re / Im of vdot(t, x) of t = out into ``partials``
+        (float64, 3 x :meth:`dot_parts` values)."""
+        ws = self.workspace(1)
+        with tuned(self.xpass_variant):
+            _lib.call("em3d_matvec_dots", self._kind, ctypes_ref(self._grid_c), self._dt, self._spectrum.data_ptr(),
+                      self._chi_layout, self._chi.data_ptr(), x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(),
+                      skip_ptr, partials.data_ptr(), _lib.stream_handle(stream))
+        return out
+
     # x-pass implementation chosen for this operator by ``em3d_b200.tune.autotune``
     # (None: the library's process-wide setting)
     xpass_variant = None

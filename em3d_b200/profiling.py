@@ -15,6 +15,7 @@ to save iterations); ``uneven`` applies the 48 uneven sphere problems
     python -m em3d_b200.profiling guess-curve --n 128 --seeds 10000,10001,10002,10003
     python -m em3d_b200.profiling delta-sweep --n 128
     python -m em3d_b200.profiling uneven --precision single --count 48
+    python -m em3d_b200.profiling fno --n 64 --row-mode 0
 """
 from __future__ import annotations
 
@@ -69,6 +70,43 @@ def uneven(precision: str, count: int, reps: int, per_size: bool = False) -> flo
         group.apply_into(x, out)
     torch.cuda.synchronize()
     return float(out.abs().sum())
+
+
+def fno(n: int, reps: int, row_mode: int) -> float:
+    """``reps`` forwards of the benchmark's network shape (4 layers, width 32,
+    12 modes, bf16) on an n^3 grid with the FNO row pass ``row_mode``
+    (``EM3D_TUNE_FNO_SIMT``: 0 automatic / tcgen05, 1 CUDA cores, 3 mma.sync);
+    returns ms per forward (CUDA events)."""
+    import numpy as np
+    import torch
+
+    from . import _lib
+    from .fno import FNO
+
+    rng = np.random.default_rng(0)
+    N = (n, n, n)
+    chi = torch.as_tensor(((rng.standard_normal((1, 3, 3) + N) + 1j * rng.standard_normal((1, 3, 3) + N)) * 0.1)
+                          .astype(np.complex64), device="cuda")
+    wave = torch.as_tensor((rng.standard_normal((1, 3) + N) + 1j * rng.standard_normal((1, 3) + N))
+                           .astype(np.complex64), device="cuda")
+    net = FNO(width=32, modes=12, layers=4, act="bf16", seed=0)
+    old = int(_lib.load().em3d_get_tuning(_lib.EM3D_TUNE_FNO_SIMT))
+    try:
+        _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FNO_SIMT, int(row_mode))
+        for _ in range(3):
+            net.forward(chi, wave)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            net.forward(chi, wave)
+        b.record()
+        torch.cuda.synchronize()
+    finally:
+        _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FNO_SIMT, old)
+    failures = _lib.load().em3d_fno_failures(1)
+    if failures:
+        raise _lib.NativeError(f"{failures} bounded wait(s) of the tcgen05 row pass gave up")
+    return a.elapsed_time(b) / reps
 
 
 def step(n: int, seed: int):
@@ -148,6 +186,10 @@ def main(argv=None) -> int:
     u.add_argument("--count", type=int, default=48)
     u.add_argument("--reps", type=int, default=3)
     u.add_argument("--per-size", action="store_true", help="one grouped application per grid size instead")
+    f = sub.add_parser("fno", help="forwards of the warm-start network (ms per forward)")
+    f.add_argument("--n", type=int, default=64)
+    f.add_argument("--reps", type=int, default=20)
+    f.add_argument("--row-mode", type=int, default=0, help="EM3D_TUNE_FNO_SIMT: 0 tcgen05, 1 CUDA cores, 3 mma.sync")
     s = sub.add_parser("step")
     s.add_argument("--n", type=int, default=128)
     s.add_argument("--seed", type=int, default=10001)
@@ -166,6 +208,8 @@ def main(argv=None) -> int:
         v = args.xpass_variant
         v = None if v is None else (v if v == "generic" else int(v))
         print("ok", matvec(args.precision, args.n, args.reps, v))
+    elif args.what == "fno":
+        print("ok", fno(args.n, args.reps, args.row_mode))
     elif args.what == "uneven":
         print("ok", uneven(args.precision, args.count, args.reps, args.per_size))
     elif args.what == "delta-sweep":

@@ -277,6 +277,26 @@ class _Engine:
         _lib.check(status, name)
         _lib.count_launches(name)
 
+    def omega_step(self, s, t, fuse: bool = True):
+        """``t = A s`` and BiCGStab's omega step.  With one right-hand side and
+        an operator that supports it, the inner products |t|^2 and vdot(t, s)
+        come from the operator's last pass (per-CTA partial sums added by one
+        CTA), so t and s are not read again; otherwise the apply and the
+        omega kernel run separately."""
+        parts = self.op.dot_parts() if (fuse and self.batch == 1 and hasattr(self.op, "dot_parts")) else 0
+        if parts <= 0:
+            self.apply(s, t)
+            self.step("em3d_bicgstab_omega", t.data_ptr(), s.data_ptr())
+            return
+        buf = self.vectors.get("_dot_parts")
+        if buf is None:
+            import torch
+
+            buf = torch.zeros(3 * parts, dtype=torch.float64, device=self.rhs.device)
+            self.vectors["_dot_parts"] = buf
+        self.op.apply_dots_into(s, t, buf, skip_ptr=self.state.done_ptr)
+        _lib.call("em3d_bicgstab_omega_parts", parts, self.state.ptr, buf.data_ptr(), self.stream())
+
     def run(self, iteration, chunk: int, use_graph: bool):
         """Launch ``iteration`` until every right-hand side has stopped.  With a
         native operator the iterations are replayed ``chunk`` at a time from a
@@ -459,6 +479,8 @@ class BiCGStab(_KrylovSolver):
     """BiCGStab (reference ``src/em3d/solvers/bicgstab.py``), device resident."""
 
     graph_chunk = 4
+    # one right-hand side: omega's inner products formed in the operator's last pass
+    fuse_dots = True
 
     def __init__(self, config: SolverConfig):
         self.cfg = config
@@ -512,8 +534,7 @@ class BiCGStab(_KrylovSolver):
             eng.apply(p, v)
             eng.step("em3d_bicgstab_alpha", r_hat.data_ptr(), v.data_ptr())
             eng.step("em3d_bicgstab_s", r.data_ptr(), v.data_ptr(), s.data_ptr())
-            eng.apply(s, t)
-            eng.step("em3d_bicgstab_omega", t.data_ptr(), s.data_ptr())
+            eng.omega_step(s, t, self.fuse_dots)
             eng.step("em3d_bicgstab_update", u.data_ptr(), p.data_ptr(), s.data_ptr(), t.data_ptr(), r.data_ptr(),
                      r_hat.data_ptr())
             eng.step("em3d_bicgstab_finalize", u.data_ptr(), p.data_ptr())
@@ -845,6 +866,8 @@ class MixedBiCGStab:
 
     graph_chunk = 4
     max_cached = 2
+    # one right-hand side: omega's inner products formed in the operator's last pass
+    fuse_dots = True
 
     def __init__(self, config: SolverConfig, *, delta: float = 1e-3, safety: float = 0.5,
                  guess_fallback: bool = True, max_cycles: int = 200):
@@ -998,8 +1021,7 @@ class MixedBiCGStab:
             e32.apply(p, v)
             e32.step("em3d_bicgstab_alpha", rh.data_ptr(), v.data_ptr())
             e32.step("em3d_bicgstab_s", r32.data_ptr(), v.data_ptr(), s.data_ptr())
-            e32.apply(s, tt)
-            e32.step("em3d_bicgstab_omega", tt.data_ptr(), s.data_ptr())
+            e32.omega_step(s, tt, self.fuse_dots)
             e32.step("em3d_bicgstab_update", u32.data_ptr(), p.data_ptr(), s.data_ptr(), tt.data_ptr(), r32.data_ptr(),
                      rh.data_ptr())
             e32.step("em3d_bicgstab_finalize", u32.data_ptr(), p.data_ptr())

@@ -71,8 +71,9 @@ enum em3d_tune_key {
                                    shared memory does not fit is replaced by the first that fits in the
                                    order 6, 4, 1, 2, 0, 5, 3 */
   EM3D_TUNE_FFT_GENERIC = 1,   /* 1 = use the generic shared-memory FFT passes for every axis length */
-  EM3D_TUNE_FNO_SIMT = 2,      /* FNO row pass: 0 = warp-level tensor cores (mma.sync) where they apply, 1 = CUDA cores,
-                                   2 = fifth-generation tensor cores (tcgen05, TMEM accumulators) for the layer passes */
+  EM3D_TUNE_FNO_SIMT = 2,      /* FNO row pass (bf16, width 32, Z a multiple of 32): 0 = automatic (the layer passes on
+                                   tcgen05 with TMEM accumulators, the lift on mma.sync), 1 = CUDA cores everywhere,
+                                   2 = the same as 0, 3 = mma.sync for the layer passes too */
   EM3D_TUNE_FNO_CONTRACT = 3,  /* FNO truncated-DFT contractions: 0 automatic, else outputs per thread (2, 4, 8, 12, 24) */
   EM3D_TUNE_COUNT = 4,
 };
@@ -251,6 +252,20 @@ int em3d_acoustic_matvec_uneven(int dtype, int nseg, const em3d_segment* segs, v
 int em3d_acoustic_rmatvec_uneven(int dtype, int nseg, const em3d_segment* segs, void* workspace,
                                  size_t workspace_bytes, const int* skip, void* stream);
 
+/* A matvec of one right-hand side (EM with chi stored in chi_layout, or
+ * acoustic) whose last pass also writes, per CTA, the partial sums of
+ * |t|^2 and Re / Im of vdot(t, u) of its output t = u - A' u, three doubles
+ * per CTA at partials[3 * cta]: the inner products BiCGStab forms right after
+ * t = A s (src/em3d/solvers/bicgstab.py:153-163), without reading t and s
+ * again.  em3d_matvec_dot_parts gives the number of CTAs (partials holds 3x
+ * that many doubles); 0 when the z axis has no register FFT (then this call
+ * returns EM3D_ERR_UNSUPPORTED).  em3d_bicgstab_omega_parts finishes omega
+ * from the partials. */
+int em3d_matvec_dot_parts(int kind, const em3d_grid* g, int dtype);
+int em3d_matvec_dots(int kind, const em3d_grid* g, int dtype, const void* spectrum, int chi_layout, const void* chi,
+                     const void* u, void* out, void* ws, size_t ws_bytes, const int* skip, double* partials,
+                     void* stream);
+
 /* Scalar versions.  Replace AcousticOperator.matvec / rmatvec
  * (src/em3d/acoustics/operator.py:40-67). */
 int em3d_acoustic_matvec(const em3d_grid* g, int dtype, int batch, const void* spectrum, const void* chi,
@@ -349,6 +364,9 @@ int em3d_bicgstab_p(int dtype, size_t n, int batch, void* state, size_t state_st
 int em3d_bicgstab_alpha(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* r_hat, const void* v, void* stream);
 int em3d_bicgstab_s(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* r, const void* v, void* s, void* stream);
 int em3d_bicgstab_omega(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* t, const void* s, void* stream);
+/* The same omega step for one right-hand side from the nparts per-CTA partial
+ * sums (3 doubles each) that em3d_matvec_dots wrote while forming t = A s. */
+int em3d_bicgstab_omega_parts(int nparts, void* state, const double* partials, void* stream);
 int em3d_bicgstab_update(int dtype, size_t n, int batch, void* state, size_t state_stride, void* u, const void* p, const void* s, const void* t,
                          void* r, const void* r_hat, void* stream);
 int em3d_bicgstab_finalize(int dtype, size_t n, int batch, void* state, size_t state_stride, void* u, const void* p, void* stream);

@@ -171,7 +171,7 @@ def test_tcgen05_row_pass_matches_mma_sync_pass(N, m):
     _lib.load().em3d_fno_failures(1)
     out = {}
     try:
-        for mode in (0, 2):
+        for mode in (3, 2):
             _lib.call("em3d_set_tuning", _lib.EM3D_TUNE_FNO_SIMT, mode)
             for train in (False, True):
                 u = net.forward(chi, wave, train).clone()
@@ -184,10 +184,10 @@ def test_tcgen05_row_pass_matches_mma_sync_pass(N, m):
     torch.cuda.synchronize()
     assert _lib.load().em3d_fno_failures(1) == 0
     for train in (False, True):
-        a, b = out[(2, train)][0] - wave, out[(0, train)][0] - wave   # the network's output proper
-        assert float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) < 1e-2
-        for x, y in zip(out[(2, train)][1] + out[(2, train)][2], out[(0, train)][1] + out[(0, train)][2]):
-            assert float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)) < 1e-2
+        a, b = out[(2, train)][0] - wave, out[(3, train)][0] - wave   # the network's output proper
+        assert float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) < 2e-3
+        for x, y in zip(out[(2, train)][1] + out[(2, train)][2], out[(3, train)][1] + out[(3, train)][2]):
+            assert float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)) < 2e-3
 
 
 @pytest.mark.parametrize("src", ["complex64", "complex128"])

@@ -236,3 +236,37 @@ def test_defect_correction_rejects_a_bad_guess():
     assert rel_err(be.to_host(bad.u), be.to_host(cold.u)) < 1e-7
     good = dc.solve(op, prob.wave, x0=cold.u * (1 + 1e-5))
     assert not good.guess_rejected and good.residual_history[0] < 1e-3
+
+
+@pytest.mark.parametrize("N", [(32, 32, 32), (24, 20, 40)])
+def test_fused_omega_dots_match_separate_kernels(N):
+    """BiCGStab and MixedBiCGStab with omega's inner products formed in the
+    operator's last pass (one right-hand side) follow the same iterations as
+    with the separate omega kernel; a z axis without a register FFT (2 Nz =
+    80) falls back to the separate kernel."""
+    import em3d_b200 as e
+    from em3d_b200 import scenes
+    from em3d_b200.solvers import BiCGStab, MixedBiCGStab, SolverConfig
+
+    be = e.Backend.b200(e.Precision.DOUBLE)
+    grid = e.Grid(N=N, L=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0), backend=be)
+    shape = scenes.EllipsoidShape((0.0, 0.05, 0.0), (0.3, 0.2, 0.25), None, 2.5 + 0.1j)
+    wave = scenes.plane_wave(grid, k=6.0, orient=(0.0, 0.0, 1.0), amplitude=(1.0, 0.0, 0.0))
+    p = e.Problem(grid=grid, eps_tensor=scenes.sample_scene(grid, [shape]), wave=wave, k0=6.0, volume=1.0)
+    op = e.Operator(p)
+    lo = op.with_precision(e.Precision.SINGLE)
+    assert (op.dot_parts() > 0) == (N[2] != 40)
+    cfg = SolverConfig(max_iter=300, rtol=1e-9)
+    runs = {}
+    for fuse in (True, False):
+        b = BiCGStab(cfg)
+        b.fuse_dots = fuse
+        m = MixedBiCGStab(cfg)
+        m.fuse_dots = fuse
+        runs[fuse] = (b.solve(op, p.wave), m.solve(op, p.wave, operator_low=lo))
+    for k in range(2):
+        a, c = runs[True][k], runs[False][k]
+        assert a.status == c.status == "converged"
+        assert a.iterations == c.iterations and a.matvec_count == c.matvec_count
+        np.testing.assert_allclose(a.residual_history, c.residual_history, rtol=1e-6)
+        assert rel_err(a.u.cpu().numpy(), c.u.cpu().numpy()) < 1e-8

@@ -102,3 +102,24 @@ def test_invalid_arguments_are_reported_not_launched():
         L.call("em3d_acoustic_matvec_uneven", L.EM3D_C64, 1, one, 64, big, None, None)
     with pytest.raises(ValueError, match="dtype"):
         L.call("em3d_em_rmatvec_uneven", 5, 2, segs, 64, big, None, None)
+
+
+def test_fused_dot_parts_counts():
+    """CTAs of the last pass that em3d_matvec_dots writes partial sums for:
+    ceil(Nx Ny / rows per CTA) on register-FFT z lengths, 0 elsewhere."""
+    L, lib = _lib()
+
+    def parts(N, kind, dtype):
+        g = L.make_grid(N, (1.0, 1.0, 1.0))
+        return lib.em3d_matvec_dot_parts(kind, ctypes.byref(g), dtype)
+
+    # complex64 EM, 2 Nz = 256: 16 threads per row, 5 rows of 3 components per CTA
+    assert parts((128, 128, 128), L.EM3D_EM, L.EM3D_C64) == -(-128 * 128 // 5)
+    # acoustic: 16 rows per CTA
+    assert parts((128, 128, 128), L.EM3D_ACOUSTIC, L.EM3D_C64) == 128 * 128 // 16
+    assert parts((16, 16, 40), L.EM3D_EM, L.EM3D_C64) == 0          # 80 points: generic passes
+    assert parts((16, 16, 16), 2, L.EM3D_C64) == 0
+    g = L.make_grid((16, 16, 16), (1.0, 1.0, 1.0))
+    with pytest.raises(ValueError, match="partials"):
+        L.call("em3d_matvec_dots", L.EM3D_EM, ctypes.byref(g), L.EM3D_C64, 16, 9, 16, 32, 48, 64, 1 << 30, None,
+               None, None)
