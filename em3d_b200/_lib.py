@@ -102,8 +102,11 @@ SIGNATURES = {
     "em3d_fno_failures": (c_int, [c_int]),
     "em3d_matvec_dot_parts": (c_int, [c_int, _GRID, c_int]),
     "em3d_matvec_dots": (c_int, [c_int, _GRID, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
-                                 c_size_t, c_void_p, c_void_p, c_void_p]),
+                                 c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
     "em3d_bicgstab_omega_parts": (c_int, [c_int, c_void_p, c_void_p, c_void_p]),
+    "em3d_bicgstab_alpha_parts": (c_int, [c_int, c_void_p, c_void_p, c_void_p]),
+    "em3d_copy_small_max_bytes": (c_size_t, []),
+    "em3d_copy_small": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
     "em3d_fno_spectral": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                   c_void_p]),
     "em3d_em_farfield": (c_int, [_GRID, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_double,

@@ -72,8 +72,10 @@ struct BatchStrides {
   // 0: back to back (C cells each)
   size_t field = 0;
   // nullable: the last pass of a matvec also writes, per CTA, the partial
-  // sums |t|^2, Re and Im of vdot(t, u) of its output t = u - y (one entry)
+  // sums |t|^2, Re and Im of vdot(t, w) of its output t = u - y (one entry),
+  // w = dot_with (same element type and layout as t) or, when that is null, u
   double* dots = nullptr;
+  const void* dot_with = nullptr;
 };
 
 // Index of entry (r, c) of a symmetric 3x3 contrast stored as its six

@@ -211,7 +211,7 @@ __global__ void k_convert(size_t n, const S* src, D* dst, int accumulate) {
 }
 
 // ---------------------------------------------------------------------------
-// BiCGStab (src/em3d/solvers/bicgstab.py:139-251)
+// BiCGStab (src/em3d/solvers/bicgstab.py:84-197)
 // ---------------------------------------------------------------------------
 
 // rho / omega checks, beta, p = r + beta (p - omega v) (p = r on the first
@@ -246,6 +246,17 @@ __global__ void __launch_bounds__(kThreads) k_bicg_p(size_t n, void* state, size
   }
 }
 
+// alpha = rho / den with den = vdot(r_hat, v), and the breakdown check
+// (src/em3d/solvers/bicgstab.py:106-112); one thread.
+__device__ inline void alpha_from_dot(StateView& sv, void* state, double2 den) {
+  em3d_krylov_state* st = sv.st;
+  st->matvecs += 1;
+  if (cabs2(den) == 0.0) { stop_rhs(st, state, EM3D_BREAKDOWN_ALPHA); return; }
+  const double2 al = cdiv(make_double2(st->rho_re, st->rho_im), den);
+  st->alpha_re = al.x;
+  st->alpha_im = al.y;
+}
+
 // den = vdot(r_hat, v); alpha = rho / den.
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, size_t sstride, const cx<R>* rh, const cx<R>* v) {
@@ -266,15 +277,22 @@ __global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, 
   }
   for (; i < n; i += gs) acc_dot(a[0], a[1], rh[i], v[i]);
   double tot[2];
-  if (reduce_last<2>(sv, a, tot) && threadIdx.x == 0) {
-    em3d_krylov_state* st = sv.st;
-    st->matvecs += 1;
-    const double2 den = make_double2(tot[0], tot[1]);
-    if (cabs2(den) == 0.0) { stop_rhs(st, state, EM3D_BREAKDOWN_ALPHA); return; }
-    const double2 al = cdiv(make_double2(st->rho_re, st->rho_im), den);
-    st->alpha_re = al.x;
-    st->alpha_im = al.y;
+  if (reduce_last<2>(sv, a, tot) && threadIdx.x == 0) alpha_from_dot(sv, state, make_double2(tot[0], tot[1]));
+}
+
+// The same alpha from per-CTA partial sums (|v|^2, Re / Im of vdot(v, r_hat))
+// that the operator's last pass wrote while it produced v = A p
+// (em3d_matvec_dots with r_hat as the second vector): den = conj of their sum.
+__global__ void __launch_bounds__(kThreads) k_bicg_alpha_parts(int nparts, void* state, const double* parts) {
+  StateView sv = view(state, 0);
+  if (!running(sv.st)) return;
+  double a[2] = {0, 0};
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    a[0] += parts[(size_t)3 * i + 1];
+    a[1] += parts[(size_t)3 * i + 2];
   }
+  block_sum<2>(a);
+  if (threadIdx.x == 0) alpha_from_dot(sv, state, make_double2(a[0], -a[1]));
 }
 
 // s = r - alpha v, ||s||; stopping checks on ||s|| (the update u += alpha p
@@ -314,7 +332,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_s(size_t n, void* state, size
 }
 
 // omega = ts / tt from tot = (tt, Re ts, Im ts), with the breakdown checks
-// (src/em3d/solvers/bicgstab.py:153-170); one thread.
+// (src/em3d/solvers/bicgstab.py:151-168); one thread.
 __device__ inline void omega_from_dots(StateView& sv, void* state, const double (&tot)[3]) {
   em3d_krylov_state* st = sv.st;
   st->matvecs += 1;
@@ -708,6 +726,14 @@ int em3d_bicgstab_omega_parts(int nparts, void* state, const double* partials, v
   if (int rc = check_state(state, 1)) return rc;
   if (nparts < 1 || !partials) { em3d_set_last_error("em3d_bicgstab_omega_parts: no partial sums"); return EM3D_ERR_INVALID; }
   k_bicg_omega_parts<<<1, kThreads, 0, (cudaStream_t)stream>>>(nparts, state, partials);
+  EM3D_LAUNCH_CHECK();
+  return EM3D_OK;
+}
+
+int em3d_bicgstab_alpha_parts(int nparts, void* state, const double* partials, void* stream) {
+  if (int rc = check_state(state, 1)) return rc;
+  if (nparts < 1 || !partials) { em3d_set_last_error("em3d_bicgstab_alpha_parts: no partial sums"); return EM3D_ERR_INVALID; }
+  k_bicg_alpha_parts<<<1, kThreads, 0, (cudaStream_t)stream>>>(nparts, state, partials);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }

@@ -302,13 +302,14 @@ int em3d_matvec_dot_parts(int kind, const em3d_grid* g, int dtype) {
 
 int em3d_matvec_dots(int kind, const em3d_grid* g, int dtype, const void* spectrum, int chi_layout, const void* chi,
                      const void* u, void* out, void* ws, size_t wsb, const int* skip, double* partials,
-                     void* stream) {
+                     const void* dot_with, void* stream) {
   Dims d;
   int rc = check_grid(g, &d);
   if (rc) return rc;
   if (!partials) { em3d_set_last_error("partials is NULL"); return EM3D_ERR_INVALID; }
   BatchStrides bs{};
   bs.dots = partials;
+  bs.dot_with = dot_with;
   cudaStream_t st = (cudaStream_t)stream;
   if (kind == EM3D_EM) {
     if (chi_layout != EM3D_CHI_FULL && chi_layout != EM3D_CHI_SYMMETRIC && chi_layout != EM3D_CHI_ISOTROPIC) {

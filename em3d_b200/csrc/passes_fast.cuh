@@ -18,7 +18,7 @@ namespace em3d {
 // v - chi^H y for the three EM layouts, v - conj(chi) y (acoustic).
 enum { FLD_PLAIN = 0, FLD_EM_CHI = 1, FLD_AC_CHI = 2, FLD_EM_CHI6 = 3, FLD_EM_CHI1 = 4 };
 enum { FST_PLAIN = 0, FST_SUB = 1, FST_EM_ADJ = 2, FST_AC_ADJ = 3, FST_EM_ADJ6 = 4, FST_EM_ADJ1 = 5,
-       FST_SUB_DOTS = 6 };  // u - y, and the CTA's partial sums of |t|^2 and vdot(t, u) (t = u - y) into bs.dots
+       FST_SUB_DOTS = 6 };  // u - y, and the CTA's partial sums of |t|^2 and vdot(t, w) (t = u - y; w = bs.dot_with, else u) into bs.dots
 
 // Elements per thread: power-of-two axes 16 (complex64) or 8 (complex128);
 // mixed axes 12 (3 x 2^k) or 20 (5 x 2^k).
@@ -148,6 +148,7 @@ __device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restri
     // every thread takes part in the CTA's reduction (no early return); the
     // exchange buffer, free once the transform is done, holds the partials
     double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+    const T* wv = static_cast<const T*>(bs.dot_with);
     if (valid) {
 #pragma unroll
       for (int q = 0; q < E / RL; ++q) {
@@ -159,9 +160,10 @@ __device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restri
           const T s = base[oo];
           const T v = csub(s, a[0][q * RL + r]);
           out[oo] = v;
+          const T w = wv ? wv[oo] : s;
           d0 += (double)v.x * v.x + (double)v.y * v.y;
-          d1 += (double)v.x * s.x + (double)v.y * s.y;
-          d2 += (double)v.x * s.y - (double)v.y * s.x;
+          d1 += (double)v.x * w.x + (double)v.y * w.y;
+          d2 += (double)v.x * w.y - (double)v.y * w.x;
         }
       }
     }

@@ -343,4 +343,6 @@ def predict_x0(net: FNO, problem, dtype=None):
     chi = problem.eps_tensor.to(torch.complex64)[None]
     wave = problem.wave.to(torch.complex64)[None]
     u = net.forward(chi, wave, train=False)[0]
-    return u.to(dtype or problem.wave.dtype).clone()
+    out = u.to(dtype or problem.wave.dtype)
+    # a tensor of its own: the network's output buffer is reused by its next forward
+    return out.clone() if out.data_ptr() == u.data_ptr() else out

@@ -323,15 +323,17 @@ class _Applier:
             self._dot_parts = n
         return n
 
-    def apply_dots_into(self, x, out, partials, *, skip_ptr=None, stream=None):
+    def apply_dots_into(self, x, out, partials, *, dot_with=None, skip_ptr=None, stream=None):
         """``out = A x`` for one right-hand side, the last pass also writing, per
-        CTA, |t|^2 and Re / Im of vdot(t, x) of t = out into ``partials``
-        (float64, 3 x :meth:`dot_parts` values)."""
+        CTA, |t|^2 and Re / Im of vdot(t, w) of t = out into ``partials``
+        (float64, 3 x :meth:`dot_parts` values); w = ``dot_with`` (a vector
+        shaped like ``x``), or ``x`` itself."""
         ws = self.workspace(1)
+        w = None if dot_with is None else dot_with.data_ptr()
         with tuned(self.xpass_variant):
             _lib.call("em3d_matvec_dots", self._kind, ctypes_ref(self._grid_c), self._dt, self._spectrum.data_ptr(),
                       self._chi_layout, self._chi.data_ptr(), x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(),
-                      skip_ptr, partials.data_ptr(), _lib.stream_handle(stream))
+                      skip_ptr, partials.data_ptr(), w, _lib.stream_handle(stream))
         return out
 
     # x-pass implementation chosen for this operator by ``em3d_b200.tune.autotune``

@@ -117,6 +117,32 @@ class DeviceState:
         for h in self.hosts:
             h.hist_cap = self.cap
         self._done_view = self.buf[self.DONE_OFFSET:self.DONE_OFFSET + 4].view(torch.int32)
+        # pinned mirrors of the buffer: read-backs and uploads go through them
+        # by em3d_copy_small (a kernel on the solving stream), so they never wait
+        # behind a large copy-engine transfer issued on another stream
+        nbytes = self.stride * self.batch
+        self._small = nbytes <= int(lib.em3d_copy_small_max_bytes())
+        self._hbuf = self._hstage = None
+        self._staged = None  # event after the last upload from the staging buffer
+        if self._small:
+            self._hbuf = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+            self._hstage = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+            self._hview = self._hbuf.numpy()
+            self._sview = self._hstage.numpy()
+
+    def _read(self, off: int, nbytes: int) -> np.ndarray:
+        """Bytes [off, off + nbytes) of the device buffer once the current
+        stream has reached this point (a view into the pinned mirror, valid
+        until the next read)."""
+        import torch
+
+        if not self._small:
+            return self.buf.cpu().numpy()
+        stream = torch.cuda.current_stream(self.buf.device)
+        _lib.call("em3d_copy_small", self._hbuf.data_ptr() + off, self.buf.data_ptr() + off, nbytes,
+                  stream.cuda_stream)
+        stream.synchronize()
+        return self._hview
 
     @property
     def host(self) -> KrylovState:
@@ -153,14 +179,26 @@ class DeviceState:
                 blk[self.hist_off:self.hist_off + len(hv)] = hv
                 blk[self.counts_off:self.counts_off + len(cv)] = cv
             raw += blk
-        self.buf.copy_(torch.frombuffer(raw, dtype=torch.uint8))
+        if not self._small:
+            self.buf.copy_(torch.frombuffer(raw, dtype=torch.uint8))
+            return
+        if self._staged is not None:
+            self._staged.synchronize()  # the previous upload has left the staging buffer
+        self._sview[:len(raw)] = np.frombuffer(bytes(raw), dtype=np.uint8)
+        stream = torch.cuda.current_stream(self.buf.device)
+        _lib.call("em3d_copy_small", self.buf.data_ptr(), self._hstage.data_ptr(), len(raw), stream.cuda_stream)
+        self._staged = torch.cuda.Event()
+        self._staged.record(stream)
 
     def done(self) -> bool:
-        return int(self._done_view.item()) != 0
+        if not self._small:
+            return int(self._done_view.item()) != 0
+        host = self._read(self.DONE_OFFSET, 4)
+        return int(host[self.DONE_OFFSET:self.DONE_OFFSET + 4].view(np.int32)[0]) != 0
 
     def download(self):
         """[(state, history, counts)] for every right-hand side."""
-        host = self.buf.cpu().numpy()
+        host = self._read(0, self.stride * self.batch)
         out = []
         sz = ctypes.sizeof(KrylovState)
         for b in range(self.batch):
@@ -174,7 +212,7 @@ class DeviceState:
 
     def dots(self):
         """[(dot0, dot1)] per right-hand side from the last em3d_vec_dots."""
-        host = self.buf.cpu().numpy()
+        host = self._read(0, self.stride * self.batch)
         sz = ctypes.sizeof(KrylovState)
         res = []
         for b in range(self.batch):
@@ -188,6 +226,32 @@ def _check_status(operator) -> None:
     of this package; other operators have no status words)."""
     if hasattr(operator, "check_status"):
         operator.check_status()
+
+
+def _dcopy(dst, src):
+    """``dst = src``.  Between contiguous CUDA complex tensors of one dtype and
+    size this is the library's vector kernel on the current stream: a
+    device-to-device memcpy would run on a copy engine, queued behind any
+    large host transfer that another stream has issued there.  Otherwise
+    torch's copy."""
+    import torch
+
+    if (dst.is_cuda and src.is_cuda and dst.device == src.device and dst.dtype == src.dtype
+            and dst.dtype in (torch.complex64, torch.complex128) and dst.numel() == src.numel()
+            and dst.is_contiguous() and src.is_contiguous()):
+        if dst.numel():
+            dt = _native_dtype(dst)
+            _lib.call("em3d_vec_convert", dst.numel(), dt, src.data_ptr(), dt, dst.data_ptr(), 0,
+                      _lib.stream_handle())
+        return dst
+    return dst.copy_(src)
+
+
+def _dclone(x):
+    """A copy of ``x`` (see :func:`_dcopy`)."""
+    import torch
+
+    return _dcopy(torch.empty_like(x, memory_format=torch.contiguous_format), x)
 
 
 def _native_dtype(t) -> int:
@@ -213,7 +277,7 @@ class _Engine:
             rhs = torch.as_tensor(np.asarray(rhs))
         tc = self.be.precision.torch_complex if hasattr(self.be, "precision") else rhs.dtype
         self.rhs = torch.empty(rhs.shape, dtype=tc, device=self.be.torch_device)
-        self.rhs.copy_(rhs)
+        _dcopy(self.rhs, rhs)
         self.batch = int(batch)
         self.n = int(self.rhs.numel()) // self.batch
         self.dt = _native_dtype(self.rhs)
@@ -234,7 +298,7 @@ class _Engine:
 
     def load_rhs(self, rhs):
         """Reuse this engine (its buffers and captured graph) for a new right-hand side."""
-        self.rhs.copy_(rhs.reshape(self.rhs.shape))
+        _dcopy(self.rhs, rhs.reshape(self.rhs.shape))
 
     def vec(self):
         import torch
@@ -277,23 +341,45 @@ class _Engine:
         _lib.check(status, name)
         _lib.count_launches(name)
 
-    def omega_step(self, s, t, fuse: bool = True):
-        """``t = A s`` and BiCGStab's omega step.  With one right-hand side and
-        an operator that supports it, the inner products |t|^2 and vdot(t, s)
-        come from the operator's last pass (per-CTA partial sums added by one
-        CTA), so t and s are not read again; otherwise the apply and the
-        omega kernel run separately."""
+    def _dot_parts(self, fuse: bool):
+        """(CTAs, partials buffer) of the fused inner products, or (0, None)
+        when they are not available (several right-hand sides, an operator
+        without them, or a z axis without a register FFT)."""
         parts = self.op.dot_parts() if (fuse and self.batch == 1 and hasattr(self.op, "dot_parts")) else 0
         if parts <= 0:
-            self.apply(s, t)
-            self.step("em3d_bicgstab_omega", t.data_ptr(), s.data_ptr())
-            return
+            return 0, None
         buf = self.vectors.get("_dot_parts")
         if buf is None:
             import torch
 
             buf = torch.zeros(3 * parts, dtype=torch.float64, device=self.rhs.device)
             self.vectors["_dot_parts"] = buf
+        return parts, buf
+
+    def alpha_step(self, p, v, r_hat, fuse: bool = True):
+        """``v = A p`` and BiCGStab's alpha step.  With one right-hand side and
+        an operator that supports it, vdot(r_hat, v) comes from the operator's
+        last pass (per-CTA partial sums added by one CTA), so v is not read
+        again; otherwise the apply and the alpha kernel run separately."""
+        parts, buf = self._dot_parts(fuse)
+        if parts <= 0:
+            self.apply(p, v)
+            self.step("em3d_bicgstab_alpha", r_hat.data_ptr(), v.data_ptr())
+            return
+        self.op.apply_dots_into(p, v, buf, dot_with=r_hat, skip_ptr=self.state.done_ptr)
+        _lib.call("em3d_bicgstab_alpha_parts", parts, self.state.ptr, buf.data_ptr(), self.stream())
+
+    def omega_step(self, s, t, fuse: bool = True):
+        """``t = A s`` and BiCGStab's omega step.  With one right-hand side and
+        an operator that supports it, the inner products |t|^2 and vdot(t, s)
+        come from the operator's last pass (per-CTA partial sums added by one
+        CTA), so t and s are not read again; otherwise the apply and the
+        omega kernel run separately."""
+        parts, buf = self._dot_parts(fuse)
+        if parts <= 0:
+            self.apply(s, t)
+            self.step("em3d_bicgstab_omega", t.data_ptr(), s.data_ptr())
+            return
         self.op.apply_dots_into(s, t, buf, skip_ptr=self.state.done_ptr)
         _lib.call("em3d_bicgstab_omega_parts", parts, self.state.ptr, buf.data_ptr(), self.stream())
 
@@ -342,7 +428,8 @@ class _Engine:
         if src is not None:
             if getattr(self, "_status_host", None) is None:
                 self._status_host = torch.zeros(1, dtype=torch.int32).pin_memory()
-            self._status_host.copy_(src, non_blocking=True)
+            # by a kernel on this stream (em3d_copy_small), not a copy engine
+            _lib.call("em3d_copy_small", self._status_host.data_ptr(), src.data_ptr(), 4, self.stream())
         done = self.state.done()
         if src is not None and int(self._status_host[0]) != 0:
             self.op.check_status()
@@ -387,7 +474,7 @@ def _load_u(buf, x0):
         buf.zero_()
     else:
         x = x0 if isinstance(x0, torch.Tensor) else torch.as_tensor(np.asarray(x0))
-        buf.copy_(x.to(device=buf.device, dtype=buf.dtype).reshape(buf.shape))
+        _dcopy(buf, x.to(device=buf.device, dtype=buf.dtype).reshape(buf.shape))
     return buf
 
 
@@ -465,7 +552,7 @@ class _KrylovSolver:
 
     def _results(self, eng, u, trivial):
         out = []
-        u = u.clone()  # the engine's buffer is reused by the next solve
+        u = _dclone(u)  # the engine's buffer is reused by the next solve
         for b, (st, hist, counts) in enumerate(eng.state.download()):
             ub = _entry(eng.op, u, b, eng.batch)
             if trivial[b]:
@@ -479,7 +566,7 @@ class BiCGStab(_KrylovSolver):
     """BiCGStab (reference ``src/em3d/solvers/bicgstab.py``), device resident."""
 
     graph_chunk = 4
-    # one right-hand side: omega's inner products formed in the operator's last pass
+    # one right-hand side: alpha's and omega's inner products formed in the operator's last pass
     fuse_dots = True
 
     def __init__(self, config: SolverConfig):
@@ -526,13 +613,12 @@ class BiCGStab(_KrylovSolver):
             counts.append([1])
         eng.state.upload(hists, counts)
         r_hat = self._vec(eng, "r_hat")
-        r_hat.copy_(r)
+        _dcopy(r_hat, r)
         p, v, s, t = (self._vec(eng, k) for k in ("p", "v", "s", "t"))
 
         def iteration():
             eng.step("em3d_bicgstab_p", r.data_ptr(), p.data_ptr(), v.data_ptr())
-            eng.apply(p, v)
-            eng.step("em3d_bicgstab_alpha", r_hat.data_ptr(), v.data_ptr())
+            eng.alpha_step(p, v, r_hat, self.fuse_dots)
             eng.step("em3d_bicgstab_s", r.data_ptr(), v.data_ptr(), s.data_ptr())
             eng.omega_step(s, t, self.fuse_dots)
             eng.step("em3d_bicgstab_update", u.data_ptr(), p.data_ptr(), s.data_ptr(), t.data_ptr(), r.data_ptr(),
@@ -770,7 +856,7 @@ class DefectCorrection:
         for outer in range(self.max_outer + 1):
             if outer == 0 and x0 is None:
                 # zero guess: the residual is f itself (A 0 = 0), no FP64 application
-                r.copy_(f)
+                _dcopy(r, f)
                 rel = np.where(fn == 0.0, 0.0, 1.0)
             else:
                 operator.apply_into(u, r)
@@ -783,7 +869,7 @@ class DefectCorrection:
                 for b in range(batch):
                     if status[b] is None and not rel[b] < 1.0:
                         (u if batch == 1 else u[b]).zero_()
-                        (r if batch == 1 else r[b]).copy_(f if batch == 1 else f[b])
+                        _dcopy(r if batch == 1 else r[b], f if batch == 1 else f[b])
                         rel[b] = 1.0
                         rejected[b] = True
             for b in range(batch):
@@ -824,7 +910,7 @@ class DefectCorrection:
             _lib.call("em3d_vec_convert", eng.n * batch, _lib.EM3D_C64, d.data_ptr(), eng.dt, u.data_ptr(), 1,
                       eng.stream())
         out = []
-        u = u.clone()  # the cached buffer is reused by the next solve
+        u = _dclone(u)  # the cached buffer is reused by the next solve
         for b in range(batch):
             ub = _entry(operator, u, b, batch)
             h = hist[b] if hist[b] else [0.0]
@@ -866,7 +952,7 @@ class MixedBiCGStab:
 
     graph_chunk = 4
     max_cached = 2
-    # one right-hand side: omega's inner products formed in the operator's last pass
+    # one right-hand side: alpha's and omega's inner products formed in the operator's last pass
     fuse_dots = True
 
     def __init__(self, config: SolverConfig, *, delta: float = 1e-3, safety: float = 0.5,
@@ -979,7 +1065,7 @@ class MixedBiCGStab:
         if active:
             if x0 is None:
                 # zero guess: the residual is f itself (A 0 = 0), no FP64 application
-                r.copy_(f)
+                _dcopy(r, f)
                 rel = np.ones(batch)
             else:
                 # a guess only starts the iteration: its residual is formed with
@@ -1000,7 +1086,7 @@ class MixedBiCGStab:
             for b in active:
                 if x0 is not None and self.guess_fallback and not rel[b] < 1.0:
                     row(x, b).zero_()
-                    row(r, b).copy_(row(f, b))
+                    _dcopy(row(r, b), row(f, b))
                     if r32_ready:
                         _lib.call("em3d_vec_convert", eng.n, eng.dt, row(f, b).data_ptr(), _lib.EM3D_C64,
                                   row(r32, b).data_ptr(), 0, stream)
@@ -1018,8 +1104,7 @@ class MixedBiCGStab:
 
         def iteration():
             e32.step("em3d_bicgstab_p", r32.data_ptr(), p.data_ptr(), v.data_ptr())
-            e32.apply(p, v)
-            e32.step("em3d_bicgstab_alpha", rh.data_ptr(), v.data_ptr())
+            e32.alpha_step(p, v, rh, self.fuse_dots)
             e32.step("em3d_bicgstab_s", r32.data_ptr(), v.data_ptr(), s.data_ptr())
             e32.omega_step(s, tt, self.fuse_dots)
             e32.step("em3d_bicgstab_update", u32.data_ptr(), p.data_ptr(), s.data_ptr(), tt.data_ptr(), r32.data_ptr(),
@@ -1059,7 +1144,7 @@ class MixedBiCGStab:
                     st.pending = 0
                     continue
                 if restart[b]:
-                    row(rh, b).copy_(row(r32, b))
+                    _dcopy(row(rh, b), row(r32, b))
                     st.iter = 0
                     st.rho_re, st.rho_im = n0[b] * n0[b], 0.0
                     st.rho_prev_re, st.rho_prev_im = 1.0, 0.0
@@ -1126,7 +1211,7 @@ class MixedBiCGStab:
             rel_t = true_residual(late)
             for b in late:
                 final[b] = float(rel_t[b])
-        u = x.clone()  # the cached buffer is reused by the next solve
+        u = _dclone(x)  # the cached buffer is reused by the next solve
         out = []
         for b in range(batch):
             ub = _entry(operator, u, b, batch)

@@ -254,17 +254,22 @@ int em3d_acoustic_rmatvec_uneven(int dtype, int nseg, const em3d_segment* segs, 
 
 /* A matvec of one right-hand side (EM with chi stored in chi_layout, or
  * acoustic) whose last pass also writes, per CTA, the partial sums of
- * |t|^2 and Re / Im of vdot(t, u) of its output t = u - A' u, three doubles
- * per CTA at partials[3 * cta]: the inner products BiCGStab forms right after
- * t = A s (src/em3d/solvers/bicgstab.py:153-163), without reading t and s
- * again.  em3d_matvec_dot_parts gives the number of CTAs (partials holds 3x
- * that many doubles); 0 when the z axis has no register FFT (then this call
- * returns EM3D_ERR_UNSUPPORTED).  em3d_bicgstab_omega_parts finishes omega
- * from the partials. */
+ * |t|^2 and Re / Im of vdot(t, w) of its output t = u - A' u, three doubles
+ * per CTA at partials[3 * cta]; w = dot_with (nullable; the layout and
+ * element type of u), u itself when dot_with is NULL.  These are the inner
+ * products BiCGStab forms right after each matvec, without reading the
+ * vectors again: vdot(t, t) and vdot(t, s) after t = A s (u = s, dot_with
+ * NULL; src/em3d/solvers/bicgstab.py:151-161) and vdot(r_hat, v) =
+ * conj(vdot(v, r_hat)) after v = A p (u = p, dot_with = r_hat;
+ * bicgstab.py:106-108).  em3d_matvec_dot_parts gives the number of CTAs
+ * (partials holds 3x that many doubles); 0 when the z axis has no register
+ * FFT (then this call returns EM3D_ERR_UNSUPPORTED).
+ * em3d_bicgstab_omega_parts and em3d_bicgstab_alpha_parts finish omega and
+ * alpha from the partials. */
 int em3d_matvec_dot_parts(int kind, const em3d_grid* g, int dtype);
 int em3d_matvec_dots(int kind, const em3d_grid* g, int dtype, const void* spectrum, int chi_layout, const void* chi,
                      const void* u, void* out, void* ws, size_t ws_bytes, const int* skip, double* partials,
-                     void* stream);
+                     const void* dot_with, void* stream);
 
 /* Scalar versions.  Replace AcousticOperator.matvec / rmatvec
  * (src/em3d/acoustics/operator.py:40-67). */
@@ -353,6 +358,15 @@ int em3d_vec_dots(int dtype, size_t n, int batch, const void* x0, const void* y0
 /* out = a*x + b*y (scalars rounded to the vector dtype; y may be NULL). */
 int em3d_vec_axpby(int dtype, size_t n, void* out, double a_re, double a_im, const void* x, double b_re,
                    double b_im, const void* y, void* stream);
+/* dst = src for a few bytes (at most em3d_copy_small_max_bytes(), both
+ * 4-byte aligned) between device memory and pinned host memory, by a kernel
+ * on `stream` rather than a copy engine: a small read-back or state upload
+ * of a solver then never waits behind a large transfer that another stream
+ * queued on the copy engines.  Pageable host memory is refused
+ * (EM3D_ERR_INVALID); the copy is complete once the stream has reached it. */
+size_t em3d_copy_small_max_bytes(void);
+int em3d_copy_small(void* dst, const void* src, size_t bytes, void* stream);
+
 /* Precision conversion dst = src (complex64 <-> complex128), or, with
  * accumulate = 1, dst += src. */
 int em3d_vec_convert(size_t n, int src_dtype, const void* src, int dst_dtype, void* dst, int accumulate,
@@ -367,6 +381,9 @@ int em3d_bicgstab_omega(int dtype, size_t n, int batch, void* state, size_t stat
 /* The same omega step for one right-hand side from the nparts per-CTA partial
  * sums (3 doubles each) that em3d_matvec_dots wrote while forming t = A s. */
 int em3d_bicgstab_omega_parts(int nparts, void* state, const double* partials, void* stream);
+/* The alpha step for one right-hand side from the nparts per-CTA partial sums
+ * that em3d_matvec_dots wrote while forming v = A p with dot_with = r_hat. */
+int em3d_bicgstab_alpha_parts(int nparts, void* state, const double* partials, void* stream);
 int em3d_bicgstab_update(int dtype, size_t n, int batch, void* state, size_t state_stride, void* u, const void* p, const void* s, const void* t,
                          void* r, const void* r_hat, void* stream);
 int em3d_bicgstab_finalize(int dtype, size_t n, int batch, void* state, size_t state_stride, void* u, const void* p, void* stream);

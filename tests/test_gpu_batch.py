@@ -43,6 +43,7 @@ def test_batched_solver_matches_single_rhs_solves(solver):
     rhs = torch.cat([rhs, torch.zeros_like(rhs[:1])])
     if solver == "bicgstab":
         s = BiCGStab(SolverConfig(max_iter=200, rtol=1e-9))
+        s.fuse_dots = False  # the batched kernels' inner products, for a like-for-like single solve
     elif solver == "twostep":
         s = TwoStep(SolverConfig(max_iter=200, rtol=1e-8))
     else:
@@ -113,6 +114,7 @@ def test_batched_acoustic_bicgstab():
     dirs = [(0, 0, 1), (1, 0, 0), (0.6, 0.8, 0.0)]
     rhs = torch.stack([ea.plane_wave_scalar(grid, k=20.0, direction=d) for d in dirs])
     s = BiCGStab(SolverConfig(max_iter=300, rtol=1e-8))
+    s.fuse_dots = False  # the batched kernels' inner products, for a like-for-like single solve
     batch = s.solve_batch(op, rhs)
     for b in range(len(dirs)):
         single = s.solve(op, rhs[b])

@@ -240,10 +240,10 @@ def test_defect_correction_rejects_a_bad_guess():
 
 @pytest.mark.parametrize("N", [(32, 32, 32), (24, 20, 40)])
 def test_fused_omega_dots_match_separate_kernels(N):
-    """BiCGStab and MixedBiCGStab with omega's inner products formed in the
-    operator's last pass (one right-hand side) follow the same iterations as
-    with the separate omega kernel; a z axis without a register FFT (2 Nz =
-    80) falls back to the separate kernel."""
+    """BiCGStab and MixedBiCGStab with alpha's and omega's inner products
+    formed in the operator's last pass (one right-hand side) follow the same
+    iterations as with the separate alpha and omega kernels; a z axis without
+    a register FFT (2 Nz = 80) falls back to the separate kernels."""
     import em3d_b200 as e
     from em3d_b200 import scenes
     from em3d_b200.solvers import BiCGStab, MixedBiCGStab, SolverConfig
@@ -270,3 +270,26 @@ def test_fused_omega_dots_match_separate_kernels(N):
         assert a.iterations == c.iterations and a.matvec_count == c.matvec_count
         np.testing.assert_allclose(a.residual_history, c.residual_history, rtol=1e-6)
         assert rel_err(a.u.cpu().numpy(), c.u.cpu().numpy()) < 1e-8
+
+
+def test_copy_small_between_device_and_pinned_host():
+    """em3d_copy_small moves a few bytes (a ragged tail included) from device
+    memory to pinned host memory and back by a kernel, and refuses pageable
+    host memory."""
+    import torch
+
+    from em3d_b200 import _lib
+
+    src = torch.arange(1001, dtype=torch.int32, device="cuda").view(torch.uint8)[:4002]
+    host = torch.zeros(4004, dtype=torch.uint8).pin_memory()
+    stream = torch.cuda.current_stream()
+    _lib.call("em3d_copy_small", host.data_ptr(), src.data_ptr(), 4002, stream.cuda_stream)
+    stream.synchronize()
+    assert torch.equal(host[:4002], src.cpu()) and int(host[4002:].sum()) == 0
+    host[:4002] = torch.arange(4002, dtype=torch.int64).remainder(251).to(torch.uint8)
+    back = torch.zeros(4004, dtype=torch.uint8, device="cuda")
+    _lib.call("em3d_copy_small", back.data_ptr(), host.data_ptr(), 4002, stream.cuda_stream)
+    assert torch.equal(back[:4002].cpu(), host[:4002]) and int(back[4002:].sum()) == 0
+    pageable = torch.zeros(16, dtype=torch.uint8)
+    with pytest.raises(ValueError, match="pinned host memory"):
+        _lib.call("em3d_copy_small", pageable.data_ptr(), src.data_ptr(), 16, stream.cuda_stream)

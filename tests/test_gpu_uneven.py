@@ -187,6 +187,7 @@ def test_uneven_bicgstab_matches_problem_by_problem():
     probs = _problems([(16, 16, 16), (32, 16, 48), (16, 16, 16), (32, 32, 32)], "double")
     group = UnevenGroup(probs)
     s = BiCGStab(SolverConfig(max_iter=300, rtol=1e-9))
+    s.fuse_dots = False  # the batched kernels' inner products, for a like-for-like single solve
     batch = s.solve_batch(group, group.waves())
     iters = []
     for b in range(len(group)):

@@ -122,4 +122,4 @@ def test_fused_dot_parts_counts():
     g = L.make_grid((16, 16, 16), (1.0, 1.0, 1.0))
     with pytest.raises(ValueError, match="partials"):
         L.call("em3d_matvec_dots", L.EM3D_EM, ctypes.byref(g), L.EM3D_C64, 16, 9, 16, 32, 48, 64, 1 << 30, None,
-               None, None)
+               None, None, None)
