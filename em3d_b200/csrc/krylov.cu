@@ -16,6 +16,9 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 148 * 8;
 constexpr int kPartials = 8;  // values per block
+// threads of the one CTA that adds an operator pass's per-CTA partial sums
+// (a few thousand values: many loads in flight, one block_sum)
+constexpr int kPartsThreads = 1024;
 constexpr size_t kStateHeader = 256;
 
 static_assert(sizeof(em3d_krylov_state) <= kStateHeader, "state header too small");
@@ -283,10 +286,11 @@ __global__ void __launch_bounds__(kThreads) k_bicg_alpha(size_t n, void* state, 
 // The same alpha from per-CTA partial sums (|v|^2, Re / Im of vdot(v, r_hat))
 // that the operator's last pass wrote while it produced v = A p
 // (em3d_matvec_dots with r_hat as the second vector): den = conj of their sum.
-__global__ void __launch_bounds__(kThreads) k_bicg_alpha_parts(int nparts, void* state, const double* parts) {
+__global__ void __launch_bounds__(kPartsThreads) k_bicg_alpha_parts(int nparts, void* state, const double* parts) {
   StateView sv = view(state, 0);
   if (!running(sv.st)) return;
   double a[2] = {0, 0};
+#pragma unroll 4
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
     a[0] += parts[(size_t)3 * i + 1];
     a[1] += parts[(size_t)3 * i + 2];
@@ -374,10 +378,11 @@ __global__ void __launch_bounds__(kThreads) k_bicg_omega(size_t n, void* state, 
 // The same omega from per-CTA partial sums (|t|^2, Re / Im of vdot(t, s))
 // that the operator's last pass wrote while it produced t = A s
 // (em3d_matvec_dots): one CTA adds them in a fixed order.
-__global__ void __launch_bounds__(kThreads) k_bicg_omega_parts(int nparts, void* state, const double* parts) {
+__global__ void __launch_bounds__(kPartsThreads) k_bicg_omega_parts(int nparts, void* state, const double* parts) {
   StateView sv = view(state, 0);
   if (!running(sv.st)) return;
   double a[3] = {0, 0, 0};
+#pragma unroll 4
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
 #pragma unroll
     for (int q = 0; q < 3; ++q) a[q] += parts[(size_t)3 * i + q];
@@ -386,14 +391,33 @@ __global__ void __launch_bounds__(kThreads) k_bicg_omega_parts(int nparts, void*
   if (threadIdx.x == 0) omega_from_dots(sv, state, a);
 }
 
+// Early exits at s (converged / guard / budget / breakdown_t / breakdown_omega)
+// return u + alpha p: applied once (pending 1 -> 2) by the update kernel of
+// the iteration that stopped, or by k_bicg_finalize.  u, p: this right-hand
+// side's vectors.
+template <typename R>
+__device__ __forceinline__ void bicg_finish_early(StateView& sv, size_t n, cx<R>* u, const cx<R>* p) {
+  n = used_len(sv.st, n);
+  const cx<R> al = cast_s<R>(sv.st->alpha_re, sv.st->alpha_im);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    u[i] = cadd(u[i], cmul(al, p[i]));
+  double a[1] = {0};
+  double tot[1];
+  if (reduce_last<1>(sv, a, tot) && threadIdx.x == 0) sv.st->pending = 2;
+}
+
 // u = (u + alpha p) + omega s;  r = s - omega t;  ||r||, vdot(r_hat, r) for the
-// next rho; stopping checks on ||r||.
+// next rho; stopping checks on ||r||.  A right-hand side that stopped earlier
+// in this iteration with an early exit pending gets u + alpha p instead.
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_bicg_update(size_t n, void* state, size_t sstride, cx<R>* u, const cx<R>* p,
                                                           const cx<R>* s, const cx<R>* t, cx<R>* r,
                                                           const cx<R>* rh) {
   StateView sv = view(state, sstride);
-  if (!running(sv.st)) return;
+  if (!running(sv.st)) {
+    if (*(volatile int*)&sv.st->pending == 1) bicg_finish_early<R>(sv, n, u + blockIdx.y * n, p + blockIdx.y * n);
+    return;
+  }
   { const size_t vo = blockIdx.y * n; u += vo; p += vo; s += vo; t += vo; r += vo; rh += vo; }
   n = used_len(sv.st, n);
   const cx<R> al = cast_s<R>(sv.st->alpha_re, sv.st->alpha_im);
@@ -429,20 +453,13 @@ __global__ void __launch_bounds__(kThreads) k_bicg_update(size_t n, void* state,
   }
 }
 
-// Early exits at s (converged / guard / budget / breakdown_t / breakdown_omega)
-// return u + alpha p.  Runs whatever the status; pending goes 1 -> 2 when done.
+// The same completion of an early exit as a kernel of its own (for drivers
+// that stop between the s and update steps); a no-op once it has been applied.
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_bicg_finalize(size_t n, void* state, size_t sstride, cx<R>* u, const cx<R>* p) {
   StateView sv = view(state, sstride);
   if (*(volatile int*)&sv.st->pending != 1) return;
-  { const size_t vo = blockIdx.y * n; u += vo; p += vo; }
-  n = used_len(sv.st, n);
-  const cx<R> al = cast_s<R>(sv.st->alpha_re, sv.st->alpha_im);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    u[i] = cadd(u[i], cmul(al, p[i]));
-  double a[1] = {0};
-  double tot[1];
-  if (reduce_last<1>(sv, a, tot) && threadIdx.x == 0) sv.st->pending = 2;
+  bicg_finish_early<R>(sv, n, u + blockIdx.y * n, p + blockIdx.y * n);
 }
 
 // ---------------------------------------------------------------------------
@@ -725,7 +742,7 @@ EM3D_STEP(em3d_bicgstab_s, k_bicg_s,
 int em3d_bicgstab_omega_parts(int nparts, void* state, const double* partials, void* stream) {
   if (int rc = check_state(state, 1)) return rc;
   if (nparts < 1 || !partials) { em3d_set_last_error("em3d_bicgstab_omega_parts: no partial sums"); return EM3D_ERR_INVALID; }
-  k_bicg_omega_parts<<<1, kThreads, 0, (cudaStream_t)stream>>>(nparts, state, partials);
+  k_bicg_omega_parts<<<1, kPartsThreads, 0, (cudaStream_t)stream>>>(nparts, state, partials);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }
@@ -733,7 +750,7 @@ int em3d_bicgstab_omega_parts(int nparts, void* state, const double* partials, v
 int em3d_bicgstab_alpha_parts(int nparts, void* state, const double* partials, void* stream) {
   if (int rc = check_state(state, 1)) return rc;
   if (nparts < 1 || !partials) { em3d_set_last_error("em3d_bicgstab_alpha_parts: no partial sums"); return EM3D_ERR_INVALID; }
-  k_bicg_alpha_parts<<<1, kThreads, 0, (cudaStream_t)stream>>>(nparts, state, partials);
+  k_bicg_alpha_parts<<<1, kPartsThreads, 0, (cudaStream_t)stream>>>(nparts, state, partials);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }

@@ -621,9 +621,9 @@ class BiCGStab(_KrylovSolver):
             eng.alpha_step(p, v, r_hat, self.fuse_dots)
             eng.step("em3d_bicgstab_s", r.data_ptr(), v.data_ptr(), s.data_ptr())
             eng.omega_step(s, t, self.fuse_dots)
+            # (the update also completes an early exit taken at s: u + alpha p)
             eng.step("em3d_bicgstab_update", u.data_ptr(), p.data_ptr(), s.data_ptr(), t.data_ptr(), r.data_ptr(),
                      r_hat.data_ptr())
-            eng.step("em3d_bicgstab_finalize", u.data_ptr(), p.data_ptr())
 
         eng.run(iteration, self.graph_chunk, use_graph=True)
         res = self._results(eng, u, trivial)
@@ -1109,7 +1109,6 @@ class MixedBiCGStab:
             e32.omega_step(s, tt, self.fuse_dots)
             e32.step("em3d_bicgstab_update", u32.data_ptr(), p.data_ptr(), s.data_ptr(), tt.data_ptr(), r32.data_ptr(),
                      rh.data_ptr())
-            e32.step("em3d_bicgstab_finalize", u32.data_ptr(), p.data_ptr())
 
         hosts = e32.state.hosts
         restart = [True] * batch

@@ -373,7 +373,11 @@ int em3d_vec_convert(size_t n, int src_dtype, const void* src, int dst_dtype, vo
                      void* stream);
 
 /* BiCGStab (src/em3d/solvers/bicgstab.py:12-211), one iteration =
- *   p -> [matvec v = A p] -> alpha -> s -> [matvec t = A s] -> omega -> update -> finalize */
+ *   p -> [matvec v = A p] -> alpha -> s -> [matvec t = A s] -> omega -> update
+ * The update also completes an early exit taken at s in the same iteration
+ * (the reference returns u + alpha p there); em3d_bicgstab_finalize does only
+ * that, for a driver that stops between s and update, and is a no-op once the
+ * exit has been completed. */
 int em3d_bicgstab_p(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* r, void* p, const void* v, void* stream);
 int em3d_bicgstab_alpha(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* r_hat, const void* v, void* stream);
 int em3d_bicgstab_s(int dtype, size_t n, int batch, void* state, size_t state_stride, const void* r, const void* v, void* s, void* stream);
