@@ -384,12 +384,15 @@ class _Engine:
         _lib.call("em3d_bicgstab_omega_parts", parts, self.state.ptr, buf.data_ptr(), self.stream())
 
     def run(self, iteration, chunk: int, use_graph: bool):
-        """Launch ``iteration`` until every right-hand side has stopped.  With a
-        native operator the iterations are replayed ``chunk`` at a time from a
-        CUDA graph."""
+        """Launch ``iteration`` until every right-hand side has stopped (the
+        states as last uploaded by :meth:`DeviceState.upload`).  With a native
+        operator the iterations are replayed ``chunk`` at a time from a CUDA
+        graph."""
         import torch
 
-        if self.poll():
+        # every caller uploads the states right before: whether any right-hand
+        # side runs is known on the host, without a read-back
+        if not any(int(h.status) == 0 for h in self.state.hosts):
             return
         if self.graph is None and use_graph and self.native_op:
             iteration()  # the first iteration runs eagerly (and loads the kernels)
