@@ -18,16 +18,19 @@ namespace em3d {
 
 constexpr int kIoThreads = 256;
 
+// W-byte words (16 when both addresses are 16-byte aligned: fewer, larger
+// requests over the host link), then the ragged tail byte by byte.  Loads
+// bypass the caches (ld.global.cv): a pinned staging buffer is rewritten by
+// the host between uploads.
+template <typename W>
 __global__ void __launch_bounds__(kIoThreads) k_copy_small(unsigned char* dst, const unsigned char* src, size_t bytes) {
-  const size_t words = bytes / 4;
+  const size_t words = bytes / sizeof(W);
   const size_t gs = (size_t)gridDim.x * blockDim.x;
-  uint32_t* d4 = reinterpret_cast<uint32_t*>(dst);
-  const uint32_t* s4 = reinterpret_cast<const uint32_t*>(src);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += gs)
-    d4[i] = *reinterpret_cast<const volatile uint32_t*>(s4 + i);
-  const size_t tail = words * 4;
-  if (blockIdx.x == 0 && threadIdx.x < bytes - tail)
-    dst[tail + threadIdx.x] = *reinterpret_cast<const volatile unsigned char*>(src + tail + threadIdx.x);
+  W* dw = reinterpret_cast<W*>(dst);
+  const W* sw = reinterpret_cast<const W*>(src);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += gs) dw[i] = __ldcv(sw + i);
+  const size_t tail = words * sizeof(W);
+  if (blockIdx.x == 0 && threadIdx.x < bytes - tail) dst[tail + threadIdx.x] = __ldcv(src + tail + threadIdx.x);
 }
 
 // The address a kernel uses for p: device memory as is, pinned host memory by
@@ -47,7 +50,7 @@ static const void* device_address(const void* p) {
 
 using namespace em3d;
 
-size_t em3d_copy_small_max_bytes(void) { return (size_t)1 << 20; }
+size_t em3d_copy_small_max_bytes(void) { return (size_t)16 << 20; }
 
 int em3d_copy_small(void* dst, const void* src, size_t bytes, void* stream) {
   if (bytes == 0) return EM3D_OK;
@@ -66,10 +69,13 @@ int em3d_copy_small(void* dst, const void* src, size_t bytes, void* stream) {
     em3d_set_last_error("em3d_copy_small: dst and src must be device memory or pinned host memory");
     return EM3D_ERR_INVALID;
   }
-  const size_t words = bytes / 4;
-  const int blocks = (int)std::min<size_t>(64, std::max<size_t>(1, (words + kIoThreads - 1) / kIoThreads));
-  k_copy_small<<<blocks, kIoThreads, 0, (cudaStream_t)stream>>>(static_cast<unsigned char*>(d),
-                                                                 static_cast<const unsigned char*>(s), bytes);
+  const bool wide = (((uintptr_t)d | (uintptr_t)s) & 15) == 0;
+  const size_t words = bytes / (wide ? 16 : 4);
+  const int blocks = (int)std::min<size_t>(148, std::max<size_t>(1, (words + kIoThreads - 1) / kIoThreads));
+  unsigned char* dd = static_cast<unsigned char*>(d);
+  const unsigned char* ss = static_cast<const unsigned char*>(s);
+  if (wide) k_copy_small<uint4><<<blocks, kIoThreads, 0, (cudaStream_t)stream>>>(dd, ss, bytes);
+  else k_copy_small<uint32_t><<<blocks, kIoThreads, 0, (cudaStream_t)stream>>>(dd, ss, bytes);
   EM3D_LAUNCH_CHECK();
   return EM3D_OK;
 }

@@ -101,6 +101,10 @@ class DeviceState:
     block per right-hand side (struct + history + reduction partials)."""
 
     DONE_OFFSET = KrylovState.batch_done.offset
+    # states up to this size (one or a few right-hand sides) move by
+    # em3d_copy_small; a wide batch's megabytes of states upload faster by a
+    # copy engine than by a kernel reading host memory
+    SMALL_LIMIT = 256 * 1024
 
     def __init__(self, device, hist_cap: int, batch: int = 1):
         import torch
@@ -121,7 +125,7 @@ class DeviceState:
         # by em3d_copy_small (a kernel on the solving stream), so they never wait
         # behind a large copy-engine transfer issued on another stream
         nbytes = self.stride * self.batch
-        self._small = nbytes <= int(lib.em3d_copy_small_max_bytes())
+        self._small = nbytes <= min(self.SMALL_LIMIT, int(lib.em3d_copy_small_max_bytes()))
         self._hbuf = self._hstage = None
         self._staged = None  # event after the last upload from the staging buffer
         if self._small:
@@ -129,6 +133,16 @@ class DeviceState:
             self._hstage = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
             self._hview = self._hbuf.numpy()
             self._sview = self._hstage.numpy()
+            # pinned memory that this device cannot address (an allocation made
+            # for another device's context) is refused: the copies then stay
+            # with torch (copy engines)
+            status = lib.em3d_copy_small(self._hbuf.data_ptr(), self.buf.data_ptr(), 4,
+                                         torch.cuda.current_stream(self.buf.device).cuda_stream)
+            if status != 0:
+                self._small = False
+                self._hbuf = self._hstage = None
+            else:
+                _lib.count_launches("em3d_copy_small")
 
     def _read(self, off: int, nbytes: int) -> np.ndarray:
         """Bytes [off, off + nbytes) of the device buffer once the current
