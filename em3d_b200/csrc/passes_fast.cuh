@@ -109,6 +109,19 @@ __device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restri
       a[0][q * R1 + r] = v;
     }
   }
+  // u - y (the last pass of a matvec): u at this thread's output positions is
+  // loaded before the transform, so its latency overlaps the butterflies
+  constexpr bool PRE = INV && (ST == FST_SUB || ST == FST_SUB_DOTS);
+  T pre[PRE ? E / 2 : 1];
+  if constexpr (PRE) {
+#pragma unroll
+    for (int q = 0; q < E / RL; ++q) {
+      const int j = t + q * TT;
+#pragma unroll
+      for (int r = 0; r < RL / 2; ++r)
+        pre[q * (RL / 2) + r] = valid ? base[ob + ((size_t)c * rows_pb + row) * LOUT + j + r * ML] : mk<R>(0, 0);
+    }
+  }
   __syncthreads();
   const LayRows lay{pen * G::PSTRIDE, G::PSTRIDE};
   reg_fft<L, E, INV, false, 1, !INV>(a, t, sm, tw, lay);
@@ -157,7 +170,7 @@ __device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restri
         for (int r = 0; r < RL / 2; ++r) {
           const int pos = j + r * ML;
           const size_t oo = ob + ((size_t)c * rows_pb + row) * LOUT + pos;
-          const T s = base[oo];
+          const T s = pre[q * (RL / 2) + r];
           const T v = csub(s, a[0][q * RL + r]);
           out[oo] = v;
           const T w = wv ? wv[oo] : s;
@@ -195,7 +208,7 @@ __device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restri
         const T y = a[0][q * RL + r];
         const size_t oo = ob + ((size_t)c * rows_pb + row) * LOUT + pos;
         if constexpr (ST == FST_PLAIN) out[oo] = y;
-        else if constexpr (ST == FST_SUB) out[oo] = csub(base[oo], y);
+        else if constexpr (ST == FST_SUB) out[oo] = csub(PRE ? pre[q * (RL / 2) + r] : base[oo], y);
         else if constexpr (ST == FST_AC_ADJ || ST == FST_EM_ADJ1)  // chi^H y = conj(s) y per component
           out[oo] = csub(base[oo], cmulcj(chb[(size_t)row * LOUT + pos], y));
       }

@@ -1067,14 +1067,14 @@ class MixedBiCGStab:
             mv64[list(active)] += 1
             _lib.call("em3d_vec_axpby", eng.dt, eng.n * batch, r.data_ptr(), 1.0, 0.0, f.data_ptr(), -1.0, 0.0,
                       r.data_ptr(), stream)
-            rel_ = eng.norms(r) / fs
-            _check_status(operator)
-            return rel_
+            # (the FP64 operator's status words are read once, at the end)
+            return eng.norms(r) / fs
 
         hist = [[] for _ in range(batch)]
         counts = [[] for _ in range(batch)]
         rejected = [False] * batch
         estimated = [False] * batch  # history holds only the FP32 estimate
+        n32_guess = None  # FP32 norms of r32 as the guess left it (the first cycle reuses them)
         u32, r32, rh, p, v, s, tt = (V[k] for k in ("u", "r", "r_hat", "p", "v", "s", "t"))
         mv32 = np.zeros(batch, dtype=np.int64)
         r32_ready = False  # the first cycle starts from r32 as it stands
@@ -1095,13 +1095,16 @@ class MixedBiCGStab:
                 _lib.call("em3d_vec_axpby", _lib.EM3D_C64, n_all, r32.data_ptr(), 1.0, 0.0, r32.data_ptr(), -1.0, 0.0,
                           v.data_ptr(), stream)
                 mv32[active] += 1
-                rel = e32.norms(r32) / fs
+                n32 = e32.norms(r32)
+                rel = n32 / fs
                 if any(rel[b] < 10.0 * tol[b] or not np.isfinite(rel[b]) for b in active):
                     rel = true_residual(active)
                 else:
                     r32_ready = True
+                    n32_guess = n32
             for b in active:
                 if x0 is not None and self.guess_fallback and not rel[b] < 1.0:
+                    n32_guess = None  # r32 changes below
                     row(x, b).zero_()
                     _dcopy(row(r, b), row(f, b))
                     if r32_ready:
@@ -1145,9 +1148,10 @@ class MixedBiCGStab:
             if not r32_ready:
                 _lib.call("em3d_vec_convert", eng.n * batch, eng.dt, r.data_ptr(), _lib.EM3D_C64, r32.data_ptr(), 0,
                           stream)
+            n0 = n32_guess if (r32_ready and n32_guess is not None) else e32.norms(r32)
             r32_ready = False
+            n32_guess = None
             u32.zero_()
-            n0 = e32.norms(r32)
             dots = None
             if any(not restart[b] for b in running):
                 _lib.call("em3d_vec_dots", _lib.EM3D_C64, e32.n, batch, rh.data_ptr(), r32.data_ptr(), None, None,
@@ -1227,6 +1231,7 @@ class MixedBiCGStab:
             rel_t = true_residual(late)
             for b in late:
                 final[b] = float(rel_t[b])
+        _check_status(operator)  # a lost transfer in any FP64 application of this solve
         u = _dclone(x)  # the cached buffer is reused by the next solve
         out = []
         for b in range(batch):
