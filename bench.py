@@ -60,7 +60,7 @@ CONFIG = {"workload": f"warmstart_heldout_scenes_{N_GRID}^3", "scenes": SCENE_SE
 # 128^3 (all five passes, default x-pass variant, the contrast stored as its
 # six symmetric components) from an ncu launch list of the same operator
 # (-k regex:kf_, second matvec of the run).
-NCU_TRAFFIC_BYTES = 1349.6e6
+NCU_TRAFFIC_BYTES = 1348.0e6
 
 
 def byte_model(n: int, c: int) -> int:
