@@ -290,6 +290,11 @@ def test_copy_small_between_device_and_pinned_host():
     back = torch.zeros(4004, dtype=torch.uint8, device="cuda")
     _lib.call("em3d_copy_small", back.data_ptr(), host.data_ptr(), 4002, stream.cuda_stream)
     assert torch.equal(back[:4002].cpu(), host[:4002]) and int(back[4002:].sum()) == 0
+    # addresses 4-byte but not 16-byte aligned take the 4-byte word path
+    host.zero_()
+    _lib.call("em3d_copy_small", host.data_ptr() + 4, src.data_ptr() + 4, 998, stream.cuda_stream)
+    stream.synchronize()
+    assert torch.equal(host[4:1002], src[4:1002].cpu()) and int(host[:4].sum()) == 0 and int(host[1002:].sum()) == 0
     pageable = torch.zeros(16, dtype=torch.uint8)
     with pytest.raises(ValueError, match="pinned host memory"):
         _lib.call("em3d_copy_small", pageable.data_ptr(), src.data_ptr(), 16, stream.cuda_stream)
