@@ -70,6 +70,23 @@ def test_invalid_arguments_are_reported_not_launched():
         _lib.call("em3d_bicgstab_p", _lib.EM3D_C64, 10, 1, None, 0, 1, 1, 1, None)
     with pytest.raises(ValueError, match="batch"):
         _lib.call("em3d_bicgstab_p", _lib.EM3D_C64, 10, 0, 1, 0, 1, 1, 1, None)
+    # the one-CTA finishes of the fused inner products
+    with pytest.raises(ValueError, match="state is NULL"):
+        _lib.call("em3d_bicgstab_alpha_parts", 4, None, 16, None)
+    with pytest.raises(ValueError, match="no partial sums"):
+        _lib.call("em3d_bicgstab_omega_parts", 0, 16, 16, None)
+    with pytest.raises(ValueError, match="no partial sums"):
+        _lib.call("em3d_bicgstab_alpha_parts", 4, 16, None, None)
+    # small transfers by kernel: null, oversized and misaligned requests
+    lib = _lib.load()
+    assert lib.em3d_copy_small_max_bytes() >= 1 << 20
+    with pytest.raises(ValueError, match="null pointer"):
+        _lib.call("em3d_copy_small", None, 16, 16, None)
+    with pytest.raises(ValueError, match="max_bytes"):
+        _lib.call("em3d_copy_small", 16, 32, lib.em3d_copy_small_max_bytes() + 4, None)
+    with pytest.raises(ValueError, match="4-byte aligned"):
+        _lib.call("em3d_copy_small", 18, 32, 16, None)
+    assert lib.em3d_copy_small(16, 32, 0, None) == 0  # nothing to copy
 
 
 def test_krylov_state_layout_matches_library():
