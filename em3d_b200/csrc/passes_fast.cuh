@@ -109,9 +109,10 @@ __device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restri
       a[0][q * R1 + r] = v;
     }
   }
-  // u - y (the last pass of a matvec): u at this thread's output positions is
-  // loaded before the transform, so its latency overlaps the butterflies
-  constexpr bool PRE = INV && (ST == FST_SUB || ST == FST_SUB_DOTS);
+  // u - y (the last pass of a matvec) or v - chi^H y (of an adjoint): u or v
+  // at this thread's output positions is loaded before the transform, so its
+  // latency overlaps the butterflies
+  constexpr bool PRE = INV && ST != FST_PLAIN;
   T pre[PRE ? E / 2 : 1];
   if constexpr (PRE) {
 #pragma unroll
@@ -153,7 +154,7 @@ __device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restri
           acc = cadd(acc, cmulcj(chb[(size_t)ci * cs + o], yk));
         }
         const size_t oo = ob + (size_t)c * cs + o;
-        out[oo] = csub(base[oo], acc);
+        out[oo] = csub(pre[q * (RL / 2) + r], acc);
       }
     }
     return;
@@ -210,7 +211,7 @@ __device__ __forceinline__ void rows_body(const cx<R>* in, const cx<R>* __restri
         if constexpr (ST == FST_PLAIN) out[oo] = y;
         else if constexpr (ST == FST_SUB) out[oo] = csub(PRE ? pre[q * (RL / 2) + r] : base[oo], y);
         else if constexpr (ST == FST_AC_ADJ || ST == FST_EM_ADJ1)  // chi^H y = conj(s) y per component
-          out[oo] = csub(base[oo], cmulcj(chb[(size_t)row * LOUT + pos], y));
+          out[oo] = csub(PRE ? pre[q * (RL / 2) + r] : base[oo], cmulcj(chb[(size_t)row * LOUT + pos], y));
       }
     }
   }
