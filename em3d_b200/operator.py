@@ -18,6 +18,7 @@ Drop-in mirror of the reference ``src/em3d/operator.py:151-428``:
 """
 from __future__ import annotations
 
+import threading
 from dataclasses import dataclass, field
 from math import prod
 from typing import Literal
@@ -121,6 +122,25 @@ def status_word(ws):
     return ws[n - STATUS_BYTES:n - STATUS_BYTES + 4].view(torch.int32)
 
 
+_status_reads = threading.local()
+
+
+def _read_int32(v) -> int:
+    """The int32 at device view ``v``, read through a pinned word by a kernel
+    on the current stream (``em3d_copy_small``) rather than a copy engine,
+    where it could wait behind a large host transfer of another stream."""
+    import torch
+
+    buf = getattr(_status_reads, "buf", None)
+    if buf is None:
+        buf = torch.zeros(4, dtype=torch.int32).pin_memory()
+        _status_reads.buf = buf
+    stream = torch.cuda.current_stream(v.device)
+    _lib.call("em3d_copy_small", buf.data_ptr(), v.data_ptr(), 4, stream.cuda_stream)
+    stream.synchronize()
+    return int(buf[0])
+
+
 def raise_on_failed_waits(workspaces, what: str, counts=None) -> None:
     """Raise ``NativeError`` when a workspace's give-up count is non-zero.
 
@@ -129,7 +149,7 @@ def raise_on_failed_waits(workspaces, what: str, counts=None) -> None:
     count is reset to zero before raising, so the operator stays usable."""
     for i, ws in enumerate(workspaces):
         v = status_word(ws)
-        n = int(v.item()) if counts is None else int(counts[i])
+        n = _read_int32(v) if counts is None else int(counts[i])
         if n:
             v.zero_()
             raise _lib.NativeError(
